@@ -1,0 +1,186 @@
+/* uaamg.h -- C-ABI of the B200-native UAAMG-preconditioned CG pressure solver.
+ *
+ * Drop-in boundary for the reference's pressure-solve path (A-006/UAAMGPCG):
+ * a host C++ Solver / Solver3D subclass (or any FFI) calls these functions in
+ * place of PCG(UAAMGPreconditioner)::solve.  Plain pointers and sizes only.
+ *
+ * Data contract (the reference's, include/core/mesh.h:30-35, mesh_3d.h:38):
+ * every cell array is ghost-padded and column-major with i fastest,
+ *   2D: (nx+2)*(ny+2) cells, id = i + j*(nx+2)
+ *   3D: (nx+2)*(ny+2)*(nz+2) cells, id = i + j*(nx+2) + k*(nx+2)*(ny+2)
+ * interior cells are 1..nx etc.  The solid mask is one byte per padded cell
+ * (non-zero = solid), the expansion of Grid::solid (std::vector<bool>) that the
+ * reference's GPU adapter uploads (src/solver/cuda/cuda_pcg_solver.cu:45-49).
+ *
+ * Sign and null-space convention: identical to PCG::solve (src/solver/pcg.cpp:
+ * 18-33, pcg_3d.cpp:18-36): the solver solves lap(p) = rhs on fluid cells with
+ * Neumann walls and solids, after removing the fluid mean of rhs; the pressure is
+ * accumulated into p (callers zero it first, src/pressure/pressure.cpp:17).
+ *
+ * Every call returns a uaamg_status; none prints or aborts.  A handle is not
+ * thread-safe: one host thread per handle (as the reference's per-object GPU
+ * buffers, include/solver/cuda/cuda_pcg_3d.h:36-40).  All GPU work of a handle is
+ * issued on its stream (uaamg_set_stream; default: the legacy default stream).
+ */
+#ifndef UAAMG_H
+#define UAAMG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define UAAMG_API __attribute__((visibility("default")))
+#else
+#define UAAMG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum uaamg_status {
+    UAAMG_OK = 0,             /* converged (or operation succeeded) */
+    UAAMG_NOT_CONVERGED = 1,  /* max_iter reached; result is the last iterate */
+    UAAMG_BREAKDOWN = 2,      /* p.Ap below the breakdown threshold (pcg.cpp:100) */
+    UAAMG_NAN = 3,            /* a NaN/Inf appeared in a reduction */
+    UAAMG_OOM = 4,            /* device allocation failed */
+    UAAMG_INVALID_ARG = 5,
+    UAAMG_CUDA_ERROR = 6,
+    UAAMG_TIMEOUT = 7,        /* reserved for bounded device waits */
+    UAAMG_NO_PROBLEM = 8      /* solve before uaamg_set_problem_* */
+} uaamg_status;
+
+typedef enum uaamg_precision {
+    UAAMG_FP64 = 0,   /* reference-exact: FP64 everywhere (CudaPCG3D::solve analogue) */
+    UAAMG_FP32 = 1,   /* plain FP32 PCG: FP32 vectors and V-cycle, FP64 reductions */
+    UAAMG_MIXED = 2   /* FP32 CG + FP32 V-cycle, FP64 reductions, FP64 solution with
+                         true-residual replacement every replace_every iterations */
+} uaamg_precision;
+
+typedef enum uaamg_tol_mode {
+    UAAMG_TOL_ABS = 0, /* stop when sqrt(r.r) < tol (PCG::solve, pcg.cpp:111-112) */
+    UAAMG_TOL_REL = 1  /* stop when sqrt(r.r) < tol * ||b||, b the normalised RHS */
+} uaamg_tol_mode;
+
+typedef struct uaamg_options {
+    int precision;      /* uaamg_precision, default UAAMG_FP64 */
+    int tol_mode;       /* uaamg_tol_mode, default UAAMG_TOL_ABS */
+    int max_iter;       /* default 2000 (Config::solve_iters, include/config/config.h:30) */
+    double tol;         /* default 1e-6 (Config::solve_tol, config.h:31) */
+    int warm_start;     /* 0: r0 = b and p is accumulated into (the reference);
+                           1: r0 = b - A p_in, the result is p_in + correction */
+    int replace_every;  /* UAAMG_MIXED residual-replacement period, default 10 */
+    int project_mean;   /* 1: subtract the fluid mean of the result in FP64 */
+    int preconditioner; /* 1: UAAMG V(1,1) (Factory key "pcg_uaamg"); 0: identity ("cg") */
+} uaamg_options;
+
+typedef struct uaamg_stats {
+    int status;                 /* uaamg_status of the solve */
+    int iterations;             /* x/r updates performed */
+    int replacements;           /* FP64 residual replacements (UAAMG_MIXED) */
+    int levels;                 /* multigrid levels */
+    double residual;            /* FP64 true ||b - A p|| at exit (fluid cells) */
+    double rel_residual;        /* residual / ||b|| */
+    double recursive_residual;  /* the CG's recursive ||r|| at exit */
+    double rhs_norm;            /* ||b|| */
+    double solve_ms;            /* wall time of the call, host clock */
+    long long kernel_launches;  /* kernels launched by the call */
+} uaamg_stats;
+
+typedef struct uaamg_handle uaamg_handle;
+
+/* Fills *o with the defaults above. */
+UAAMG_API void uaamg_default_options(uaamg_options* o);
+
+/* Creates a solver handle on CUDA device `device`.  Replaces construction of
+ * CudaPCGSolver / CudaPCGSolver3D (include/solver/cuda_pcg_solver.h:14-32,
+ * cuda_pcg_solver_3d.h:14-32). */
+UAAMG_API uaamg_status uaamg_create(uaamg_handle** out, int device);
+UAAMG_API uaamg_status uaamg_destroy(uaamg_handle* h);
+
+/* Work stream of the handle (a cudaStream_t passed as void*). */
+UAAMG_API uaamg_status uaamg_set_stream(uaamg_handle* h, void* stream);
+
+/* Problem (grid + solid mask) set-up: builds the level masks and Galerkin
+ * coefficients on the device for every precision, once per mask.  Replaces the
+ * per-apply set-up of UAAMGPreconditioner[3D]::apply (uaamg_preconditioner.cpp:
+ * 183-189, uaamg_preconditioner_3d.cpp:205-214) and the GPU adapter's mask
+ * upload (cuda_pcg_solver.cu:27-49).  `solid` is a HOST byte mask (padded). */
+UAAMG_API uaamg_status uaamg_set_problem_2d(uaamg_handle* h, int nx, int ny, double dx, double dy,
+                                  const uint8_t* solid);
+UAAMG_API uaamg_status uaamg_set_problem_3d(uaamg_handle* h, int nx, int ny, int nz, double dx,
+                                  double dy, double dz, const uint8_t* solid);
+/* Same, mask already on the device. */
+UAAMG_API uaamg_status uaamg_set_problem_device(uaamg_handle* h, int dim, int nx, int ny, int nz,
+                                      double dx, double dy, double dz,
+                                      const uint8_t* d_solid);
+/* Cell-centred Dirichlet p = 0 on every domain wall instead of Neumann (the
+ * standalone Ax=b check of test/solver/test_amgpcg.cpp:29-70, on the MAC grid).
+ * Takes effect at the next uaamg_set_problem_*. */
+UAAMG_API uaamg_status uaamg_set_dirichlet_walls(uaamg_handle* h, int on);
+
+/* V-cycle kernels of this handle: 0 (default) = fused, one kernel per level and
+ * direction (sweep + residual + restriction down, prolongation + sweep up);
+ * 1 = one kernel per colour sweep, restriction and prolongation, step by step as
+ * UAAMGPreconditioner3D::vCycle (uaamg_preconditioner_3d.cpp:183-196).  Both give
+ * identical results; 1 exists to cross-check 0. */
+UAAMG_API uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps);
+
+/* Solve lap(p) = rhs with HOST FP64 arrays (padded): the Solver::solve /
+ * Solver3D::solve drop-in (include/solver/solver.h:18-34, solver_3d.h:7-12;
+ * CudaPCGSolver::solve, cuda_pcg_solver.cu:21-63).  Host<->device copies are
+ * part of the call.  opts may be NULL (defaults); stats may be NULL. */
+UAAMG_API uaamg_status uaamg_solve(uaamg_handle* h, const double* rhs, double* p,
+                         const uaamg_options* opts, uaamg_stats* stats);
+
+/* Same with DEVICE FP64 arrays (CudaPCG3D::solve_optimized's device-pointer
+ * form, include/solver/cuda/cuda_pcg_3d.h:10-13). */
+UAAMG_API uaamg_status uaamg_solve_device(uaamg_handle* h, const double* d_rhs, double* d_p,
+                                const uaamg_options* opts, uaamg_stats* stats);
+
+/* One V(1,1) cycle z = M^{-1} r with HOST FP64 arrays: the
+ * Preconditioner[3D]::apply drop-in (include/solver/preconditioner/
+ * preconditioner_3d.h:18-33, UAAMGPreconditioner3D::apply). */
+UAAMG_API uaamg_status uaamg_precond_apply(uaamg_handle* h, int precision, const double* r, double* z);
+
+/* Residual history of the last solve: hist[k] = ||r_k|| for k = 0..iterations
+ * (recursive residual; hist[0] = ||r0||).  n = capacity. */
+UAAMG_API uaamg_status uaamg_residual_history(uaamg_handle* h, double* hist, int n);
+
+/* Hierarchy inspection (bit-exact parity checks): number of levels, level dims,
+ * and host copies of level l's padded mask and couplings (FP64 values of the
+ * given precision's hierarchy; cz ignored in 2D; any pointer may be NULL). */
+UAAMG_API uaamg_status uaamg_num_levels(uaamg_handle* h, int* nlevels);
+UAAMG_API uaamg_status uaamg_level_dims(uaamg_handle* h, int l, int* nx, int* ny, int* nz);
+UAAMG_API uaamg_status uaamg_copy_level(uaamg_handle* h, int precision, int l, uint8_t* solid,
+                              double* cx, double* cy, double* cz);
+
+/* In-situ kernel timing: runs uaamg_solve_device with a CUDA event pair around
+ * every kernel launch and returns, per (kernel class, level), the launch count,
+ * total device time and algorithmic bytes per launch (the compulsory traffic the
+ * roofline is computed from).  Up to cap entries are written; *count receives
+ * the number available.  The extra events make this solve slightly slower than
+ * an unprofiled one.  (No reference counterpart: the reference times whole
+ * solves with host clocks, src/solver/cuda/test_paper_bench.cu:21-28.) */
+typedef struct uaamg_kernel_time {
+    char name[32];
+    int level;
+    int launches;
+    double total_ms;
+    double bytes_per_launch;
+} uaamg_kernel_time;
+UAAMG_API uaamg_status uaamg_profile_solve(uaamg_handle* h, const double* d_rhs, double* d_p,
+                                           const uaamg_options* opts, uaamg_stats* stats,
+                                           uaamg_kernel_time* out, int cap, int* count);
+
+/* Device memory held by the handle, bytes. */
+UAAMG_API uaamg_status uaamg_device_bytes(uaamg_handle* h, size_t* bytes);
+
+/* Text of the last error on this handle (never NULL). */
+UAAMG_API const char* uaamg_last_error(uaamg_handle* h);
+UAAMG_API const char* uaamg_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UAAMG_H */

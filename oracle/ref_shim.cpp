@@ -1,0 +1,157 @@
+// Test infrastructure only: a C-ABI shim around the reference's own CPU solver
+// classes, compiled together with the reference's unmodified source files by
+// oracle/Makefile into oracle/_ref/libuaamg_ref.so.  Nothing in the product links
+// this; tests, smoke() and the bench's CPU-baseline leg load it as the checker.
+//
+// Reference classes driven here:
+//   PCG / PCG3D                    src/solver/pcg.cpp:18-126, src/solver/pcg_3d.cpp:18-125
+//   UAAMGPreconditioner[3D]        src/solver/preconditioner/uaamg_preconditioner.cpp:177-199,
+//                                  src/solver/preconditioner/uaamg_preconditioner_3d.cpp:198-229
+//   IdentityPreconditioner[3D]     include/solver/preconditioner/identity_preconditioner*.h
+//   PressureProjection[3D]         src/pressure/pressure.cpp:5-33, src/pressure/pressure_3d.cpp:5-40
+//   Grid / Grid3D                  include/core/grid.h:16-48, include/core/grid_3d.h:14-38
+#include "core/grid.h"
+#include "core/grid_3d.h"
+#include "solver/pcg.h"
+#include "solver/pcg_3d.h"
+#include "solver/preconditioner/uaamg_preconditioner.h"
+#include "solver/preconditioner/uaamg_preconditioner_3d.h"
+#include "solver/preconditioner/identity_preconditioner.h"
+#include "solver/preconditioner/identity_preconditioner_3d.h"
+#include "pressure/pressure.h"
+#include "pressure/pressure_3d.h"
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+namespace {
+
+// Counts preconditioner applications so the caller can learn how many PCG
+// iterations the reference ran (PCG::solve returns void).
+template <class Base, class GridT>
+class Counting : public Base {
+public:
+    Counting(std::unique_ptr<Base> inner, int* counter) : inner_(std::move(inner)), counter_(counter) {}
+    void apply(const GridT& g, const std::vector<double>& r, std::vector<double>& z) override {
+        if (counter_) ++*counter_;
+        inner_->apply(g, r, z);
+    }
+    std::string name() const override { return inner_->name(); }
+private:
+    std::unique_ptr<Base> inner_;
+    int* counter_;
+};
+
+Grid make2(int nx, int ny, double dx, double dy, const uint8_t* solid) {
+    Grid g(nx, ny, nx * dx, ny * dy);
+    g.dx = dx; g.dy = dy;  // exact spacing, no Lx/nx round trip
+    const int n = g.p_size();
+    if (solid) for (int c = 0; c < n; ++c) g.solid[c] = solid[c] != 0;
+    return g;
+}
+
+Grid3D make3(int nx, int ny, int nz, double dx, double dy, double dz, const uint8_t* solid) {
+    Grid3D g(nx, ny, nz, nx * dx, ny * dy, nz * dz);
+    g.dx = dx; g.dy = dy; g.dz = dz;
+    const int n = g.p_size();
+    if (solid) for (int c = 0; c < n; ++c) g.solid[c] = solid[c] != 0;
+    return g;
+}
+
+}  // namespace
+
+extern "C" {
+
+// One UAAMG V-cycle z = M^{-1} r on padded (nx+2)(ny+2) arrays.
+void ref_vcycle_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+                   const double* r, double* z) {
+    Grid g = make2(nx, ny, dx, dy, solid);
+    const int n = g.p_size();
+    std::vector<double> rv(r, r + n), zv(n, 0.0);
+    UAAMGPreconditioner pc;
+    pc.apply(g, rv, zv);
+    std::memcpy(z, zv.data(), sizeof(double) * n);
+}
+
+void ref_vcycle_3d(int nx, int ny, int nz, double dx, double dy, double dz,
+                   const uint8_t* solid, const double* r, double* z) {
+    Grid3D g = make3(nx, ny, nz, dx, dy, dz, solid);
+    const int n = g.p_size();
+    std::vector<double> rv(r, r + n), zv(n, 0.0);
+    UAAMGPreconditioner3D pc;
+    pc.apply(g, rv, zv);
+    std::memcpy(z, zv.data(), sizeof(double) * n);
+}
+
+// PCG(UAAMG) (precond=1) or PCG(Identity) (precond=0); p is in/out exactly like
+// Grid::p in Solver::solve (callers zero it first).  Returns the number of
+// preconditioner applications.
+int ref_pcg_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+               const double* rhs, double* p, int max_iter, double tol, int precond) {
+    Grid g = make2(nx, ny, dx, dy, solid);
+    const int n = g.p_size();
+    std::memcpy(g.p.data(), p, sizeof(double) * n);
+    int applies = 0;
+    std::unique_ptr<Preconditioner> inner;
+    if (precond) inner = std::make_unique<UAAMGPreconditioner>();
+    else         inner = std::make_unique<IdentityPreconditioner>();
+    PCG solver(std::make_unique<Counting<Preconditioner, Grid>>(std::move(inner), &applies));
+    std::vector<double> rv(rhs, rhs + n);
+    solver.solve(g, rv, max_iter, tol);
+    std::memcpy(p, g.p.data(), sizeof(double) * n);
+    return applies;
+}
+
+int ref_pcg_3d(int nx, int ny, int nz, double dx, double dy, double dz, const uint8_t* solid,
+               const double* rhs, double* p, int max_iter, double tol, int precond) {
+    Grid3D g = make3(nx, ny, nz, dx, dy, dz, solid);
+    const int n = g.p_size();
+    std::memcpy(g.p.data(), p, sizeof(double) * n);
+    int applies = 0;
+    std::unique_ptr<Preconditioner3D> inner;
+    if (precond) inner = std::make_unique<UAAMGPreconditioner3D>();
+    else         inner = std::make_unique<IdentityPreconditioner3D>();
+    PCG3D solver(std::make_unique<Counting<Preconditioner3D, Grid3D>>(std::move(inner), &applies));
+    std::vector<double> rv(rhs, rhs + n);
+    solver.solve(g, rv, max_iter, tol);
+    std::memcpy(p, g.p.data(), sizeof(double) * n);
+    return applies;
+}
+
+// PressureProjection::project with PCG(UAAMG): u (nx+1)(ny+2), v (nx+2)(ny+1)
+// are corrected in place; p (padded) receives the pressure.
+int ref_project_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+                   double* u, double* v, double dt, int max_iter, double tol, double* p) {
+    Grid g = make2(nx, ny, dx, dy, solid);
+    std::memcpy(g.u.data(), u, sizeof(double) * g.u_size());
+    std::memcpy(g.v.data(), v, sizeof(double) * g.v_size());
+    int applies = 0;
+    PCG solver(std::make_unique<Counting<Preconditioner, Grid>>(
+        std::make_unique<UAAMGPreconditioner>(), &applies));
+    PressureProjection::project(g, dt, solver, max_iter, tol);
+    std::memcpy(u, g.u.data(), sizeof(double) * g.u_size());
+    std::memcpy(v, g.v.data(), sizeof(double) * g.v_size());
+    std::memcpy(p, g.p.data(), sizeof(double) * g.p_size());
+    return applies;
+}
+
+int ref_project_3d(int nx, int ny, int nz, double dx, double dy, double dz, const uint8_t* solid,
+                   double* u, double* v, double* w, double dt, int max_iter, double tol, double* p) {
+    Grid3D g = make3(nx, ny, nz, dx, dy, dz, solid);
+    std::memcpy(g.u.data(), u, sizeof(double) * g.u_size());
+    std::memcpy(g.v.data(), v, sizeof(double) * g.v_size());
+    std::memcpy(g.w.data(), w, sizeof(double) * g.w_size());
+    int applies = 0;
+    PCG3D solver(std::make_unique<Counting<Preconditioner3D, Grid3D>>(
+        std::make_unique<UAAMGPreconditioner3D>(), &applies));
+    PressureProjection3D::project(g, dt, solver, max_iter, tol);
+    std::memcpy(u, g.u.data(), sizeof(double) * g.u_size());
+    std::memcpy(v, g.v.data(), sizeof(double) * g.v_size());
+    std::memcpy(w, g.w.data(), sizeof(double) * g.w_size());
+    std::memcpy(p, g.p.data(), sizeof(double) * g.p_size());
+    return applies;
+}
+
+}  // extern "C"

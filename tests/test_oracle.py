@@ -1,0 +1,109 @@
+"""The oracle (plain-C restatement) pinned against the reference: the golden
+fixtures generated from the reference's own code, the compiled reference itself
+where available, and the reference's own known-answer test."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import ROOT, golden_names, load_golden
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_restatement_matches_golden_bit_exact(name):
+    g = load_golden(name)
+    if g["kind"] == "vcycle":
+        z = O.Hierarchy(g["solid"], g["dx"], g["dy"], g["dz"]).vcycle(g["r"])
+        inner = z.copy()
+        assert np.array_equal(inner, g["z"]), f"max diff {np.abs(inner - g['z']).max()}"
+    elif g["kind"] == "pcg":
+        p, n, _ = O.pcg(g["solid"], g["r"], g["dx"], g["dy"], g["dz"], g["max_iter"], g["tol"],
+                        tol_mode=0)
+        assert np.array_equal(p, g["p"]), f"max diff {np.abs(p - g['p']).max()}"
+    else:
+        w = g["w"] if g["w"].size else None
+        rhs = O.divergence_rhs(g["solid"], g["u"], g["v"], w, g["dx"], g["dy"], g["dz"], g["dt"])
+        p, n, _ = O.pcg(g["solid"], rhs, g["dx"], g["dy"], g["dz"], g["max_iter"], g["tol"],
+                        tol_mode=0)
+        assert np.array_equal(p, g["p"])
+        u, v, w2 = O.correct_velocity(g["solid"], p, g["dt"], g["u"], g["v"], w, g["dx"], g["dy"],
+                                      g["dz"])
+        assert np.array_equal(u, g["u_out"]) and np.array_equal(v, g["v_out"])
+        if w is not None:
+            assert np.array_equal(w2, g["w_out"])
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference (oracle/_ref) not present")
+@pytest.mark.parametrize("seed", range(6))
+def test_restatement_matches_compiled_reference_random(seed):
+    rng = np.random.default_rng(100 + seed)
+    dim = 2 + seed % 2
+    shape = tuple(int(x) + 2 for x in rng.integers(2, 21, size=dim))
+    frac = [0.0, 0.1, 0.3, 0.55][seed % 4]
+    solid = (rng.random(shape) < frac).astype(np.uint8)
+    r = rng.standard_normal(shape)
+    sp = rng.uniform(0.05, 2.0, size=3)
+    z_ref = O.ref_vcycle(solid, r, *sp)
+    z = O.Hierarchy(solid, *sp).vcycle(r)
+    assert np.array_equal(z, z_ref)
+    p_ref, _ = O.ref_pcg(solid, r, *sp, max_iter=20, tol=1e-10)
+    p, _, _ = O.pcg(solid, r, *sp, max_iter=20, tol=1e-10, tol_mode=0)
+    assert np.array_equal(p, p_ref)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "test_amgpcg")),
+                    reason="compiled reference test not present")
+def test_reference_known_answer_amgpcg_passes():
+    out = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "test_amgpcg")],
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout
+    assert "Failed: 0" in out.stdout
+
+
+def _dirichlet_problem(n):
+    h = 1.0 / n
+    x = (np.arange(n + 2) - 0.5) * h
+    X, Y = np.meshgrid(x, x, indexing="xy")  # [j, i]
+    exact = np.sin(np.pi * X) * np.sin(np.pi * Y)
+    f = 2 * np.pi ** 2 * exact
+    rhs = np.zeros((n + 2, n + 2))
+    rhs[1:-1, 1:-1] = -f[1:-1, 1:-1]       # lap(p) = rhs  <=>  -lap(p) = f
+    return h, rhs, exact
+
+
+def test_dirichlet_64_analytic_error():
+    """The CPU-runnable plain method: 64x64 cells on [0,1]^2, h = 1/64, Dirichlet
+    p = 0 walls, f = 2 pi^2 sin sin, one V-cycle per iteration, rel. residual
+    1e-10; the error against sin(pi x) sin(pi y) is second order in h."""
+    n = 64
+    h, rhs, exact = _dirichlet_problem(n)
+    solid = np.zeros((n + 2, n + 2), np.uint8)
+    p, it, st = O.pcg(solid, rhs, h, h, max_iter=100, tol=1e-10, tol_mode=1, dirichlet=True)
+    assert st == 0 and it <= 30
+    err = np.abs(p - exact)[1:-1, 1:-1].max()
+    assert err < 1e-3                         # O(h^2): pi^2 h^2 / 8 ~ 3e-4
+    hier = O.Hierarchy(solid, h, h, dirichlet=True)
+    assert hier.nlevels == 5 and hier.dims(4)[:2] == (4, 4)
+    # halving h divides the error by ~4
+    h2, rhs2, exact2 = _dirichlet_problem(32)
+    p2, _, _ = O.pcg(np.zeros((34, 34), np.uint8), rhs2, h2, h2, max_iter=100, tol=1e-10,
+                     tol_mode=1, dirichlet=True)
+    err2 = np.abs(p2 - exact2)[1:-1, 1:-1].max()
+    assert 3.0 < err2 / err < 5.0
+
+
+def test_oracle_relative_mode_reaches_tolerance():
+    rng = np.random.default_rng(7)
+    shape = (14, 18, 22)
+    solid = np.zeros(shape, np.uint8)
+    solid[1:-1, 1:-1, 1:-1] = rng.random((12, 16, 20)) < 0.1
+    rhs = rng.standard_normal(shape)
+    p, it, st = O.pcg(solid, rhs, 0.1, 0.1, 0.1, max_iter=200, tol=1e-8, tol_mode=1)
+    res, bn = O.true_residual(solid, rhs, p, 0.1, 0.1, 0.1)
+    assert st == 0 and res / bn < 2e-8
+    # warm start from the answer converges at once
+    p2, it2, st2 = O.pcg(solid, rhs, 0.1, 0.1, 0.1, max_iter=200, tol=1e-6, tol_mode=1, x0=p,
+                         warm=True)
+    assert it2 <= 1

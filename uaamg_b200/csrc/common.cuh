@@ -1,0 +1,83 @@
+// Shared device-side definitions of the B200 UAAMG-PCG engine.
+//
+// Memory layout (the reference's, include/core/mesh_3d.h:38 and mesh.h:35): every
+// per-cell array of a level is ghost-padded and column-major with i fastest,
+// id = i + j*(nx+2) + k*(nx+2)*(ny+2).  2D levels have no z ghosts: the interior
+// is the single plane k = 0.  Ghost entries of vectors and coefficient channels
+// stay 0, which is what makes Neumann walls need no special-casing in the
+// V-cycle kernels.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace uaamg {
+
+struct Geom {
+    int nx, ny, nz;  // interior cells; nz == 0 for a 2D level
+    int sx, sxy;     // strides in cells: sx = nx+2, sxy = (nx+2)(ny+2)
+    int n;           // padded cell count
+};
+
+inline Geom make_geom(int dim, int nx, int ny, int nz) {
+    Geom g;
+    g.nx = nx; g.ny = ny; g.nz = dim == 3 ? nz : 0;
+    g.sx = nx + 2;
+    g.sxy = (nx + 2) * (ny + 2);
+    g.n = dim == 3 ? g.sxy * (nz + 2) : g.sxy;
+    return g;
+}
+
+// Run status written by the device-side finalisers (CGState::status).
+enum : int {
+    CG_RUNNING = 0,
+    CG_CONVERGED = 1,
+    CG_MAXITER = 2,
+    CG_BREAKDOWN = 3,
+    CG_NAN = 4,
+};
+
+// Device-resident PCG state.  All scalars are FP64; the loop never copies a
+// scalar to the host: alpha/beta/stopping decisions are taken by the last block
+// of the kernel that finishes each reduction.
+struct CGState {
+    double rz_old;     // r.z of the previous iteration
+    double pap;        // p.Ap
+    double alpha, beta;
+    double rr;         // recursive r.r
+    double rr_true;    // FP64 true residual b - A x (residual replacement / exit)
+    double r0;         // ||r0||
+    double tol_abs;    // stop when sqrt(r.r) < tol_abs
+    double mean_z;     // fluid mean of z (null-space projection)
+    double nfluid;     // fluid cell count
+    double sum0, sum1; // scratch sums (RHS normalisation)
+    double bnorm;      // ||b|| of the normalised right-hand side
+    double breakdown;  // p.Ap below this stops the solve (the reference's 1e-15)
+    int done;          // 1 once the solve stopped; every loop kernel then returns at once
+    int status;        // CG_* above
+    int iter;          // completed x/r updates
+    int cand;          // mixed mode: recursive residual met tol, confirm with the true one
+    int max_iter;
+    int replace_every; // mixed mode residual-replacement period (0 = off)
+    int replacements;  // replacements performed
+    int dirichlet;     // 1: no null space (skip mean projections)
+    int init;          // 1 while forming p0 = z0 (beta = 0)
+    int pad_;
+    unsigned int counter[8];  // last-block counters, one per reduction site
+};
+
+// Host-visible launch helpers ------------------------------------------------
+
+template <int DIM>
+inline dim3 cell_block() { return DIM == 3 ? dim3(32, 4, 2) : dim3(32, 8, 1); }
+
+template <int DIM>
+inline dim3 cell_grid(int nx, int ny, int nz) {
+    dim3 b = cell_block<DIM>();
+    return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y,
+                DIM == 3 ? (nz + b.z - 1) / b.z : 1);
+}
+
+inline size_t grid_blocks(dim3 g) { return (size_t)g.x * g.y * g.z; }
+
+}  // namespace uaamg

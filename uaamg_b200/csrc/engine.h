@@ -1,0 +1,80 @@
+// Host-side interface between the C-ABI layer (api.cpp) and the per-precision
+// engines (kernels_f64.cu, kernels_f32.cu).  No CUDA device code here.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace uaamg {
+
+// Engine precision modes (match uaamg_precision in include/uaamg.h).
+enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_MIXED = 2 };
+
+struct SolveArgs {
+    const double* rhs;   // device, padded FP64 right-hand side of  lap(p) = rhs
+    double* x;           // device, padded FP64 pressure: in = accumulate target / warm start
+    int max_iter;
+    double tol;
+    int tol_mode;        // 0 absolute (the reference), 1 relative to ||b||
+    int warm;            // 1: r0 = b - A x_in
+    int replace_every;   // mixed: residual replacement period (iterations)
+    int project_mean;    // subtract the fluid mean of the result (FP64)
+    int precond;         // 1 UAAMG V-cycle, 0 identity (plain CG)
+    double* hist;        // optional device array, max_iter+1: ||r_k|| per update
+};
+
+struct SolveResult {
+    int status;          // CG_* (common.cuh)
+    int iterations;
+    int replacements;
+    double rr;           // recursive r.r at exit
+    double rr_true;      // FP64 ||b - A x||^2 at exit
+    double bnorm;        // ||b||
+    double r0;           // ||r0||
+    double tol_abs;
+};
+
+// Error codes returned by engine calls (0 = success), mapped to uaamg_status
+// by the C-ABI layer.
+enum EngineError : int { E_OK = 0, E_OOM = 1, E_CUDA = 2, E_ARG = 3, E_NOPROB = 4 };
+
+// Aggregated in-situ timing of one kernel class on one level.
+struct KernelTime {
+    int cls;
+    const char* name;
+    int level;
+    int launches;
+    double total_ms;
+    double bytes;  // algorithmic bytes per launch
+};
+
+class Engine {
+public:
+    virtual ~Engine() {}
+    // Builds the level hierarchy for a padded level-0 mask already on the device.
+    virtual int set_problem(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
+                            const uint8_t* d_solid, int dirichlet) = 0;
+    // z = M^{-1} r (one V(1,1) cycle); FP64 device arrays, padded.
+    virtual int precond_apply(const double* d_r, double* d_z) = 0;
+    virtual int solve(const SolveArgs& a, SolveResult* res) = 0;
+    virtual int nlevels() const = 0;
+    virtual void level_dims(int l, int* nx, int* ny, int* nz) const = 0;
+    // Host copies of level l: mask and FP64 views of cx, cy, cz (nullable).
+    virtual int copy_level(int l, uint8_t* solid, double* cx, double* cy, double* cz) = 0;
+    virtual void set_stream(cudaStream_t s) = 0;
+    virtual size_t device_bytes() const = 0;
+    // Number of kernel launches issued by the last solve() (for launch accounting).
+    virtual long launches() const = 0;
+    // V-cycle as per-colour sweep kernels (the cross-check) instead of the fused kernels.
+    virtual void set_vcycle_sweeps(bool on) = 0;
+    // Per-launch CUDA-event timing of subsequent solves (adds two events per launch).
+    virtual void set_profiling(bool on) = 0;
+    virtual int profile_results(std::vector<KernelTime>& out) = 0;
+};
+
+Engine* create_engine_f64();
+Engine* create_engine_f32(int mixed);
+
+}  // namespace uaamg

@@ -1,0 +1,621 @@
+// Device kernels of the B200 UAAMG-PCG engine, templated on the dimension (2 or 3)
+// and the arithmetic type T (double for the reference-exact mode, float for the
+// FP32 and mixed modes).  Included by kernels_f64.cu (built with -fmad=false so
+// every a*b+c rounds twice, as the reference's x86-64 build does) and by
+// kernels_f32.cu; everything here has internal linkage so each translation unit
+// owns its copy.
+//
+// Reference algorithm (A-006/UAAMGPCG, src/solver/preconditioner/
+// uaamg_preconditioner_3d.cpp and uaamg_preconditioner.cpp; src/solver/pcg_3d.cpp
+// and pcg.cpp).  Per-cell arithmetic follows the reference's operation order so the
+// FP64 mode reproduces it bit for bit; reductions are FP64, deterministic
+// (fixed block partials + fixed-order last-block sum) but ordered differently
+// from the reference's sequential loops.
+#pragma once
+#include "common.cuh"
+
+namespace uaamg {
+namespace {
+
+// ---------------------------------------------------------------------------
+// helpers
+
+template <int DIM>
+__device__ __forceinline__ bool thread_cell(const Geom& g, int& i, int& j, int& k) {
+    i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    k = DIM == 3 ? 1 + (int)(blockIdx.z * blockDim.z + threadIdx.z) : 0;
+    return i <= g.nx && j <= g.ny && (DIM == 2 || k <= g.nz);
+}
+
+__device__ __forceinline__ int cidx(const Geom& g, int i, int j, int k) {
+    return i + j * g.sx + k * g.sxy;
+}
+
+// Deterministic block + grid reduction of NV FP64 values.  Every thread of every
+// block must call it (out-of-range threads contribute 0).  Each block writes its
+// partial sums to partials[block*NV + q]; the last block to arrive (atomic
+// counter) re-reads all partials in a fixed order and returns true in its thread 0
+// with the totals in tot.  The counter is reset for the next launch.
+template <int NV>
+__device__ __forceinline__ bool reduce_last(double (&v)[NV], double* partials,
+                                            unsigned int* counter, double (&tot)[NV]) {
+    __shared__ double sm[32][NV];
+    __shared__ int am_last;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
+    const int lane = tid & 31, warp = tid >> 5, nwarp = (nthr + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q)
+        for (int off = 16; off > 0; off >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], off);
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sm[warp][q] = v[q];
+    __syncthreads();
+    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < nwarp; ++w) s += sm[w][q];
+            partials[(size_t)bid * NV + q] = s;
+        }
+        __threadfence();
+        unsigned prev = atomicAdd(counter, 1u);
+        am_last = (prev == nblk - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+    for (unsigned b = tid; b < nblk; b += nthr)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] += __ldcg(&partials[(size_t)b * NV + q]);
+#pragma unroll
+    for (int q = 0; q < NV; ++q)
+        for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], off);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sm[warp][q] = acc[q];
+    __syncthreads();
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < nwarp; ++w) s += sm[w][q];
+            tot[q] = s;
+        }
+        *counter = 0u;
+        return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Hierarchy set-up
+
+// Coarse cell solid iff at least half of its 2^DIM children are solid
+// (uaamg_preconditioner_3d.cpp:34-45; uaamg_preconditioner.cpp:43-53).
+template <int DIM>
+__global__ void k_restrict_solid(Geom f, const uint8_t* __restrict__ fs, Geom c,
+                                 uint8_t* __restrict__ cs) {
+    int ic, jc, kc;
+    if (!thread_cell<DIM>(c, ic, jc, kc)) return;
+    const int i_f = 2 * ic - 1, j_f = 2 * jc - 1, k_f = DIM == 3 ? 2 * kc - 1 : 0;
+    int sc = 0;
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+            for (int dk = 0; dk < (DIM == 3 ? 2 : 1); ++dk)
+                sc += fs[cidx(f, i_f + di, j_f + dj, k_f + dk)] != 0;
+    cs[cidx(c, ic, jc, kc)] = (uint8_t)(2 * sc >= (DIM == 3 ? 8 : 4));
+}
+
+// Finest-level couplings from the mask (uaamg_preconditioner_3d.cpp:50-66):
+// cx[c] = h_x^-2 when c and c+e_x are fluid and i < nx.  Channels are zeroed
+// beforehand.  wd (optional) is the Dirichlet-wall diagonal channel.
+template <int DIM, class T>
+__global__ void k_fine_coeffs(Geom g, const uint8_t* __restrict__ s, T* cx, T* cy, T* cz, T* wd,
+                              T idx2, T idy2, T idz2) {
+    int i, j, k;
+    if (!thread_cell<DIM>(g, i, j, k)) return;
+    const int id = cidx(g, i, j, k);
+    if (s[id]) return;
+    if (i < g.nx && !s[id + 1]) cx[id] = idx2;
+    if (j < g.ny && !s[id + g.sx]) cy[id] = idy2;
+    if (DIM == 3 && k < g.nz && !s[id + g.sxy]) cz[id] = idz2;
+    if (wd) {
+        T w = T(0);
+        if (i == 1) w += T(2) * idx2;
+        if (i == g.nx) w += T(2) * idx2;
+        if (j == 1) w += T(2) * idy2;
+        if (j == g.ny) w += T(2) * idy2;
+        if (DIM == 3 && k == 1) w += T(2) * idz2;
+        if (DIM == 3 && k == g.nz) w += T(2) * idz2;
+        wd[id] = w;
+    }
+}
+
+// Galerkin coarse couplings (uaamg_preconditioner_3d.cpp:81-106): the coarse +x
+// coupling is the sum of the fine +x couplings across the shared face, summed in
+// the reference's (dj, dk) order.  The wall channel sums over all children.
+template <int DIM, class T>
+__global__ void k_galerkin(Geom f, const T* __restrict__ fcx, const T* __restrict__ fcy,
+                           const T* __restrict__ fcz, const T* __restrict__ fwd, Geom c,
+                           const uint8_t* __restrict__ cs, T* ccx, T* ccy, T* ccz, T* cwd) {
+    int ic, jc, kc;
+    if (!thread_cell<DIM>(c, ic, jc, kc)) return;
+    const int id = cidx(c, ic, jc, kc);
+    if (cs[id]) return;
+    const int i_f = 2 * ic - 1, j_f = 2 * jc - 1, k_f = DIM == 3 ? 2 * kc - 1 : 0;
+    constexpr int KC = DIM == 3 ? 2 : 1;
+    T sx = T(0), sy = T(0), sz = T(0), sw = T(0);
+    for (int dj = 0; dj < 2; ++dj)
+        for (int dk = 0; dk < KC; ++dk) sx += fcx[cidx(f, i_f + 1, j_f + dj, k_f + dk)];
+    for (int di = 0; di < 2; ++di)
+        for (int dk = 0; dk < KC; ++dk) sy += fcy[cidx(f, i_f + di, j_f + 1, k_f + dk)];
+    if (DIM == 3)
+        for (int di = 0; di < 2; ++di)
+            for (int dj = 0; dj < 2; ++dj) sz += fcz[cidx(f, i_f + di, j_f + dj, k_f + 1)];
+    if (cwd) {
+        for (int di = 0; di < 2; ++di)
+            for (int dj = 0; dj < 2; ++dj)
+                for (int dk = 0; dk < KC; ++dk) sw += fwd[cidx(f, i_f + di, j_f + dj, k_f + dk)];
+        cwd[id] = sw;
+    }
+    ccx[id] = sx;
+    ccy[id] = sy;
+    if (DIM == 3) ccz[id] = sz;
+}
+
+// Level arrays as seen by the V-cycle kernels.
+template <class T>
+struct LevelView {
+    Geom g;
+    const uint8_t* solid;
+    const T* cx;
+    const T* cy;
+    const T* cz;
+    const T* wd;  // nullptr unless Dirichlet walls
+    T* x;
+    const T* b;
+};
+
+// Diagonal in the reference's summation order (uaamg_preconditioner_3d.cpp:72-74).
+template <int DIM, class T>
+__device__ __forceinline__ T diag_at(const LevelView<T>& L, int id) {
+    T d = L.cx[id] + L.cx[id - 1] + L.cy[id] + L.cy[id - L.g.sx];
+    if (DIM == 3) d = d + L.cz[id] + L.cz[id - L.g.sxy];
+    if (L.wd) d = d + L.wd[id];
+    return d;
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle kernels
+
+// One colour of red-black Gauss-Seidel (uaamg_preconditioner_3d.cpp:123-138):
+// x = (b + sum c*x_nb)/diag on cells with (i+j+k)&1 == parity, skipping solid
+// cells and diag < 1e-30.  One thread per x-pair of cells.
+template <int DIM, class T>
+__global__ void k_sweep(LevelView<T> L, int parity, const int* __restrict__ done) {
+    if (done && *done) return;
+    const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    const int k = DIM == 3 ? 1 + (int)(blockIdx.z * blockDim.z + threadIdx.z) : 0;
+    if (j > L.g.ny || (DIM == 3 && k > L.g.nz)) return;
+    const int i0 = (((1 + j + k) & 1) == parity) ? 1 : 2;
+    const int i = i0 + 2 * t;
+    if (i > L.g.nx) return;
+    const int id = cidx(L.g, i, j, k);
+    if (L.solid[id]) return;
+    const T d = diag_at<DIM>(L, id);
+    if (d < T(1e-30)) return;
+    const int sx = L.g.sx, sxy = L.g.sxy;
+    T nb = L.cx[id] * L.x[id + 1] + L.cx[id - 1] * L.x[id - 1]
+         + L.cy[id] * L.x[id + sx] + L.cy[id - sx] * L.x[id - sx];
+    if (DIM == 3) nb = nb + L.cz[id] * L.x[id + sxy] + L.cz[id - sxy] * L.x[id - sxy];
+    L.x[id] = (L.b[id] + nb) / d;
+}
+
+// Residual restriction b_c = sum over fluid children of (b - A x)
+// (uaamg_preconditioner_3d.cpp:144-165).  One thread per coarse cell.
+template <int DIM, class T>
+__global__ void k_restrict(LevelView<T> F, Geom cg, const uint8_t* __restrict__ cs, T* cb,
+                           const int* __restrict__ done) {
+    if (done && *done) return;
+    int ic, jc, kc;
+    if (!thread_cell<DIM>(cg, ic, jc, kc)) return;
+    const int cid = cidx(cg, ic, jc, kc);
+    if (cs[cid]) return;
+    const int i_f = 2 * ic - 1, j_f = 2 * jc - 1, k_f = DIM == 3 ? 2 * kc - 1 : 0;
+    const int sx = F.g.sx, sxy = F.g.sxy;
+    T sum = T(0);
+    for (int di = 0; di < 2; ++di)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int dk = 0; dk < (DIM == 3 ? 2 : 1); ++dk) {
+                const int fid = cidx(F.g, i_f + di, j_f + dj, k_f + dk);
+                if (F.solid[fid]) continue;
+                const T d = diag_at<DIM>(F, fid);
+                T ax = d * F.x[fid] - F.cx[fid] * F.x[fid + 1] - F.cx[fid - 1] * F.x[fid - 1]
+                     - F.cy[fid] * F.x[fid + sx] - F.cy[fid - sx] * F.x[fid - sx];
+                if (DIM == 3) ax = ax - F.cz[fid] * F.x[fid + sxy] - F.cz[fid - sxy] * F.x[fid - sxy];
+                sum += F.b[fid] - ax;
+            }
+    cb[cid] = sum;
+}
+
+// Prolongation x_f += 2 x_c for fluid coarse/fluid fine cells
+// (uaamg_preconditioner_3d.cpp:168-181).
+template <int DIM, class T>
+__global__ void k_prolong(Geom cg, const uint8_t* __restrict__ cs, const T* __restrict__ cx_,
+                          Geom fg, const uint8_t* __restrict__ fs, T* fx,
+                          const int* __restrict__ done) {
+    if (done && *done) return;
+    int ic, jc, kc;
+    if (!thread_cell<DIM>(cg, ic, jc, kc)) return;
+    const int cid = cidx(cg, ic, jc, kc);
+    if (cs[cid]) return;
+    const T val = T(2) * cx_[cid];
+    const int i_f = 2 * ic - 1, j_f = 2 * jc - 1, k_f = DIM == 3 ? 2 * kc - 1 : 0;
+    for (int di = 0; di < 2; ++di)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int dk = 0; dk < (DIM == 3 ? 2 : 1); ++dk) {
+                const int fid = cidx(fg, i_f + di, j_f + dj, k_f + dk);
+                if (!fs[fid]) fx[fid] += val;
+            }
+}
+
+// Coarsest level: 10 x (forward + reverse) RBGS sweeps (uaamg_preconditioner_3d.cpp:
+// 185-186) in ONE block; colours are separated by __syncthreads, which makes the
+// block's global-memory writes visible to all its threads.
+template <int DIM, class T>
+__global__ void k_coarsest(LevelView<T> L, const int* __restrict__ done) {
+    if (done && *done) return;
+    const int nx = L.g.nx, ny = L.g.ny, nzi = DIM == 3 ? L.g.nz : 1;
+    const int ncell = nx * ny * nzi;
+    const int sx = L.g.sx, sxy = L.g.sxy;
+    for (int s = 0; s < 10; ++s)
+        for (int h = 0; h < 4; ++h) {
+            const int parity = (h == 0 || h == 3) ? 1 : 0;  // fwd: 1,0  rev: 0,1
+            for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
+                const int i = 1 + c % nx;
+                const int j = 1 + (c / nx) % ny;
+                const int k = DIM == 3 ? 1 + c / (nx * ny) : 0;
+                if (((i + j + k) & 1) != parity) continue;
+                const int id = cidx(L.g, i, j, k);
+                if (L.solid[id]) continue;
+                const T d = diag_at<DIM>(L, id);
+                if (d < T(1e-30)) continue;
+                T nb = L.cx[id] * L.x[id + 1] + L.cx[id - 1] * L.x[id - 1]
+                     + L.cy[id] * L.x[id + sx] + L.cy[id - sx] * L.x[id - sx];
+                if (DIM == 3) nb = nb + L.cz[id] * L.x[id + sxy] + L.cz[id - sxy] * L.x[id - sxy];
+                L.x[id] = (L.b[id] + nb) / d;
+            }
+            __syncthreads();
+        }
+}
+
+// ---------------------------------------------------------------------------
+// PCG kernels
+
+struct Stencil {
+    double idx2, idy2, idz2, diag;
+    int dirichlet;
+};
+
+// Reference PCG operator (pcg_3d.cpp:38-55, pcg.cpp:47-59): a solid or out-of-domain
+// neighbour reads p_C (Neumann; -p_C for a Dirichlet wall); solid rows are 0.
+template <int DIM, class T>
+__device__ __forceinline__ T apply_A(const Geom& g, const uint8_t* __restrict__ s,
+                                     const T* __restrict__ v, int i, int j, int k, int id,
+                                     T idx2, T idy2, T idz2, T diag, int dirichlet) {
+    const T vc = v[id];
+    const T wall = dirichlet ? -vc : vc;
+    const int sx = g.sx, sxy = g.sxy;
+    const T vL = i > 1 ? (!s[id - 1] ? v[id - 1] : vc) : wall;
+    const T vR = i < g.nx ? (!s[id + 1] ? v[id + 1] : vc) : wall;
+    const T vB = j > 1 ? (!s[id - sx] ? v[id - sx] : vc) : wall;
+    const T vT = j < g.ny ? (!s[id + sx] ? v[id + sx] : vc) : wall;
+    if (DIM == 3) {
+        const T vF = k > 1 ? (!s[id - sxy] ? v[id - sxy] : vc) : wall;
+        const T vK = k < g.nz ? (!s[id + sxy] ? v[id + sxy] : vc) : wall;
+        return diag * vc - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
+    }
+    return diag * vc - (vL + vR) * idx2 - (vB + vT) * idy2;
+}
+
+// Grid-stride walk over the interior in rows of 32 cells along x: a warp owns 32
+// consecutive cells of one row.  Blocks are (32, 8); the grid is capped at a few
+// blocks per SM, which keeps a reduction's last-block combine short.
+template <int DIM, class F>
+__device__ __forceinline__ void for_cells(const Geom& g, F&& f) {
+    const int nxc = (g.nx + 31) >> 5;
+    const int nrows = g.ny * (DIM == 3 ? g.nz : 1);
+    const long long nitems = (long long)nrows * nxc;
+    for (long long it = (long long)blockIdx.x * blockDim.y + threadIdx.y; it < nitems;
+         it += (long long)gridDim.x * blockDim.y) {
+        const int row = (int)(it / nxc);
+        const int ch = (int)(it - (long long)row * nxc);
+        const int i = 1 + (ch << 5) + (int)threadIdx.x;
+        if (i > g.nx) continue;
+        const int j = 1 + row % g.ny;
+        const int k = DIM == 3 ? 1 + row / g.ny : 0;
+        f(i, j, k, cidx(g, i, j, k));
+    }
+}
+
+// Sum and count over fluid interior cells of a FP64 field: cg->sum0, cg->nfluid.
+template <int DIM>
+__global__ void k_sum_count(Geom g, const uint8_t* __restrict__ s, const double* __restrict__ v,
+                            double* partials, CGState* cg, int slot) {
+    double acc[2] = {0.0, 0.0};
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        if (!s[id]) { acc[0] += v[id]; acc[1] += 1.0; }
+    });
+    double tot[2];
+    if (reduce_last<2>(acc, partials, &cg->counter[slot], tot)) {
+        cg->sum0 = tot[0];
+        cg->nfluid = tot[1];
+    }
+}
+
+// b = -(rhs - mean) on fluid interior cells, 0 elsewhere (pcg_3d.cpp:22-36);
+// mean = sum0/nfluid unless Dirichlet.
+template <int DIM>
+__global__ void k_rhs_negate(Geom g, const uint8_t* __restrict__ s, const double* __restrict__ rhs,
+                             double* b, const CGState* cg) {
+    double mean = cg->nfluid > 0.0 ? cg->sum0 / cg->nfluid : 0.0;
+    if (cg->dirichlet) mean = 0.0;
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        b[id] = s[id] ? 0.0 : -(rhs[id] - mean);
+    });
+}
+
+// v -= mean over fluid cells (pcg_3d.cpp:66-77), mean = sum0/nfluid.
+template <int DIM>
+__global__ void k_sub_mean(Geom g, const uint8_t* __restrict__ s, double* v, const CGState* cg) {
+    if (cg->dirichlet) return;
+    const double mean = cg->nfluid > 0.0 ? cg->sum0 / cg->nfluid : 0.0;
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        if (!s[id]) v[id] -= mean;
+    });
+}
+
+// r = b - A x (FP64), copied into the working residual rw (type T), with
+// ||r||^2 reduced.  mode 0: initial residual (sets r0, and tol_abs = tol or
+// tol*||b|| for the relative rule, ||b|| being the RHS norm, not ||r0||);
+// mode 1: residual replacement (mixed); mode 2: exit diagnostics only;
+// mode 3: plain b <- b - A x for a warm start (rw may alias b: each cell reads
+// its own b before writing it).  When x == nullptr the residual is b itself.
+template <int DIM, class T>
+__global__ void k_true_residual(Geom g, const uint8_t* __restrict__ s, const double* b,
+                                const double* __restrict__ x, T* rw, Stencil st, double* partials,
+                                CGState* cg, int slot, int mode, double tol, int tol_mode) {
+    if (mode == 1) {
+        if (cg->done) return;
+        if (!(cg->cand || (cg->replace_every > 0 && cg->iter > 0 &&
+                           cg->iter % cg->replace_every == 0)))
+            return;
+    }
+    double acc[1] = {0.0};
+    for_cells<DIM>(g, [&](int i, int j, int k, int id) {
+        if (!s[id]) {
+            double r = b[id];
+            if (x) r = r - apply_A<DIM, double>(g, s, x, i, j, k, id, st.idx2, st.idy2, st.idz2,
+                                                st.diag, st.dirichlet);
+            if (rw) rw[id] = (T)r;
+            acc[0] += r * r;
+        } else if (rw) {
+            rw[id] = T(0);
+        }
+    });
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[slot], tot)) {
+        const double rr = tot[0];
+        cg->rr_true = rr;
+        if (mode == 0) {
+            cg->r0 = sqrt(rr);
+            cg->rr = rr;
+            cg->tol_abs = tol_mode ? tol * cg->bnorm : tol;
+            if (rr == 0.0) { cg->status = CG_CONVERGED; cg->done = 1; }  // b = 0: x = 0 exactly
+        } else if (mode == 1) {
+            cg->rr = rr;
+            cg->replacements += 1;
+            if (cg->cand) {
+                cg->cand = 0;
+                if (sqrt(rr) < cg->tol_abs) { cg->status = CG_CONVERGED; cg->done = 1; }
+            }
+            if (!(rr == rr)) { cg->status = CG_NAN; cg->done = 1; }
+        }
+    }
+}
+
+// ||b||^2 over fluid cells -> cg->bnorm (FP64).
+template <int DIM>
+__global__ void k_norm(Geom g, const uint8_t* __restrict__ s, const double* __restrict__ b,
+                       double* partials, CGState* cg, int slot) {
+    double acc[1] = {0.0};
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        if (!s[id]) acc[0] += b[id] * b[id];
+    });
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[slot], tot)) cg->bnorm = sqrt(tot[0]);
+}
+
+// New search direction fused with the operator: p = (z - m) + beta p_old on fluid
+// cells (pcg_3d.cpp:115-122 with the mean projection of :113), Ap = A p with the
+// neighbours' new p formed on the fly from z and p_old, and p.Ap reduced; the
+// last block sets alpha = rz_old / p.Ap or stops on breakdown (pcg_3d.cpp:94-99).
+// p_old and p_new are distinct buffers (ping-pong), so no thread reads a p value
+// another thread is rewriting.
+template <int DIM, class T>
+__global__ void k_pmatvec(Geom g, const uint8_t* __restrict__ s, const T* __restrict__ z,
+                          const T* __restrict__ pold, T* __restrict__ pnew, T* __restrict__ ap,
+                          Stencil st, double* partials, CGState* cg) {
+    if (cg->done) return;
+    const T m = (T)cg->mean_z, beta = (T)cg->beta;
+    const T idx2 = (T)st.idx2, idy2 = (T)st.idy2, idz2 = (T)st.idz2, diag = (T)st.diag;
+    const int sx = g.sx, sxy = g.sxy;
+    double acc[1] = {0.0};
+    for_cells<DIM>(g, [&](int i, int j, int k, int id) {
+        if (s[id]) {
+            ap[id] = T(0);
+            pnew[id] = T(0);
+            return;
+        }
+        auto pv = [&](int q) -> T { return (z[q] - m) + beta * pold[q]; };
+        const T pc = pv(id);
+        const T wall = st.dirichlet ? -pc : pc;
+        const T vL = i > 1 ? (!s[id - 1] ? pv(id - 1) : pc) : wall;
+        const T vR = i < g.nx ? (!s[id + 1] ? pv(id + 1) : pc) : wall;
+        const T vB = j > 1 ? (!s[id - sx] ? pv(id - sx) : pc) : wall;
+        const T vT = j < g.ny ? (!s[id + sx] ? pv(id + sx) : pc) : wall;
+        T a;
+        if (DIM == 3) {
+            const T vF = k > 1 ? (!s[id - sxy] ? pv(id - sxy) : pc) : wall;
+            const T vK = k < g.nz ? (!s[id + sxy] ? pv(id + sxy) : pc) : wall;
+            a = diag * pc - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
+        } else {
+            a = diag * pc - (vL + vR) * idx2 - (vB + vT) * idy2;
+        }
+        pnew[id] = pc;
+        ap[id] = a;
+        acc[0] += (double)pc * (double)a;
+    });
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
+        const double pap = tot[0];
+        cg->pap = pap;
+        if (!(pap == pap)) { cg->status = CG_NAN; cg->done = 1; }
+        else if (pap < cg->breakdown) { cg->status = CG_BREAKDOWN; cg->done = 1; }
+        else cg->alpha = cg->rz_old / pap;
+    }
+}
+
+// x += alpha p, r -= alpha Ap, then r.r; the last block applies the stopping rule
+// sqrt(r.r) < tol_abs (pcg_3d.cpp:99-110).  p and Ap are 0 on solid cells and r
+// starts at 0 there, so no mask is read.  In mixed mode (replace_every > 0)
+// meeting the rule only marks a candidate that the FP64 residual replacement
+// confirms.
+template <int DIM, class T>
+__global__ void k_update(Geom g, T* x, T* r, const T* __restrict__ p, const T* __restrict__ ap,
+                         double* partials, CGState* cg, double* hist) {
+    if (cg->done) return;
+    const T alpha = (T)cg->alpha;
+    double acc[1] = {0.0};
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        x[id] += alpha * p[id];
+        const T rn = r[id] - alpha * ap[id];
+        r[id] = rn;
+        acc[0] += (double)rn * (double)rn;
+    });
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[1], tot)) {
+        const double rr = tot[0];
+        cg->rr = rr;
+        cg->iter += 1;
+        if (hist) {
+            if (cg->iter == 1) hist[0] = cg->r0;
+            hist[cg->iter] = sqrt(rr);
+        }
+        if (!(rr == rr)) { cg->status = CG_NAN; cg->done = 1; }
+        else if (sqrt(rr) < cg->tol_abs) {
+            if (cg->replace_every > 0) cg->cand = 1;
+            else { cg->status = CG_CONVERGED; cg->done = 1; }
+        } else if (cg->iter >= cg->max_iter && cg->replace_every == 0) {
+            cg->status = CG_MAXITER; cg->done = 1;
+        }
+    }
+}
+
+// Mixed mode: after a replacement that did not converge, stop at max_iter.
+__global__ void k_maxiter_check(CGState* cg) {
+    if (cg->done) return;
+    if (cg->iter >= cg->max_iter && !cg->cand) { cg->status = CG_MAXITER; cg->done = 1; }
+}
+
+// Null-space projection of z and the new r.z (pcg_3d.cpp:112-123), given the
+// fluid sums of z, r*z and r: with m = mean_fluid(z), r.(z - m) = r.z - m*sum(r).
+// Sets beta = rz/rz_old (0 when forming p0) and rz_old = rz.
+__device__ __forceinline__ void finish_zdot(CGState* cg, const double (&tot)[3]) {
+    double m = 0.0, rz = tot[1];
+    if (!cg->dirichlet) {
+        m = cg->nfluid > 0.0 ? tot[0] / cg->nfluid : 0.0;
+        rz = tot[1] - m * tot[2];
+    }
+    cg->mean_z = m;
+    cg->beta = cg->init ? 0.0 : rz / cg->rz_old;
+    cg->rz_old = rz;
+    cg->init = 0;
+    if (!(rz == rz)) { cg->status = CG_NAN; cg->done = 1; }
+}
+
+// The sums above as a separate pass (used with the per-level sweep V-cycle; the
+// fused V-cycle computes them in its last kernel).
+template <int DIM, class T>
+__global__ void k_zdot(Geom g, const uint8_t* __restrict__ s, const T* __restrict__ r,
+                       const T* __restrict__ z, double* partials, CGState* cg) {
+    if (cg->done) return;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        if (!s[id]) {
+            const double zv = (double)z[id], rv = (double)r[id];
+            acc[0] += zv;
+            acc[1] += rv * zv;
+            acc[2] += rv;
+        }
+    });
+    double tot[3];
+    if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
+}
+
+// Mixed mode: fold the FP32 correction into the FP64 solution, x_hi += x_lo,
+// x_lo = 0, when a residual replacement is due (or unconditionally at exit).
+template <int DIM, class T>
+__global__ void k_fold(Geom g, const uint8_t* __restrict__ s, double* xhi, T* xlo,
+                       const CGState* cg, int force) {
+    if (!force) {
+        if (cg->done) return;
+        if (!(cg->cand || (cg->replace_every > 0 && cg->iter > 0 &&
+                           cg->iter % cg->replace_every == 0)))
+            return;
+    }
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        if (s[id]) return;
+        xhi[id] += (double)xlo[id];
+        xlo[id] = T(0);
+    });
+}
+
+// Output: out += x on fluid cells.  Callers keep the incoming value in out, so a
+// cold start accumulates into it exactly like PCG::solve accumulates into g.p
+// (pcg_3d.cpp:105), and a warm start (whose residual already accounts for it)
+// returns x_in + correction.
+template <int DIM, class T>
+__global__ void k_output(Geom g, const uint8_t* __restrict__ s, const T* __restrict__ x,
+                         double* out) {
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        if (!s[id]) out[id] = out[id] + (double)x[id];
+    });
+}
+
+// FP64 <-> T conversions on the padded arrays.
+template <class T>
+__global__ void k_cast_from_f64(const double* __restrict__ a, T* b, int n) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) b[t] = (T)a[t];
+}
+template <class T>
+__global__ void k_cast_to_f64(const T* __restrict__ a, double* b, int n) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) b[t] = (double)a[t];
+}
+
+}  // namespace
+}  // namespace uaamg

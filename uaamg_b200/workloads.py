@@ -1,0 +1,96 @@
+"""Seeded synthetic workloads (ctypes over libuaamg_workloads.so, host code).
+
+Every generator returns padded numpy arrays in the reference's memory order
+(C-order shape (nz+2, ny+2, nx+2) / (ny+2, nx+2)).  The named workloads:
+
+* ``spheres_256``: 256^3, h = 1/256, 32 solid spheres with radius U[8, 24] cells,
+  RHS = N(0,1) noise blurred with a sigma = 4 cell Gaussian (+-16 taps), zero at
+  solids, zero fluid mean; seed 20260303.
+* ``obstacle_2d``: 2048 x 1024, dx = 1e-3, dy = 1.5e-3, disk of radius 0.05*Ly at
+  (0.25 Lx, 0.5 Ly); u = 1 + Fourier modes |k| <= 16 with N(0,1)/|k|^2
+  amplitudes, v = modes; RHS = div(u)/dt, dt = 1e-3; seed 20260202.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(HERE, "libuaamg_workloads.so")
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            from . import build as _b
+            _b.build_workloads()
+        L = C.CDLL(_LIB)
+        p, i, d, u64 = C.c_void_p, C.c_int, C.c_double, C.c_uint64
+        L.wl_spheres_3d.argtypes = [i, i, i, i, d, d, u64, d, i, p, p]
+        L.wl_spheres_3d.restype = C.c_long
+        L.wl_boxes.argtypes = [i, i, i, i, d, u64, d, i, p, p]
+        L.wl_boxes.restype = C.c_long
+        L.wl_obstacle_flow_2d.argtypes = [i, i, d, d, d, i, u64, d, p, p, p, p]
+        L.wl_obstacle_flow_2d.restype = C.c_long
+        L.wl_obstacle_flow_3d.argtypes = [i, i, i, d, d, d, d, i, u64, d, p, p, p, p, p]
+        L.wl_obstacle_flow_3d.restype = C.c_long
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def spheres_3d(nx, ny, nz, nspheres=32, rmin=8.0, rmax=24.0, seed=20260303, sigma=4.0,
+               trunc=16):
+    solid = np.zeros((nz + 2, ny + 2, nx + 2), np.uint8)
+    rhs = np.zeros((nz + 2, ny + 2, nx + 2))
+    _load().wl_spheres_3d(nx, ny, nz, nspheres, rmin, rmax, seed, sigma, trunc, _p(solid), _p(rhs))
+    return solid, rhs
+
+
+def boxes(dim, nx, ny, nz, coverage, seed, sigma=4.0, trunc=16):
+    shape = (nz + 2, ny + 2, nx + 2) if dim == 3 else (ny + 2, nx + 2)
+    solid = np.zeros(shape, np.uint8)
+    rhs = np.zeros(shape)
+    _load().wl_boxes(dim, nx, ny, nz if dim == 3 else 0, coverage, seed, sigma, trunc, _p(solid),
+                     _p(rhs))
+    return solid, rhs
+
+
+def obstacle_flow_2d(nx, ny, dx, dy, dt=1e-3, kmax=16, seed=20260202, t=0.0):
+    solid = np.zeros((ny + 2, nx + 2), np.uint8)
+    u = np.zeros((ny + 2, nx + 1))
+    v = np.zeros((ny + 1, nx + 2))
+    rhs = np.zeros((ny + 2, nx + 2))
+    _load().wl_obstacle_flow_2d(nx, ny, dx, dy, dt, kmax, seed, t, _p(solid), _p(u), _p(v), _p(rhs))
+    return solid, u, v, rhs
+
+
+def obstacle_flow_3d(nx, ny, nz, dx, dy, dz, dt=1e-3, kmax=8, seed=20260505, t=0.0):
+    solid = np.zeros((nz + 2, ny + 2, nx + 2), np.uint8)
+    u = np.zeros((nz + 2, ny + 2, nx + 1))
+    v = np.zeros((nz + 2, ny + 1, nx + 2))
+    w = np.zeros((nz + 1, ny + 2, nx + 2))
+    rhs = np.zeros((nz + 2, ny + 2, nx + 2))
+    _load().wl_obstacle_flow_3d(nx, ny, nz, dx, dy, dz, dt, kmax, seed, t, _p(solid), _p(u),
+                                _p(v), _p(w), _p(rhs))
+    return solid, u, v, w, rhs
+
+
+def spheres_256():
+    """The 256^3 mixed-precision workload: (solid, rhs, h)."""
+    s, r = spheres_3d(256, 256, 256)
+    return s, r, 1.0 / 256
+
+
+def obstacle_2d():
+    """The 2048 x 1024 projection workload: (solid, u, v, rhs, dx, dy, dt)."""
+    dx, dy, dt = 1.0e-3, 1.5e-3, 1.0e-3
+    s, u, v, r = obstacle_flow_2d(2048, 1024, dx, dy, dt)
+    return s, u, v, r, dx, dy, dt
