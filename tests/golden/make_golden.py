@@ -102,12 +102,13 @@ def cases():
         c = dict(name=name, kind=kind, solid=s, r=r, dx=sp[0], dy=sp[1], dz=sp[2])
         if kind == "pcg":
             # A random mask leaves isolated fluid pockets, so a random RHS has no
-            # solution; rhs = -A x_true is always compatible (lap(p) = rhs).
+            # solution; rhs = -A x_true is always compatible (lap(p) = rhs).  The
+            # solution is still defined only up to a constant per pocket, so these
+            # cases compare a fixed number of iterations (tol = 0), as the
+            # reference's own GPU tests do (test_cuda_uaamg_3d.cu:68-94).
             x_true = np.where(_interior(shape) & (s == 0), rng.standard_normal(shape), 0.0)
             c["r"] = -O.matvec(s, x_true, sp[0], sp[1], sp[2])
-            b = O.pcg_rhs(s, c["r"])
-            bn = float(np.sqrt((b[s == 0] ** 2).sum()))
-            c.update(max_iter=300, tol=1e-9 * bn)
+            c.update(max_iter=25, tol=0.0)
         out.append(c)
     # --- pressure projection --------------------------------------------------
     nx, ny, dx, dy, dt = 48, 24, 1.0 / 48, 0.5 / 24, 1e-2
