@@ -173,6 +173,24 @@ UAAMG_API uaamg_status uaamg_profile_solve(uaamg_handle* h, const double* d_rhs,
                                            const uaamg_options* opts, uaamg_stats* stats,
                                            uaamg_kernel_time* out, int cap, int* count);
 
+/* Allocation-free residual check, for callers that cannot call cudaMalloc:
+ * code running during CUDA-graph stream capture, inside host callbacks or
+ * allocator hooks, or in applications that own every device allocation.  No
+ * handle, no allocation: d_out[0] = ||b - A p|| and d_out[1] = ||b|| (FP64,
+ * fluid interior cells), b = -(rhs - mean_fluid(rhs)) as PCG::solve forms it and
+ * A the PCG operator with Neumann walls and solids.  All arrays are DEVICE
+ * arrays in the padded reference layout; d_out holds 2 doubles.  Work is queued
+ * on `stream` (a cudaStream_t) and the call returns without waiting.
+ * Scratch is a 16.4 KiB file-scope device array (held by every GPU that loads the
+ * library until exit); grids of 2^31 padded cells or more are rejected.  The
+ * first call on a device looks up that array and should come before any stream
+ * capture; calls that overlap on the GPU share the array and race.
+ * This entry point has no counterpart in the reference. */
+UAAMG_API uaamg_status uaamg_residual_noalloc(int dim, int nx, int ny, int nz, double dx,
+                                              double dy, double dz, const uint8_t* d_solid,
+                                              const double* d_rhs, const double* d_p,
+                                              double* d_out, void* stream);
+
 /* Device memory held by the handle, bytes. */
 UAAMG_API uaamg_status uaamg_device_bytes(uaamg_handle* h, size_t* bytes);
 

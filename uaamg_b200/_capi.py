@@ -32,7 +32,7 @@ EXPORTS = [
     "uaamg_set_dirichlet_walls", "uaamg_solve", "uaamg_solve_device", "uaamg_precond_apply",
     "uaamg_residual_history", "uaamg_num_levels", "uaamg_level_dims", "uaamg_copy_level",
     "uaamg_device_bytes", "uaamg_last_error", "uaamg_status_string", "uaamg_profile_solve",
-    "uaamg_set_vcycle_kernels",
+    "uaamg_set_vcycle_kernels", "uaamg_residual_noalloc",
 ]
 
 
@@ -107,6 +107,7 @@ def load(path: str | None = None):
     L.uaamg_set_problem_device.argtypes = [p, i, i, i, i, d, d, d, p]
     L.uaamg_set_dirichlet_walls.argtypes = [p, i]
     L.uaamg_set_vcycle_kernels.argtypes = [p, i]
+    L.uaamg_residual_noalloc.argtypes = [i, i, i, i, d, d, d, p, p, p, p, p]
     L.uaamg_solve.argtypes = [p, p, p, C.POINTER(Options), C.POINTER(Stats)]
     L.uaamg_solve_device.argtypes = [p, p, p, C.POINTER(Options), C.POINTER(Stats)]
     L.uaamg_precond_apply.argtypes = [p, i, p, p]

@@ -28,6 +28,7 @@ UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_f32.cu", []),
     ("api.cpp", ["-x", "cu"]),
+    ("noalloc.cu", ["-fmad=false"]),
 ]
 HEADERS = ["common.cuh", "kernels.cuh", "engine.cuh", "engine.h"]
 
