@@ -105,10 +105,13 @@ def cases():
             # solution; rhs = -A x_true is always compatible (lap(p) = rhs).  The
             # solution is still defined only up to a constant per pocket, so these
             # cases compare a fixed number of iterations (tol = 0), as the
-            # reference's own GPU tests do (test_cuda_uaamg_3d.cu:68-94).
+            # reference's own GPU tests do (test_cuda_uaamg_3d.cu:68-94).  On such
+            # masks the reference's own result moves by ~1e-7 after 25 iterations
+            # when its RHS is perturbed by 1e-15, so 10 iterations are compared,
+            # where it is stable to ~1e-11.
             x_true = np.where(_interior(shape) & (s == 0), rng.standard_normal(shape), 0.0)
             c["r"] = -O.matvec(s, x_true, sp[0], sp[1], sp[2])
-            c.update(max_iter=25, tol=0.0)
+            c.update(max_iter=10, tol=0.0)
         out.append(c)
     # --- pressure projection --------------------------------------------------
     nx, ny, dx, dy, dt = 48, 24, 1.0 / 48, 0.5 / 24, 1e-2
