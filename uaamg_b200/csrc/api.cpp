@@ -158,10 +158,13 @@ uaamg_status solve_dev(uaamg_handle* h, const double* d_rhs, double* d_p, const 
     a.project_mean = opts.project_mean;
     a.precond = opts.preconditioner;
     a.hist = h->d_hist;
+    a.ref_solid = h->d_solid;
     uaamg::SolveResult r;
     std::memset(&r, 0, sizeof(r));
     int e = eng->solve(a, &r);
     if (e != uaamg::E_OK) return map_engine(h, e, "solve");
+    if (eng->timed_out())
+        return fail(h, UAAMG_TIMEOUT, "solve: a kernel gave up waiting for its tile loads");
     h->last_iters = r.iterations;
     uaamg_status out;
     switch (r.status) {
@@ -302,9 +305,14 @@ uaamg_status uaamg_precond_apply(uaamg_handle* h, int precision, const double* r
     if (s != UAAMG_OK) return s;
     const size_t bytes = h->n * sizeof(double);
     cudaError_t e = cudaMemcpyAsync(h->d_rhs, r, bytes, cudaMemcpyHostToDevice, h->stream);
+    // z is written on interior cells only (UAAMGPreconditioner3D::apply,
+    // uaamg_preconditioner_3d.cpp:225-228); its ghost cells come back as 0
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_p, 0, bytes, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "upload");
     int ee = eng->precond_apply(h->d_rhs, h->d_p);
     if (ee != uaamg::E_OK) return map_engine(h, ee, "precond_apply");
+    if (eng->timed_out())
+        return fail(h, UAAMG_TIMEOUT, "precond_apply: a kernel gave up waiting for its tile loads");
     e = cudaMemcpyAsync(z, h->d_p, bytes, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "download");

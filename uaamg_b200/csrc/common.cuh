@@ -19,11 +19,25 @@ struct Geom {
     int n;           // padded cell count
 };
 
+// The reference's layout: row pitch nx+2.
 inline Geom make_geom(int dim, int nx, int ny, int nz) {
     Geom g;
     g.nx = nx; g.ny = ny; g.nz = dim == 3 ? nz : 0;
     g.sx = nx + 2;
     g.sxy = (nx + 2) * (ny + 2);
+    g.n = dim == 3 ? g.sxy * (nz + 2) : g.sxy;
+    return g;
+}
+
+// The engines' internal layout: the same ghost-padded i-fastest order with the row
+// pitch rounded up to a multiple of 16 cells, so every row of every array starts
+// on a 16-byte boundary (a tensor-map requirement for TMA, and 128-bit loads).
+// Columns nx+2 .. sx-1 are padding and stay 0.
+constexpr int kPitchAlign = 16;
+inline Geom make_geom_pitched(int dim, int nx, int ny, int nz) {
+    Geom g = make_geom(dim, nx, ny, nz);
+    g.sx = (nx + 2 + kPitchAlign - 1) / kPitchAlign * kPitchAlign;
+    g.sxy = g.sx * (ny + 2);
     g.n = dim == 3 ? g.sxy * (nz + 2) : g.sxy;
     return g;
 }

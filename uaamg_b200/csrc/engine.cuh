@@ -9,12 +9,18 @@
 //               here instead of once per apply
 //   V-cycle     vCycle (uaamg_preconditioner_3d.cpp:183-196), iterative
 //   PCG         PCG3D::solve (pcg_3d.cpp:18-125), every scalar device-resident
+//
+// Layout: every level array uses the pitched layout (common.cuh,
+// make_geom_pitched); the caller's arrays use the reference layout and are
+// converted on the way in (rhs, warm-start p, preconditioner input) and out.
 #pragma once
+#include <utility>
 #include <vector>
 
 #include "engine.h"
 #include "fused.cuh"
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace uaamg {
 namespace {
@@ -24,8 +30,10 @@ struct LevelBuf {
     Geom g;
     double hx, hy, hz;
     uint8_t* solid = nullptr;
-    T *cx = nullptr, *cy = nullptr, *cz = nullptr, *wd = nullptr;
+    T *cx = nullptr, *cy = nullptr, *cz = nullptr, *wd = nullptr, *dg = nullptr, *rdg = nullptr;
     T *x = nullptr, *b = nullptr;  // level >= 1 only (level 0 uses the CG's r and z)
+    uint8_t* code = nullptr;       // cell codes (fused.cuh)
+    CUtensorMap map_b, map_c;      // TMA maps of b and the codes for the V-cycle tiles
 };
 
 // Kernel classes for the in-situ per-kernel timing (uaamg_profile_solve).
@@ -44,16 +52,6 @@ struct KTag {
     double bytes;  // algorithmic (compulsory) bytes of this launch
 };
 
-#define UAAMG_LAUNCH(tag, kern, grid, block, ...)                         \
-    do {                                                                  \
-        const KTag tg_ = (tag);                                           \
-        cudaEvent_t e0_ = nullptr, e1_ = nullptr;                         \
-        if (prof_on_) prof_begin(tg_, &e0_, &e1_);                        \
-        kern<<<(grid), (block), 0, st_>>>(__VA_ARGS__);                   \
-        if (prof_on_) cudaEventRecord(e1_, st_);                          \
-        ++launches_;                                                      \
-    } while (0)
-
 #define UAAMG_LAUNCH_SMEM(tag, kern, grid, block, smem, ...)              \
     do {                                                                  \
         const KTag tg_ = (tag);                                           \
@@ -63,8 +61,10 @@ struct KTag {
         if (prof_on_) cudaEventRecord(e1_, st_);                          \
         ++launches_;                                                      \
     } while (0)
+#define UAAMG_LAUNCH(tag, kern, grid, block, ...) \
+    UAAMG_LAUNCH_SMEM(tag, kern, grid, block, 0, __VA_ARGS__)
 
-// Fused V-cycle tile shapes (cells per block tile; 256 threads per block).
+// Tile shapes (cells per block tile; 256 threads per block).
 template <int DIM> struct VTile;
 template <> struct VTile<3> { static constexpr int X = 32, Y = 8, Z = 8; };
 template <> struct VTile<2> { static constexpr int X = 64, Y = 32, Z = 1; };
@@ -73,7 +73,10 @@ template <class T>
 class EngineT final : public Engine {
 public:
     explicit EngineT(bool mixed) : mixed_(mixed) {}
-    ~EngineT() override { release(); }
+    ~EngineT() override {
+        release();
+        if (cap_) cudaStreamDestroy(cap_);
+    }
 
     int set_problem(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
                     const uint8_t* d_solid, int dirichlet) override {
@@ -90,20 +93,8 @@ public:
     int precond_apply(const double* d_r, double* d_z) override {
         if (lv_.empty()) return E_NOPROB;
         launches_ = 0;
-        const int n = lv_[0].g.n;
-        const int tb = 256, nb = (n + tb - 1) / tb;
-        const T* r = nullptr;
-        T* z = nullptr;
-        if (sizeof(T) == sizeof(double)) {
-            r = reinterpret_cast<const T*>(d_r);
-            z = reinterpret_cast<T*>(d_z);
-        } else {
-            UAAMG_LAUNCH((KTag{K_CAST, 0, 12.0 * n}), k_cast_from_f64<T>, nb, tb, d_r, r_, n);
-            r = r_;
-            z = z_;
-        }
-        if (dim_ == 3) vcycle<3>(r, z, nullptr, false); else vcycle<2>(r, z, nullptr, false);
-        if (sizeof(T) != sizeof(double)) UAAMG_LAUNCH((KTag{K_CAST, 0, 12.0 * n}), k_cast_to_f64<T>, nb, tb, z_, d_z, n);
+        cudaMemsetAsync(err_, 0, sizeof(int), st_);
+        if (dim_ == 3) precond_impl<3>(d_r, d_z); else precond_impl<2>(d_r, d_z);
         return sync_check();
     }
 
@@ -130,22 +121,37 @@ public:
         *nx = lv_[l].g.nx; *ny = lv_[l].g.ny; *nz = lv_[l].g.nz;
     }
 
+    // Host copies in the reference layout of level l (row pitch nx_l + 2).
     int copy_level(int l, uint8_t* solid, double* cx, double* cy, double* cz) override {
         if (l < 0 || l >= (int)lv_.size()) return E_ARG;
         const LevelBuf<T>& L = lv_[l];
-        const size_t n = (size_t)L.g.n;
+        const Geom g = L.g;
+        const Geom gr = make_geom(dim_, g.nx, g.ny, g.nz);
         if (cudaStreamSynchronize(st_) != cudaSuccess) return E_CUDA;
-        if (solid && cudaMemcpy(solid, L.solid, n, cudaMemcpyDeviceToHost) != cudaSuccess)
-            return E_CUDA;
-        std::vector<T> tmp(n);
+        const int nzi = dim_ == 3 ? g.nz + 2 : 1;
+        auto depitch = [&](auto* dst, const auto* src) {
+            for (int k = 0; k < nzi; ++k)
+                for (int j = 0; j < g.ny + 2; ++j)
+                    for (int i = 0; i < g.nx + 2; ++i)
+                        dst[i + j * gr.sx + k * gr.sxy] = src[i + j * g.sx + k * g.sxy];
+        };
+        if (solid) {
+            std::vector<uint8_t> tmp(g.n);
+            if (cudaMemcpy(tmp.data(), L.solid, g.n, cudaMemcpyDeviceToHost) != cudaSuccess)
+                return E_CUDA;
+            depitch(solid, tmp.data());
+        }
+        std::vector<T> tmp(g.n);
+        std::vector<double> tmpd(g.n);
         const T* src[3] = {L.cx, L.cy, L.cz};
         double* dst[3] = {cx, cy, cz};
         for (int q = 0; q < 3; ++q) {
             if (!dst[q]) continue;
-            if (!src[q]) { for (size_t c = 0; c < n; ++c) dst[q][c] = 0.0; continue; }
-            if (cudaMemcpy(tmp.data(), src[q], n * sizeof(T), cudaMemcpyDeviceToHost) != cudaSuccess)
+            if (!src[q]) { for (int c = 0; c < gr.n; ++c) dst[q][c] = 0.0; continue; }
+            if (cudaMemcpy(tmp.data(), src[q], g.n * sizeof(T), cudaMemcpyDeviceToHost) != cudaSuccess)
                 return E_CUDA;
-            for (size_t c = 0; c < n; ++c) dst[q][c] = (double)tmp[c];
+            for (int c = 0; c < g.n; ++c) tmpd[c] = (double)tmp[c];
+            depitch(dst[q], tmpd.data());
         }
         return E_OK;
     }
@@ -153,8 +159,8 @@ public:
     void set_stream(cudaStream_t s) override { st_ = s; }
     size_t device_bytes() const override { return bytes_; }
     long launches() const override { return launches_; }
-
     void set_vcycle_sweeps(bool on) override { sweeps_ = on; }
+    void set_graphs(bool on) override { graphs_ = on; }
 
     void set_profiling(bool on) override {
         prof_on_ = on;
@@ -189,23 +195,23 @@ public:
         return E_OK;
     }
 
+    int timed_out() override {
+        int v = 0;
+        if (!err_) return 0;
+        if (cudaMemcpy(&v, err_, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+        return v;
+    }
+
 private:
     bool mixed_;
     int dim_ = 0, dirichlet_ = 0;
     double dx_ = 1, dy_ = 1, dz_ = 1;
+    Geom gref_;                      // the caller's (reference) layout of level 0
     std::vector<LevelBuf<T>> lv_;
     T *r_ = nullptr, *z_ = nullptr, *p_ = nullptr, *p2_ = nullptr, *ap_ = nullptr, *xlo_ = nullptr;
-    int num_sms_ = 148;
-    bool sweeps_ = false;  // V-cycle as per-colour sweeps (cross-check) instead of fused
-    int max_reduce_blocks() const { return 4 * num_sms_; }
-    // grid of the row-walk kernels (kernels.cuh for_cells): capped at 4 blocks per SM
-    dim3 vec_grid(const Geom& g) const {
-        const long long items = (long long)g.ny * (g.nz ? g.nz : 1) * ((g.nx + 31) / 32);
-        long long nb = (items + 7) / 8;
-        if (nb > max_reduce_blocks()) nb = max_reduce_blocks();
-        return dim3((unsigned)(nb < 1 ? 1 : nb));
-    }
     double *b64_ = nullptr, *xd_ = nullptr, *partials_ = nullptr;
+    int* err_ = nullptr;             // set by a kernel whose TMA wait gave up
+    CUtensorMap map_z_, map_p_, map_p2_, map_c1_;  // search-direction kernel tiles
     CGState* cg_ = nullptr;
     CGState* cg_host_ = nullptr;  // pinned
     int* flag_host_ = nullptr;    // pinned, 2 slots
@@ -214,11 +220,29 @@ private:
     std::vector<void*> allocs_;
     size_t bytes_ = 0;
     long launches_ = 0;
+    int num_sms_ = 148;
+    bool sweeps_ = false;  // V-cycle as per-colour sweeps (cross-check) instead of fused
+    bool graphs_ = true;   // replay the PCG step as a CUDA graph
+    cudaStream_t cap_ = nullptr;      // capture stream
+    cudaGraphExec_t gexec_ = nullptr; // two PCG iterations
+    long long gkey_ = -1;
+    const double* ghist_ = nullptr;
+    long glaunches_ = 0;              // kernels in one graph replay
     // in-situ per-launch timing (set_profiling)
     bool prof_on_ = false;
     int prof_count_ = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev_;
     std::vector<KTag> prof_tag_;
+
+    int max_reduce_blocks() const { return 4 * num_sms_; }
+
+    // grid of the row-walk kernels (kernels.cuh for_cells): capped at 4 blocks per SM
+    dim3 vec_grid(const Geom& g) const {
+        const long long items = (long long)g.ny * (g.nz ? g.nz : 1) * ((g.nx + 31) / 32);
+        long long nb = (items + 7) / 8;
+        if (nb > max_reduce_blocks()) nb = max_reduce_blocks();
+        return dim3((unsigned)(nb < 1 ? 1 : nb));
+    }
 
     void prof_begin(const KTag& t, cudaEvent_t* e0, cudaEvent_t* e1) {
         if (prof_count_ == (int)prof_ev_.size()) {
@@ -261,12 +285,16 @@ private:
         bytes_ = 0;
         r_ = z_ = p_ = p2_ = ap_ = xlo_ = nullptr;
         b64_ = xd_ = partials_ = nullptr;
+        err_ = nullptr;
         cg_ = nullptr;
         if (cg_host_) { cudaFreeHost(cg_host_); cg_host_ = nullptr; }
         if (flag_host_) { cudaFreeHost(flag_host_); flag_host_ = nullptr; }
         for (auto& e : ev_) if (e) { cudaEventDestroy(e); e = nullptr; }
         for (auto& pr : prof_ev_) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
         prof_ev_.clear();
+        if (gexec_) { cudaGraphExecDestroy(gexec_); gexec_ = nullptr; }
+        gkey_ = -1;
+        ghist_ = nullptr;
         prof_tag_.clear();
         prof_count_ = 0;
     }
@@ -279,22 +307,35 @@ private:
 
     template <int DIM>
     int build(int nx, int ny, int nz, const uint8_t* d_solid) {
+        constexpr int TX = VTile<DIM>::X, TY = VTile<DIM>::Y, TZ = VTile<DIM>::Z;
+        using VP = VPlan<DIM, T, TX, TY, TZ>;
+        using PP = PPlan<DIM, T, TX, TY, TZ>;
+        gref_ = make_geom(DIM, nx, ny, nz);
+        {
+            const Geom gp = make_geom_pitched(DIM, nx, ny, nz);
+            if ((long long)gp.sx * (ny + 2) * (DIM == 3 ? nz + 2 : 1) >= (1LL << 31)) return E_ARG;
+        }
         double hx = dx_, hy = dy_, hz = dz_;
         while (nx >= 2 && ny >= 2 && (DIM == 2 || nz >= 2)) {
             LevelBuf<T> L;
-            L.g = make_geom(DIM, nx, ny, nz);
+            L.g = make_geom_pitched(DIM, nx, ny, nz);
             L.hx = hx; L.hy = hy; L.hz = hz;
             lv_.push_back(L);
             if (nx <= 4 || ny <= 4 || (DIM == 3 && nz <= 4)) break;
             nx /= 2; ny /= 2; nz /= 2;
             hx *= 2.0; hy *= 2.0; hz *= 2.0;
         }
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return E_CUDA;
         const int nl = (int)lv_.size();
         int e;
         for (int l = 0; l < nl; ++l) {
             LevelBuf<T>& L = lv_[l];
             const size_t n = (size_t)L.g.n;
             if ((e = alloc(L.solid, n))) return e;
+            if ((e = alloc(L.code, n))) return e;
             if ((e = alloc(L.cx, n))) return e;
             if ((e = alloc(L.cy, n))) return e;
             if (DIM == 3 && (e = alloc(L.cz, n))) return e;
@@ -302,55 +343,75 @@ private:
             if (l > 0) {
                 if ((e = alloc(L.x, n))) return e;
                 if ((e = alloc(L.b, n))) return e;
+                if ((e = alloc(L.dg, n))) return e;
+                if ((e = alloc(L.rdg, n))) return e;
             }
         }
         const Geom g0 = lv_[0].g;
         const size_t n0 = (size_t)g0.n;
         if ((e = alloc(r_, n0)) || (e = alloc(z_, n0)) || (e = alloc(p_, n0)) ||
-            (e = alloc(ap_, n0)) || (e = alloc(xlo_, n0)) || (e = alloc(b64_, n0)) ||
-            (e = alloc(xd_, n0)))
+            (e = alloc(p2_, n0)) || (e = alloc(ap_, n0)) || (e = alloc(xlo_, n0)) ||
+            (e = alloc(b64_, n0)) || (e = alloc(xd_, n0)))
             return e;
-        const dim3 blk = cell_block<DIM>();
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-            return E_CUDA;
-        if ((e = alloc(p2_, n0))) return e;
         if ((e = alloc(partials_, (size_t)max_reduce_blocks() * 4))) return e;
-        {
-            using TG = TileGeo<DIM, VTile<DIM>::X, VTile<DIM>::Y, VTile<DIM>::Z>;
-            const int sm = (int)TG::template smem_bytes<T>();
-            cudaFuncSetAttribute(k_vdown<DIM, T, VTile<DIM>::X, VTile<DIM>::Y, VTile<DIM>::Z>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-            cudaFuncSetAttribute(k_vup<DIM, T, VTile<DIM>::X, VTile<DIM>::Y, VTile<DIM>::Z, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-            cudaFuncSetAttribute(k_vup<DIM, T, VTile<DIM>::X, VTile<DIM>::Y, VTile<DIM>::Z, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        }
+        if ((e = alloc(err_, 1))) return e;
         if ((e = alloc(cg_, 1))) return e;
         if (cudaMallocHost(&cg_host_, sizeof(CGState)) != cudaSuccess) return E_OOM;
         if (cudaMallocHost(&flag_host_, 2 * sizeof(int)) != cudaSuccess) return E_OOM;
         for (auto& ev : ev_)
             if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return E_CUDA;
-
-        if (cudaMemcpyAsync(lv_[0].solid, d_solid, n0, cudaMemcpyDeviceToDevice, st_) != cudaSuccess)
+        // dynamic shared memory of the tile kernels
+        if (cudaFuncSetAttribute(k_vdown<DIM, T, TX, TY, TZ>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VP::BYTES) ||
+            cudaFuncSetAttribute(k_vup<DIM, T, TX, TY, TZ, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VP::BYTES) ||
+            cudaFuncSetAttribute(k_vup<DIM, T, TX, TY, TZ, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VP::BYTES) ||
+            cudaFuncSetAttribute(k_pmatvec_tile<DIM, T, TX, TY, TZ>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PP::BYTES))
             return E_CUDA;
+        // TMA maps
+        for (int l = 0; l < nl; ++l) {
+            LevelBuf<T>& L = lv_[l];
+            const T* b = l == 0 ? r_ : L.b;
+            if (!encode_level_map<T>(&L.map_b, b, L.g, DIM, VP::BW, VP::BY, VP::BZ) ||
+                !encode_level_map<uint8_t>(&L.map_c, L.code, L.g, DIM, VP::CW, VP::CY, VP::CZ))
+                return E_CUDA;
+        }
+        if (!encode_level_map<T>(&map_z_, z_, g0, DIM, PP::BW, PP::BY, PP::BZ) ||
+            !encode_level_map<T>(&map_p_, p_, g0, DIM, PP::BW, PP::BY, PP::BZ) ||
+            !encode_level_map<T>(&map_p2_, p2_, g0, DIM, PP::BW, PP::BY, PP::BZ) ||
+            !encode_level_map<uint8_t>(&map_c1_, lv_[0].code, g0, DIM, PP::CW, PP::CY, PP::CZ))
+            return E_CUDA;
+
+        // hierarchy: masks, couplings, coarse diagonals
+        const dim3 blk = cell_block<DIM>();
+        UAAMG_LAUNCH((KTag{K_SETUP, 0, 0.0}), k_import_mask<DIM>, vec_grid(g0), dim3(32, 8), g0, gref_,
+                     d_solid, lv_[0].solid);
         for (int l = 1; l < nl; ++l)
-            UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_restrict_solid<DIM>, cell_grid<DIM>(lv_[l].g.nx, lv_[l].g.ny, lv_[l].g.nz),
-                         blk, lv_[l - 1].g, lv_[l - 1].solid, lv_[l].g, lv_[l].solid);
+            UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_restrict_solid<DIM>,
+                         cell_grid<DIM>(lv_[l].g.nx, lv_[l].g.ny, lv_[l].g.nz), blk, lv_[l - 1].g,
+                         lv_[l - 1].solid, lv_[l].g, lv_[l].solid);
         {
             const LevelBuf<T>& L = lv_[0];
             const T idx2 = (T)(1.0 / (L.hx * L.hx)), idy2 = (T)(1.0 / (L.hy * L.hy));
             const T idz2 = DIM == 3 ? (T)(1.0 / (L.hz * L.hz)) : T(0);
-            UAAMG_LAUNCH((KTag{K_SETUP, 0, 0.0}), (k_fine_coeffs<DIM, T>), cell_grid<DIM>(L.g.nx, L.g.ny, L.g.nz), blk, L.g,
-                         L.solid, L.cx, L.cy, L.cz, L.wd, idx2, idy2, idz2);
+            UAAMG_LAUNCH((KTag{K_SETUP, 0, 0.0}), (k_fine_coeffs<DIM, T>),
+                         cell_grid<DIM>(L.g.nx, L.g.ny, L.g.nz), blk, L.g, L.solid, L.cx, L.cy, L.cz,
+                         L.wd, idx2, idy2, idz2);
         }
         for (int l = 1; l < nl; ++l) {
             const LevelBuf<T>& F = lv_[l - 1];
             LevelBuf<T>& Cl = lv_[l];
-            UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_galerkin<DIM, T>), cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, F.g,
-                         F.cx, F.cy, F.cz, F.wd, Cl.g, Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd);
+            UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_galerkin<DIM, T>),
+                         cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, F.g, F.cx, F.cy, F.cz, F.wd,
+                         Cl.g, Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd);
+            UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_diag<DIM, T>), vec_grid(Cl.g), dim3(32, 8), Cl.g,
+                         Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd, Cl.dg, Cl.rdg);
         }
+        for (int l = 0; l < nl; ++l)
+            UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_codes<DIM>, vec_grid(lv_[l].g), dim3(32, 8),
+                         lv_[l].g, lv_[l].solid, lv_[l].code, l == 0 ? 1 : 0);
         return sync_check();
     }
 
@@ -367,8 +428,9 @@ private:
 
     template <int DIM>
     void sweep(const LevelView<T>& v, int parity, const int* done, int lvl) {
-        UAAMG_LAUNCH((KTag{K_SWEEP, lvl, cells(v.g) * ((2.0 + DIM) * sizeof(T) + 0.5)}), (k_sweep<DIM, T>), cell_grid<DIM>((v.g.nx + 1) / 2, v.g.ny, v.g.nz),
-                     cell_block<DIM>(), v, parity, done);
+        UAAMG_LAUNCH((KTag{K_SWEEP, lvl, cells(v.g) * ((2.0 + DIM) * sizeof(T) + 0.5)}), (k_sweep<DIM, T>),
+                     cell_grid<DIM>((v.g.nx + 1) / 2, v.g.ny, v.g.nz), cell_block<DIM>(), v, parity,
+                     done);
     }
 
     // z = M^{-1} r with one kernel per colour sweep, restriction and prolongation
@@ -384,29 +446,40 @@ private:
             sweep<DIM>(v, 1, done, l);
             sweep<DIM>(v, 0, done, l);
             const LevelBuf<T>& Cl = lv_[l + 1];
-            UAAMG_LAUNCH((KTag{K_RESTRICT, l, cells(v.g) * ((2.0 + DIM) * sizeof(T) + 1.0) + cells(Cl.g) * sizeof(T)}), (k_restrict<DIM, T>), cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, v, Cl.g,
+            UAAMG_LAUNCH((KTag{K_RESTRICT, l, cells(v.g) * ((2.0 + DIM) * sizeof(T) + 1.0) + cells(Cl.g) * sizeof(T)}),
+                         (k_restrict<DIM, T>), cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, v, Cl.g,
                          Cl.solid, Cl.b, done);
             cudaMemsetAsync(Cl.x, 0, (size_t)Cl.g.n * sizeof(T), st_);
         }
-        {
-            const LevelView<T> v = view(nl - 1, r, z);
-            const int ncell = v.g.nx * v.g.ny * (DIM == 3 ? v.g.nz : 1);
-            if (ncell <= 65536) {
-                UAAMG_LAUNCH((KTag{K_COARSEST, nl - 1, 40.0 * cells(v.g) * ((2.0 + DIM) * sizeof(T) + 0.5)}), (k_coarsest<DIM, T>), 1, 1024, v, done);
-            } else {
-                for (int s = 0; s < 10; ++s) {
-                    sweep<DIM>(v, 1, done, nl - 1); sweep<DIM>(v, 0, done, nl - 1);
-                    sweep<DIM>(v, 0, done, nl - 1); sweep<DIM>(v, 1, done, nl - 1);
-                }
-            }
-        }
+        coarsest<DIM>(r, z, done);
         for (int l = nl - 2; l >= 0; --l) {
             const LevelView<T> v = view(l, r, z);
             const LevelBuf<T>& Cl = lv_[l + 1];
-            UAAMG_LAUNCH((KTag{K_PROLONG, l, cells(v.g) * (2.0 * sizeof(T) + 1.0) + cells(Cl.g) * (sizeof(T) + 1.0)}), (k_prolong<DIM, T>), cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, Cl.g,
+            UAAMG_LAUNCH((KTag{K_PROLONG, l, cells(v.g) * (2.0 * sizeof(T) + 1.0) + cells(Cl.g) * (sizeof(T) + 1.0)}),
+                         (k_prolong<DIM, T>), cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, Cl.g,
                          Cl.solid, Cl.x, v.g, v.solid, v.x, done);
             sweep<DIM>(v, 0, done, l);
             sweep<DIM>(v, 1, done, l);
+        }
+    }
+
+    // Coarsest level: 10 x (forward + reverse) sweeps from x = 0.
+    template <int DIM>
+    void coarsest(const T* r, T* z, const int* done) {
+        const int nl = (int)lv_.size();
+        const LevelBuf<T>& C = lv_[nl - 1];
+        T* cxp = nl == 1 ? z : C.x;
+        cudaMemsetAsync(cxp, 0, (size_t)C.g.n * sizeof(T), st_);
+        LevelView<T> v = view(nl - 1, r, z);
+        const int ncell = v.g.nx * v.g.ny * (DIM == 3 ? v.g.nz : 1);
+        if (ncell <= 65536) {
+            UAAMG_LAUNCH((KTag{K_COARSEST, nl - 1, 40.0 * cells(v.g) * ((2.0 + DIM) * sizeof(T) + 0.5)}),
+                         (k_coarsest<DIM, T>), 1, 1024, v, done);
+        } else {
+            for (int q = 0; q < 10; ++q) {
+                sweep<DIM>(v, 1, done, nl - 1); sweep<DIM>(v, 0, done, nl - 1);
+                sweep<DIM>(v, 0, done, nl - 1); sweep<DIM>(v, 1, done, nl - 1);
+            }
         }
     }
 
@@ -414,10 +487,10 @@ private:
         const LevelBuf<T>& L = lv_[l];
         VLevel<T> v;
         v.g = L.g;
-        v.solid = L.solid;
         v.cx = l == 0 ? nullptr : L.cx;
         v.cy = L.cy; v.cz = L.cz;
-        v.wd = L.wd;
+        v.dg = L.dg;
+        v.rdg = L.rdg;
         v.idx2 = (T)(1.0 / (L.hx * L.hx));
         v.idy2 = (T)(1.0 / (L.hy * L.hy));
         v.idz2 = L.g.nz ? (T)(1.0 / (L.hz * L.hz)) : T(0);
@@ -425,88 +498,89 @@ private:
         return v;
     }
 
-    // z = M^{-1} r with one fused kernel per level down (sweep + residual +
-    // restriction) and one per level up (prolongation + sweep), fused.cuh; the
-    // finest up kernel also reduces the CG's z sums when zdot is set.
     template <int DIM>
-    void vcycle_fused(const T* r, T* z, const int* done, bool zdot) {
+    void tiles(const Geom& g, int& ntx, int& nty, int& nt, int& grid, int per_sm) const {
+        ntx = (g.nx + VTile<DIM>::X - 1) / VTile<DIM>::X;
+        nty = (g.ny + VTile<DIM>::Y - 1) / VTile<DIM>::Y;
+        const int ntz = DIM == 3 ? (g.nz + VTile<DIM>::Z - 1) / VTile<DIM>::Z : 1;
+        nt = ntx * nty * ntz;
+        grid = nt < per_sm * num_sms_ ? nt : per_sm * num_sms_;
+    }
+
+    // z = M^{-1} r_ (r_ is the TMA-mapped level-0 b) with one fused kernel per level
+    // down and one per level up (fused.cuh); the finest up kernel also reduces the
+    // CG's z sums when zdot is set.
+    template <int DIM>
+    void vcycle_fused(T* z, const int* done, bool zdot) {
         constexpr int TX = VTile<DIM>::X, TY = VTile<DIM>::Y, TZ = VTile<DIM>::Z;
-        using TG = TileGeo<DIM, TX, TY, TZ>;
+        using VP = VPlan<DIM, T, TX, TY, TZ>;
         const int nl = (int)lv_.size();
-        const size_t sm = TG::template smem_bytes<T>();
-        const int per_sm = sm > 60000 ? 2 : 4;
-        auto tiles = [&](const Geom& g, int& ntx, int& nty, int& nt) {
-            ntx = (g.nx + TX - 1) / TX;
-            nty = (g.ny + TY - 1) / TY;
-            const int ntz = DIM == 3 ? (g.nz + TZ - 1) / TZ : 1;
-            nt = ntx * nty * ntz;
-        };
+        const int per_sm = VP::BYTES > 110000 ? 1 : (VP::BYTES > 74000 ? 2 : 3);
         for (int l = 0; l + 1 < nl; ++l) {
             const LevelBuf<T>& L = lv_[l];
             const LevelBuf<T>& Cl = lv_[l + 1];
-            int ntx, nty, nt;
-            tiles(L.g, ntx, nty, nt);
-            const int grid = nt < per_sm * num_sms_ ? nt : per_sm * num_sms_;
-            const double bytes = cells(L.g) * (sizeof(T) + 1.0 + (l ? DIM * sizeof(T) : 0.0)) +
+            int ntx, nty, nt, grid;
+            tiles<DIM>(L.g, ntx, nty, nt, grid, per_sm);
+            const double bytes = cells(L.g) * (sizeof(T) + 1.0 + (l ? (DIM + 1.0) * sizeof(T) : 0.0)) +
                                  cells(Cl.g) * sizeof(T);
-            UAAMG_LAUNCH_SMEM((KTag{K_VDOWN, l, bytes}), (k_vdown<DIM, T, TX, TY, TZ>), grid, 256, sm,
-                              vlevel(l), l == 0 ? r : (const T*)L.b, Cl.g, Cl.solid, Cl.b, ntx, nty, nt,
-                              done);
+            UAAMG_LAUNCH_SMEM((KTag{K_VDOWN, l, bytes}), (k_vdown<DIM, T, TX, TY, TZ>), grid, 256,
+                              VP::BYTES, L.map_b, L.map_c, vlevel(l), Cl.g, Cl.solid, Cl.b, ntx, nty,
+                              nt, done, err_);
         }
-        {
-            const LevelBuf<T>& C = lv_[nl - 1];
-            T* cx_ = nl == 1 ? z : C.x;
-            cudaMemsetAsync(cx_, 0, (size_t)C.g.n * sizeof(T), st_);
-            LevelView<T> v = view(nl - 1, r, z);
-            const int ncell = v.g.nx * v.g.ny * (DIM == 3 ? v.g.nz : 1);
-            if (ncell <= 65536) {
-                UAAMG_LAUNCH((KTag{K_COARSEST, nl - 1, 40.0 * cells(v.g) * ((2.0 + DIM) * sizeof(T) + 0.5)}),
-                             (k_coarsest<DIM, T>), 1, 1024, v, done);
-            } else {
-                for (int q = 0; q < 10; ++q) {
-                    sweep<DIM>(v, 1, done, nl - 1); sweep<DIM>(v, 0, done, nl - 1);
-                    sweep<DIM>(v, 0, done, nl - 1); sweep<DIM>(v, 1, done, nl - 1);
-                }
-            }
-            if (nl == 1 && zdot)
-                UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(C.g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>),
-                             vec_grid(C.g), dim3(32, 8), C.g, C.solid, r, z, partials_, cg_);
+        coarsest<DIM>(r_, z, done);
+        if (nl == 1 && zdot) {
+            const Geom& g = lv_[0].g;
+            UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>),
+                         vec_grid(g), dim3(32, 8), g, lv_[0].solid, r_, z, partials_, cg_);
         }
         for (int l = nl - 2; l >= 0; --l) {
             const LevelBuf<T>& L = lv_[l];
             const LevelBuf<T>& Cl = lv_[l + 1];
-            int ntx, nty, nt;
-            tiles(L.g, ntx, nty, nt);
-            const int grid = nt < per_sm * num_sms_ ? nt : per_sm * num_sms_;
-            const double bytes = cells(L.g) * (2.0 * sizeof(T) + 1.0 + (l ? DIM * sizeof(T) : 0.0)) +
+            int ntx, nty, nt, grid;
+            tiles<DIM>(L.g, ntx, nty, nt, grid, per_sm);
+            const double bytes = cells(L.g) * (2.0 * sizeof(T) + 1.0 + (l ? (DIM + 1.0) * sizeof(T) : 0.0)) +
                                  cells(Cl.g) * (sizeof(T) + 1.0);
-            const T* b = l == 0 ? r : (const T*)L.b;
             T* x = l == 0 ? z : L.x;
             if (l == 0 && zdot)
-                UAAMG_LAUNCH_SMEM((KTag{K_VUP, l, bytes}), (k_vup<DIM, T, TX, TY, TZ, true>), grid, 256, sm,
-                                  vlevel(l), b, Cl.g, Cl.solid, Cl.x, x, ntx, nty, nt, done, partials_, cg_);
+                UAAMG_LAUNCH_SMEM((KTag{K_VUP, l, bytes}), (k_vup<DIM, T, TX, TY, TZ, true>), grid, 256,
+                                  VP::BYTES, L.map_b, L.map_c, vlevel(l), Cl.g, Cl.solid, Cl.x, x, ntx,
+                                  nty, nt, done, err_, partials_, cg_);
             else
-                UAAMG_LAUNCH_SMEM((KTag{K_VUP, l, bytes}), (k_vup<DIM, T, TX, TY, TZ, false>), grid, 256, sm,
-                                  vlevel(l), b, Cl.g, Cl.solid, Cl.x, x, ntx, nty, nt, done, partials_, cg_);
+                UAAMG_LAUNCH_SMEM((KTag{K_VUP, l, bytes}), (k_vup<DIM, T, TX, TY, TZ, false>), grid, 256,
+                                  VP::BYTES, L.map_b, L.map_c, vlevel(l), Cl.g, Cl.solid, Cl.x, x, ntx,
+                                  nty, nt, done, err_, partials_, cg_);
+        }
+    }
+
+    // z = M^{-1} r_, then (zdot) the z sums -> mean, r.z, beta.
+    template <int DIM>
+    void vcycle(T* z, const int* done, bool zdot) {
+        if (sweeps_) {
+            vcycle_sweeps<DIM>(r_, z, done);
+            if (zdot) {
+                const Geom& g = lv_[0].g;
+                UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>),
+                             vec_grid(g), dim3(32, 8), g, lv_[0].solid, r_, z, partials_, cg_);
+            }
+        } else {
+            vcycle_fused<DIM>(z, done, zdot);
         }
     }
 
     template <int DIM>
-    void vcycle(const T* r, T* z, const int* done, bool zdot) {
-        if (sweeps_) {
-            vcycle_sweeps<DIM>(r, z, done);
-            if (zdot) {
-                const Geom& g = lv_[0].g;
-                UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>),
-                             vec_grid(g), dim3(32, 8), g, lv_[0].solid, r, z, partials_, cg_);
-            }
-        } else {
-            vcycle_fused<DIM>(r, z, done, zdot);
-        }
+    void precond_impl(const double* d_r, double* d_z) {
+        const Geom& g = lv_[0].g;
+        UAAMG_LAUNCH((KTag{K_CAST, 0, cells(g) * (8.0 + sizeof(T))}), (k_import<DIM, T>), vec_grid(g),
+                     dim3(32, 8), g, gref_, d_r, r_);
+        vcycle<DIM>(z_, nullptr, false);
+        UAAMG_LAUNCH((KTag{K_CAST, 0, cells(g) * (8.0 + sizeof(T))}), (k_export<DIM, T>), vec_grid(g),
+                     dim3(32, 8), g, gref_, z_, d_z, 0);
     }
 
     template <int DIM>
     int solve_impl(const SolveArgs& a) {
+        constexpr int TX = VTile<DIM>::X, TY = VTile<DIM>::Y, TZ = VTile<DIM>::Z;
+        using PP = PPlan<DIM, T, TX, TY, TZ>;
         const Geom g = lv_[0].g;
         const uint8_t* s = lv_[0].solid;
         const dim3 vb(32, 8);
@@ -528,78 +602,130 @@ private:
         *cg_host_ = init;
         if (cudaMemcpyAsync(cg_, cg_host_, sizeof(CGState), cudaMemcpyHostToDevice, st_) != cudaSuccess)
             return E_CUDA;
+        cudaMemsetAsync(err_, 0, sizeof(int), st_);
 
         // b = -(rhs - mean), re-projected; ||b|| (pcg_3d.cpp:22-36, 80-81)
-        UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 9.0}), k_sum_count<DIM>, vg, vb, g, s, a.rhs, partials_, cg_, 3);
-        UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 17.0}), k_rhs_negate<DIM>, vg, vb, g, s, a.rhs, b64_, cg_);
+        UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 16.0}), (k_import<DIM, double>), vg, vb, g, gref_, a.rhs, b64_);
+        UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 9.0}), k_sum_count<DIM>, vg, vb, g, s, b64_, partials_, cg_, 3);
+        UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 17.0}), k_rhs_negate<DIM>, vg, vb, g, s, b64_, b64_, cg_);
         UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 9.0}), k_sum_count<DIM>, vg, vb, g, s, b64_, partials_, cg_, 3);
         UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 17.0}), k_sub_mean<DIM>, vg, vb, g, s, b64_, cg_);
         UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 9.0}), k_norm<DIM>, vg, vb, g, s, b64_, partials_, cg_, 4);
-        if (a.warm)  // b <- b - A x_in: the solve then finds the correction to x_in
+        if (a.warm) {  // b <- b - A x_in: the solve then finds the correction to x_in
+            UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 16.0}), (k_import<DIM, double>), vg, vb, g, gref_, a.x, xd_);
             UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * 25.0}), (k_true_residual<DIM, double>), vg, vb,
-                         g, s, b64_, a.x, b64_, st, partials_, cg_, 5, 3, a.tol, a.tol_mode);
+                         g, s, b64_, xd_, b64_, st, partials_, cg_, 5, 3, a.tol, a.tol_mode);
+        }
         UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * (9.0 + sizeof(T))}), (k_true_residual<DIM, T>), vg, vb, g, s,
                      b64_, (const double*)nullptr, r_, st, partials_, cg_, 5, 0, a.tol, a.tol_mode);
         cudaMemsetAsync(xlo_, 0, (size_t)n * sizeof(T), st_);
         cudaMemsetAsync(p_, 0, (size_t)n * sizeof(T), st_);
-        if (mixed_) cudaMemsetAsync(xd_, 0, (size_t)n * sizeof(double), st_);
+        cudaMemsetAsync(xd_, 0, (size_t)n * sizeof(double), st_);
 
         const int* done = &cg_->done;
         // z = M r (or z = r), then the z sums -> mean, r.z, beta
         auto precond = [&]() {
             if (a.precond) {
-                vcycle<DIM>(r_, z_, done, true);
+                vcycle<DIM>(z_, done, true);
             } else {
                 cudaMemcpyAsync(z_, r_, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, st_);
                 UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>), vg, vb,
                              g, s, r_, z_, partials_, cg_);
             }
         };
+        int ntx, nty, nt, pgrid;
+        tiles<DIM>(g, ntx, nty, nt, pgrid, 4);
+        const long long nvec = (long long)n / Vec16<T>::N;
+        const int ugrid = max_reduce_blocks();
         precond();
-        T* pc = p_;   // current search direction
-        T* pn = p2_;  // next
-        for (int it = 0; it < a.max_iter; ++it) {
-            UAAMG_LAUNCH((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}), (k_pmatvec<DIM, T>), vg, vb,
-                         g, s, z_, pc, pn, ap_, st, partials_, cg_);
-            T* t = pc; pc = pn; pn = t;
-            UAAMG_LAUNCH((KTag{K_UPDATE, 0, cells(g) * (6.0 * sizeof(T))}), (k_update<DIM, T>), vg, vb, g,
-                         xlo_, r_, pc, ap_, partials_, cg_, a.hist);
+        // One PCG iteration (pcg_3d.cpp:93-124); the search direction alternates
+        // between p_ and p2_ (from_p: the current one lives in p_).
+        auto iteration = [&](bool from_p) {
+            T* pnew = from_p ? p2_ : p_;
+            UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
+                              (k_pmatvec_tile<DIM, T, TX, TY, TZ>), pgrid, 256, PP::BYTES, map_z_,
+                              from_p ? map_p_ : map_p2_, map_c1_, g, pnew, ap_, st, ntx, nty, nt,
+                              partials_, cg_, err_);
+            UAAMG_LAUNCH((KTag{K_UPDATE, 0, cells(g) * (6.0 * sizeof(T))}), k_update_flat<T>, ugrid, 256,
+                         nvec, xlo_, r_, pnew, ap_, partials_, cg_, a.hist);
             if (mixed_) {
-                UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T) + 1.0)}), (k_fold<DIM, T>), vg,
-                             vb, g, s, xd_, xlo_, cg_, 0);
+                UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T))}), k_fold_flat<T>, ugrid,
+                             256, (long long)n, xd_, xlo_, cg_, 0);
                 UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (17.0 + sizeof(T))}), (k_true_residual<DIM, T>),
                              vg, vb, g, s, b64_, xd_, r_, st, partials_, cg_, 5, 1, a.tol, a.tol_mode);
                 UAAMG_LAUNCH((KTag{K_SCALAR, 0, 0.0}), k_maxiter_check, 1, 1, cg_);
             }
             precond();
-            // Poll the device 'done' flag one iteration behind, so the host never
-            // idles the GPU waiting for a scalar.
-            const int slot = it & 1;
+        };
+        // Two iterations form one step (the search direction is back in p_ after
+        // it); outside profiling the step is a CUDA graph captured once per problem
+        // and options.  The host polls the device 'done' flag one step behind, so it
+        // never idles the GPU waiting for a scalar; kernels queued after the solve
+        // stopped return at once.
+        const bool use_graph = graphs_ && !prof_on_;
+        if (use_graph) {
+            const long long key = ((long long)a.precond << 1) | (sweeps_ ? 1 : 0);
+            if (!gexec_ || key != gkey_ || a.hist != ghist_) {
+                if (gexec_) { cudaGraphExecDestroy(gexec_); gexec_ = nullptr; }
+                if (!cap_ && cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking) != cudaSuccess)
+                    return E_CUDA;
+                cudaStream_t saved = st_;
+                const long before = launches_;
+                st_ = cap_;
+                cudaGraph_t graph = nullptr;
+                cudaError_t ce = cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal);
+                if (ce == cudaSuccess) {
+                    iteration(true);
+                    iteration(false);
+                    ce = cudaStreamEndCapture(cap_, &graph);
+                }
+                st_ = saved;
+                if (ce != cudaSuccess || !graph) return E_CUDA;
+                ce = cudaGraphInstantiate(&gexec_, graph, 0);
+                cudaGraphDestroy(graph);
+                if (ce != cudaSuccess) { gexec_ = nullptr; return E_CUDA; }
+                glaunches_ = launches_ - before;
+                launches_ = before;
+                gkey_ = key;
+                ghist_ = a.hist;
+            }
+        }
+        for (int it = 0, step = 0; it < a.max_iter; it += 2, ++step) {
+            if (use_graph) {
+                if (cudaGraphLaunch(gexec_, st_) != cudaSuccess) return E_CUDA;
+                launches_ += glaunches_;
+            } else {
+                iteration(true);
+                if (it + 1 < a.max_iter) iteration(false);
+            }
+            const int slot = step & 1;
             cudaMemcpyAsync(&flag_host_[slot], done, sizeof(int), cudaMemcpyDeviceToHost, st_);
             cudaEventRecord(ev_[slot], st_);
-            if (it > 0) {
+            if (step > 0) {
                 if (cudaEventSynchronize(ev_[slot ^ 1]) != cudaSuccess) return E_CUDA;
                 if (flag_host_[slot ^ 1]) break;
             }
         }
 
-        const int tb = 256, nb = (n + tb - 1) / tb;
         if (mixed_) {
-            UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T) + 1.0)}), (k_fold<DIM, T>), vg, vb,
-                         g, s, xd_, xlo_, cg_, 1);
+            UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T))}), k_fold_flat<T>, ugrid, 256,
+                         (long long)n, xd_, xlo_, cg_, 1);
         } else if (sizeof(T) == sizeof(double)) {
             cudaMemcpyAsync(xd_, xlo_, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_);
         } else {
-            UAAMG_LAUNCH((KTag{K_CAST, 0, 12.0 * n}), k_cast_to_f64<T>, nb, tb, xlo_, xd_, n);
+            UAAMG_LAUNCH((KTag{K_CAST, 0, 12.0 * n}), k_cast_to_f64<T>, (n + 255) / 256, 256, xlo_, xd_, n);
         }
         // exit diagnostics: FP64 true residual of the accumulated solution
         UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * 17.0}), (k_true_residual<DIM, T>), vg, vb, g, s,
                      b64_, xd_, (T*)nullptr, st, partials_, cg_, 5, 2, a.tol, a.tol_mode);
-        UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 25.0}), (k_output<DIM, double>), vg, vb, g, s, xd_, a.x);
-        if (a.project_mean) {
-            UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 9.0}), k_sum_count<DIM>, vg, vb, g, s, a.x, partials_,
-                         cg_, 3);
-            UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 17.0}), k_sub_mean<DIM>, vg, vb, g, s, a.x, cg_);
+        UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 24.0}), (k_export<DIM, double>), vg, vb, g, gref_, xd_,
+                     a.x, 1);
+        if (a.project_mean && a.ref_solid) {
+            const dim3 rg = vec_grid(gref_);
+            UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 9.0}), k_sum_count<DIM>, rg, vb, gref_, a.ref_solid,
+                         a.x, partials_, cg_, 3);
+            UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 17.0}), k_sub_mean<DIM>, rg, vb, gref_, a.ref_solid,
+                         a.x, cg_);
         }
         if (cudaMemcpyAsync(cg_host_, cg_, sizeof(CGState), cudaMemcpyDeviceToHost, st_) != cudaSuccess)
             return E_CUDA;

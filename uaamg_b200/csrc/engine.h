@@ -23,6 +23,7 @@ struct SolveArgs {
     int project_mean;    // subtract the fluid mean of the result (FP64)
     int precond;         // 1 UAAMG V-cycle, 0 identity (plain CG)
     double* hist;        // optional device array, max_iter+1: ||r_k|| per update
+    const uint8_t* ref_solid;  // the caller's mask (reference layout), for project_mean
 };
 
 struct SolveResult {
@@ -69,9 +70,13 @@ public:
     virtual long launches() const = 0;
     // V-cycle as per-colour sweep kernels (the cross-check) instead of the fused kernels.
     virtual void set_vcycle_sweeps(bool on) = 0;
+    // Replay each pair of PCG iterations as one CUDA graph (default on).
+    virtual void set_graphs(bool on) = 0;
     // Per-launch CUDA-event timing of subsequent solves (adds two events per launch).
     virtual void set_profiling(bool on) = 0;
     virtual int profile_results(std::vector<KernelTime>& out) = 0;
+    // Non-zero if a kernel of the last call gave up waiting for its TMA loads.
+    virtual int timed_out() = 0;
 };
 
 Engine* create_engine_f64();

@@ -366,10 +366,11 @@ __global__ void k_sum_count(Geom g, const uint8_t* __restrict__ s, const double*
 }
 
 // b = -(rhs - mean) on fluid interior cells, 0 elsewhere (pcg_3d.cpp:22-36);
-// mean = sum0/nfluid unless Dirichlet.
+// mean = sum0/nfluid unless Dirichlet.  b may alias rhs (each cell reads its own
+// value before writing it).
 template <int DIM>
-__global__ void k_rhs_negate(Geom g, const uint8_t* __restrict__ s, const double* __restrict__ rhs,
-                             double* b, const CGState* cg) {
+__global__ void k_rhs_negate(Geom g, const uint8_t* __restrict__ s, const double* rhs, double* b,
+                             const CGState* cg) {
     double mean = cg->nfluid > 0.0 ? cg->sum0 / cg->nfluid : 0.0;
     if (cg->dirichlet) mean = 0.0;
     for_cells<DIM>(g, [&](int, int, int, int id) {
@@ -448,92 +449,6 @@ __global__ void k_norm(Geom g, const uint8_t* __restrict__ s, const double* __re
     if (reduce_last<1>(acc, partials, &cg->counter[slot], tot)) cg->bnorm = sqrt(tot[0]);
 }
 
-// New search direction fused with the operator: p = (z - m) + beta p_old on fluid
-// cells (pcg_3d.cpp:115-122 with the mean projection of :113), Ap = A p with the
-// neighbours' new p formed on the fly from z and p_old, and p.Ap reduced; the
-// last block sets alpha = rz_old / p.Ap or stops on breakdown (pcg_3d.cpp:94-99).
-// p_old and p_new are distinct buffers (ping-pong), so no thread reads a p value
-// another thread is rewriting.
-template <int DIM, class T>
-__global__ void k_pmatvec(Geom g, const uint8_t* __restrict__ s, const T* __restrict__ z,
-                          const T* __restrict__ pold, T* __restrict__ pnew, T* __restrict__ ap,
-                          Stencil st, double* partials, CGState* cg) {
-    if (cg->done) return;
-    const T m = (T)cg->mean_z, beta = (T)cg->beta;
-    const T idx2 = (T)st.idx2, idy2 = (T)st.idy2, idz2 = (T)st.idz2, diag = (T)st.diag;
-    const int sx = g.sx, sxy = g.sxy;
-    double acc[1] = {0.0};
-    for_cells<DIM>(g, [&](int i, int j, int k, int id) {
-        if (s[id]) {
-            ap[id] = T(0);
-            pnew[id] = T(0);
-            return;
-        }
-        auto pv = [&](int q) -> T { return (z[q] - m) + beta * pold[q]; };
-        const T pc = pv(id);
-        const T wall = st.dirichlet ? -pc : pc;
-        const T vL = i > 1 ? (!s[id - 1] ? pv(id - 1) : pc) : wall;
-        const T vR = i < g.nx ? (!s[id + 1] ? pv(id + 1) : pc) : wall;
-        const T vB = j > 1 ? (!s[id - sx] ? pv(id - sx) : pc) : wall;
-        const T vT = j < g.ny ? (!s[id + sx] ? pv(id + sx) : pc) : wall;
-        T a;
-        if (DIM == 3) {
-            const T vF = k > 1 ? (!s[id - sxy] ? pv(id - sxy) : pc) : wall;
-            const T vK = k < g.nz ? (!s[id + sxy] ? pv(id + sxy) : pc) : wall;
-            a = diag * pc - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
-        } else {
-            a = diag * pc - (vL + vR) * idx2 - (vB + vT) * idy2;
-        }
-        pnew[id] = pc;
-        ap[id] = a;
-        acc[0] += (double)pc * (double)a;
-    });
-    double tot[1];
-    if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
-        const double pap = tot[0];
-        cg->pap = pap;
-        if (!(pap == pap)) { cg->status = CG_NAN; cg->done = 1; }
-        else if (pap < cg->breakdown) { cg->status = CG_BREAKDOWN; cg->done = 1; }
-        else cg->alpha = cg->rz_old / pap;
-    }
-}
-
-// x += alpha p, r -= alpha Ap, then r.r; the last block applies the stopping rule
-// sqrt(r.r) < tol_abs (pcg_3d.cpp:99-110).  p and Ap are 0 on solid cells and r
-// starts at 0 there, so no mask is read.  In mixed mode (replace_every > 0)
-// meeting the rule only marks a candidate that the FP64 residual replacement
-// confirms.
-template <int DIM, class T>
-__global__ void k_update(Geom g, T* x, T* r, const T* __restrict__ p, const T* __restrict__ ap,
-                         double* partials, CGState* cg, double* hist) {
-    if (cg->done) return;
-    const T alpha = (T)cg->alpha;
-    double acc[1] = {0.0};
-    for_cells<DIM>(g, [&](int, int, int, int id) {
-        x[id] += alpha * p[id];
-        const T rn = r[id] - alpha * ap[id];
-        r[id] = rn;
-        acc[0] += (double)rn * (double)rn;
-    });
-    double tot[1];
-    if (reduce_last<1>(acc, partials, &cg->counter[1], tot)) {
-        const double rr = tot[0];
-        cg->rr = rr;
-        cg->iter += 1;
-        if (hist) {
-            if (cg->iter == 1) hist[0] = cg->r0;
-            hist[cg->iter] = sqrt(rr);
-        }
-        if (!(rr == rr)) { cg->status = CG_NAN; cg->done = 1; }
-        else if (sqrt(rr) < cg->tol_abs) {
-            if (cg->replace_every > 0) cg->cand = 1;
-            else { cg->status = CG_CONVERGED; cg->done = 1; }
-        } else if (cg->iter >= cg->max_iter && cg->replace_every == 0) {
-            cg->status = CG_MAXITER; cg->done = 1;
-        }
-    }
-}
-
 // Mixed mode: after a replacement that did not converge, stop at max_iter.
 __global__ void k_maxiter_check(CGState* cg) {
     if (cg->done) return;
@@ -573,36 +488,6 @@ __global__ void k_zdot(Geom g, const uint8_t* __restrict__ s, const T* __restric
     });
     double tot[3];
     if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
-}
-
-// Mixed mode: fold the FP32 correction into the FP64 solution, x_hi += x_lo,
-// x_lo = 0, when a residual replacement is due (or unconditionally at exit).
-template <int DIM, class T>
-__global__ void k_fold(Geom g, const uint8_t* __restrict__ s, double* xhi, T* xlo,
-                       const CGState* cg, int force) {
-    if (!force) {
-        if (cg->done) return;
-        if (!(cg->cand || (cg->replace_every > 0 && cg->iter > 0 &&
-                           cg->iter % cg->replace_every == 0)))
-            return;
-    }
-    for_cells<DIM>(g, [&](int, int, int, int id) {
-        if (s[id]) return;
-        xhi[id] += (double)xlo[id];
-        xlo[id] = T(0);
-    });
-}
-
-// Output: out += x on fluid cells.  Callers keep the incoming value in out, so a
-// cold start accumulates into it exactly like PCG::solve accumulates into g.p
-// (pcg_3d.cpp:105), and a warm start (whose residual already accounts for it)
-// returns x_in + correction.
-template <int DIM, class T>
-__global__ void k_output(Geom g, const uint8_t* __restrict__ s, const T* __restrict__ x,
-                         double* out) {
-    for_cells<DIM>(g, [&](int, int, int, int id) {
-        if (!s[id]) out[id] = out[id] + (double)x[id];
-    });
 }
 
 // FP64 <-> T conversions on the padded arrays.
