@@ -119,8 +119,9 @@ UAAMG_API uaamg_status uaamg_set_problem_device(uaamg_handle* h, int dim, int nx
  * Takes effect at the next uaamg_set_problem_*. */
 UAAMG_API uaamg_status uaamg_set_dirichlet_walls(uaamg_handle* h, int on);
 
-/* V-cycle kernels of this handle: 0 (default) = fused, one kernel per level and
- * direction (sweep + residual + restriction down, prolongation + sweep up);
+/* V-cycle kernels of this handle: 0 (default) = z marches, four per level (forward
+ * sweep; residual + restriction; prolongation + even colour; odd colour), each
+ * streaming the level's planes through TMA-filled shared memory;
  * 1 = one kernel per colour sweep, restriction and prolongation, step by step as
  * UAAMGPreconditioner3D::vCycle (uaamg_preconditioner_3d.cpp:183-196).  Both give
  * identical results; 1 exists to cross-check 0. */

@@ -36,9 +36,9 @@ def rel_l2_meanfree(a, b, solid):
 # --- golden fixtures ---------------------------------------------------------
 
 
-@pytest.fixture(params=["fused", "sweeps"])
+@pytest.fixture(params=["march", "sweeps"])
 def vkernels(request, handle):
-    """Both V-cycle implementations: fused level kernels and per-colour sweeps."""
+    """Both V-cycle implementations: z-march level kernels and per-colour sweeps."""
     handle.set_vcycle_kernels(request.param == "sweeps")
     yield request.param
     handle.set_vcycle_kernels(False)

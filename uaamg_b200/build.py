@@ -30,7 +30,7 @@ UNITS = [
     ("api.cpp", ["-x", "cu"]),
     ("noalloc.cu", ["-fmad=false"]),
 ]
-HEADERS = ["common.cuh", "kernels.cuh", "fused.cuh", "tma.cuh", "engine.cuh", "engine.h"]
+HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "vec.cuh", "tma.cuh", "engine.cuh", "engine.h"]
 
 
 def _nvcc() -> str:

@@ -18,9 +18,9 @@
 #include <vector>
 
 #include "engine.h"
-#include "fused.cuh"
 #include "kernels.cuh"
 #include "tma.cuh"
+#include "vec.cuh"
 
 namespace uaamg {
 namespace {
@@ -30,21 +30,25 @@ struct LevelBuf {
     Geom g;
     double hx, hy, hz;
     uint8_t* solid = nullptr;
-    T *cx = nullptr, *cy = nullptr, *cz = nullptr, *wd = nullptr, *dg = nullptr, *rdg = nullptr;
+    T *cx = nullptr, *cy = nullptr, *cz = nullptr, *wd = nullptr, *dg = nullptr;
     T *x = nullptr, *b = nullptr;  // level >= 1 only (level 0 uses the CG's r and z)
-    uint8_t* code = nullptr;       // cell codes (fused.cuh)
-    CUtensorMap map_b, map_c;      // TMA maps of b and the codes for the V-cycle tiles
+    uint8_t* code = nullptr;       // cell codes (vec.cuh k_codes)
+    int zc = 2;                    // planes per block of the z marches (march.cuh)
+    // plane-box tensor maps of the marches: b, x, codes, couplings, diagonal, and x
+    // as the parent box read by the next-finer level's prolongation
+    CUtensorMap mb, mx, mcode, mcx, mcy, mcz, mdg, mxq;
 };
 
 // Kernel classes for the in-situ per-kernel timing (uaamg_profile_solve).
 enum KClass : int {
-    K_SWEEP = 0, K_RESTRICT, K_PROLONG, K_COARSEST, K_PMATVEC, K_UPDATE, K_ZDOT, K_VDOWN,
-    K_VUP, K_TRUE_RESIDUAL, K_FOLD, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_SCALAR, K_NCLASS
+    K_SWEEP = 0, K_RESTRICT, K_PROLONG, K_COARSEST, K_PMATVEC, K_UPDATE, K_ZDOT, K_FWD, K_RES,
+    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_FOLD, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_SCALAR, K_NCLASS
 };
 static const char* const kclass_names[K_NCLASS] = {
     "rbgs_sweep", "restrict_residual", "prolong_add", "coarsest_solve", "p_matvec_dot",
-    "cg_update", "z_dot", "vcycle_down", "vcycle_up", "true_residual", "fold", "rhs_prepare",
-    "output", "cast", "hierarchy_setup", "scalar"};
+    "cg_update", "z_dot", "smooth_fwd", "residual_restrict", "prolong_smooth_even",
+    "smooth_odd", "true_residual", "fold", "rhs_prepare", "output", "cast", "hierarchy_setup",
+    "scalar"};
 
 struct KTag {
     int cls;
@@ -63,11 +67,6 @@ struct KTag {
     } while (0)
 #define UAAMG_LAUNCH(tag, kern, grid, block, ...) \
     UAAMG_LAUNCH_SMEM(tag, kern, grid, block, 0, __VA_ARGS__)
-
-// Tile shapes (cells per block tile; 256 threads per block).
-template <int DIM> struct VTile;
-template <> struct VTile<3> { static constexpr int X = 32, Y = 8, Z = 8; };
-template <> struct VTile<2> { static constexpr int X = 64, Y = 32, Z = 1; };
 
 template <class T>
 class EngineT final : public Engine {
@@ -211,7 +210,8 @@ private:
     T *r_ = nullptr, *z_ = nullptr, *p_ = nullptr, *p2_ = nullptr, *ap_ = nullptr, *xlo_ = nullptr;
     double *b64_ = nullptr, *xd_ = nullptr, *partials_ = nullptr;
     int* err_ = nullptr;             // set by a kernel whose TMA wait gave up
-    CUtensorMap map_z_, map_p_, map_p2_, map_c1_;  // search-direction kernel tiles
+    CUtensorMap map_p_, map_p2_;     // plane boxes of the two search-direction buffers
+    long long reduce_blocks_ = 0;    // partials_ capacity in blocks (4 doubles each)
     CGState* cg_ = nullptr;
     CGState* cg_host_ = nullptr;  // pinned
     int* flag_host_ = nullptr;    // pinned, 2 slots
@@ -221,7 +221,7 @@ private:
     size_t bytes_ = 0;
     long launches_ = 0;
     int num_sms_ = 148;
-    bool sweeps_ = false;  // V-cycle as per-colour sweeps (cross-check) instead of fused
+    bool sweeps_ = false;  // V-cycle as per-colour sweeps (cross-check) instead of the marches
     bool graphs_ = true;   // replay the PCG step as a CUDA graph
     cudaStream_t cap_ = nullptr;      // capture stream
     cudaGraphExec_t gexec_ = nullptr; // two PCG iterations
@@ -305,11 +305,43 @@ private:
         return e == cudaSuccess ? E_OK : E_CUDA;
     }
 
+    // Blocks of a march over level g: 32 x 8 column tiles, z chunks of zc planes.
+    template <int DIM>
+    static dim3 march_grid(const Geom& g, int zc) {
+        return dim3((unsigned)((g.nx + kMX - 1) / kMX), (unsigned)((g.ny + kMY - 1) / kMY),
+                    DIM == 3 ? (unsigned)((g.nz + zc - 1) / zc) : 1u);
+    }
+
+    // Largest even chunk <= 16 planes that still gives every SM several blocks.
+    int pick_zc(const Geom& g) const {
+        const long long tiles = (long long)((g.nx + kMX - 1) / kMX) * ((g.ny + kMY - 1) / kMY);
+        int zc = 16;
+        while (zc > 2 && tiles * ((g.nz + zc - 1) / zc) < 4LL * num_sms_) zc /= 2;
+        return zc;
+    }
+
+    template <class K>
+    static int smem_attr(K kern, size_t bytes) {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
+                       cudaSuccess
+                   ? E_OK
+                   : E_CUDA;
+    }
+
+    template <int DIM, bool FINE>
+    int march_attrs() {
+        int e;
+        if ((e = smem_attr(k_fwd_smooth<DIM, T, FINE>, FwdCfg<DIM, T, FINE>::BYTES)) ||
+            (e = smem_attr(k_restrict_res<DIM, T, FINE>, ResCfg<DIM, T, FINE>::BYTES)) ||
+            (e = smem_attr(k_up_even<DIM, T, FINE>, UpeCfg<DIM, T, FINE>::BYTES)) ||
+            (e = smem_attr(k_up_odd<DIM, T, FINE, false>, UpoCfg<DIM, T, FINE>::BYTES)) ||
+            (e = smem_attr(k_up_odd<DIM, T, FINE, true>, UpoCfg<DIM, T, FINE>::BYTES)))
+            return e;
+        return E_OK;
+    }
+
     template <int DIM>
     int build(int nx, int ny, int nz, const uint8_t* d_solid) {
-        constexpr int TX = VTile<DIM>::X, TY = VTile<DIM>::Y, TZ = VTile<DIM>::Z;
-        using VP = VPlan<DIM, T, TX, TY, TZ>;
-        using PP = PPlan<DIM, T, TX, TY, TZ>;
         gref_ = make_geom(DIM, nx, ny, nz);
         {
             const Geom gp = make_geom_pitched(DIM, nx, ny, nz);
@@ -333,6 +365,7 @@ private:
         int e;
         for (int l = 0; l < nl; ++l) {
             LevelBuf<T>& L = lv_[l];
+            L.zc = DIM == 3 ? pick_zc(L.g) : 2;
             const size_t n = (size_t)L.g.n;
             if ((e = alloc(L.solid, n))) return e;
             if ((e = alloc(L.code, n))) return e;
@@ -344,7 +377,6 @@ private:
                 if ((e = alloc(L.x, n))) return e;
                 if ((e = alloc(L.b, n))) return e;
                 if ((e = alloc(L.dg, n))) return e;
-                if ((e = alloc(L.rdg, n))) return e;
             }
         }
         const Geom g0 = lv_[0].g;
@@ -353,35 +385,44 @@ private:
             (e = alloc(p2_, n0)) || (e = alloc(ap_, n0)) || (e = alloc(xlo_, n0)) ||
             (e = alloc(b64_, n0)) || (e = alloc(xd_, n0)))
             return e;
-        if ((e = alloc(partials_, (size_t)max_reduce_blocks() * 4))) return e;
+        // reductions: the finest-level marches (one partial per block) and the
+        // row-walk kernels (vec_grid)
+        {
+            const dim3 mg = march_grid<DIM>(g0, lv_[0].zc);
+            reduce_blocks_ = (long long)mg.x * mg.y * mg.z;
+            if (reduce_blocks_ < max_reduce_blocks()) reduce_blocks_ = max_reduce_blocks();
+        }
+        if ((e = alloc(partials_, (size_t)reduce_blocks_ * 4))) return e;
         if ((e = alloc(err_, 1))) return e;
         if ((e = alloc(cg_, 1))) return e;
         if (cudaMallocHost(&cg_host_, sizeof(CGState)) != cudaSuccess) return E_OOM;
         if (cudaMallocHost(&flag_host_, 2 * sizeof(int)) != cudaSuccess) return E_OOM;
         for (auto& ev : ev_)
             if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return E_CUDA;
-        // dynamic shared memory of the tile kernels
-        if (cudaFuncSetAttribute(k_vdown<DIM, T, TX, TY, TZ>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VP::BYTES) ||
-            cudaFuncSetAttribute(k_vup<DIM, T, TX, TY, TZ, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VP::BYTES) ||
-            cudaFuncSetAttribute(k_vup<DIM, T, TX, TY, TZ, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VP::BYTES) ||
-            cudaFuncSetAttribute(k_pmatvec_tile<DIM, T, TX, TY, TZ>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PP::BYTES))
-            return E_CUDA;
-        // TMA maps
+        // dynamic shared memory of the marches
+        if ((e = march_attrs<DIM, true>()) || (e = march_attrs<DIM, false>()) ||
+            (e = smem_attr(k_pmatvec<DIM, T>, PmvCfg<DIM, T>::BYTES)))
+            return e;
+        // plane-box tensor maps
+        constexpr int BW = PBox<T>::W, BH = PBox<T>::H;
         for (int l = 0; l < nl; ++l) {
             LevelBuf<T>& L = lv_[l];
             const T* b = l == 0 ? r_ : L.b;
-            if (!encode_level_map<T>(&L.map_b, b, L.g, DIM, VP::BW, VP::BY, VP::BZ) ||
-                !encode_level_map<uint8_t>(&L.map_c, L.code, L.g, DIM, VP::CW, VP::CY, VP::CZ))
-                return E_CUDA;
+            const T* x = l == 0 ? z_ : L.x;
+            bool ok = encode_level_map<T>(&L.mb, b, L.g, DIM, BW, BH, 1) &&
+                      encode_level_map<T>(&L.mx, x, L.g, DIM, BW, BH, 1) &&
+                      encode_level_map<uint8_t>(&L.mcode, L.code, L.g, DIM, PBox<uint8_t>::W,
+                                                PBox<uint8_t>::H, 1);
+            if (ok && l > 0)
+                ok = encode_level_map<T>(&L.mcx, L.cx, L.g, DIM, BW, BH, 1) &&
+                     encode_level_map<T>(&L.mcy, L.cy, L.g, DIM, BW, BH, 1) &&
+                     (DIM == 2 || encode_level_map<T>(&L.mcz, L.cz, L.g, DIM, BW, BH, 1)) &&
+                     encode_level_map<T>(&L.mdg, L.dg, L.g, DIM, BW, BH, 1) &&
+                     encode_level_map<T>(&L.mxq, L.x, L.g, DIM, QBox<T>::W, QBox<T>::H, 1);
+            if (!ok) return E_CUDA;
         }
-        if (!encode_level_map<T>(&map_z_, z_, g0, DIM, PP::BW, PP::BY, PP::BZ) ||
-            !encode_level_map<T>(&map_p_, p_, g0, DIM, PP::BW, PP::BY, PP::BZ) ||
-            !encode_level_map<T>(&map_p2_, p2_, g0, DIM, PP::BW, PP::BY, PP::BZ) ||
-            !encode_level_map<uint8_t>(&map_c1_, lv_[0].code, g0, DIM, PP::CW, PP::CY, PP::CZ))
+        if (!encode_level_map<T>(&map_p_, p_, g0, DIM, BW, BH, 1) ||
+            !encode_level_map<T>(&map_p2_, p2_, g0, DIM, BW, BH, 1))
             return E_CUDA;
 
         // hierarchy: masks, couplings, coarse diagonals
@@ -407,7 +448,7 @@ private:
                          cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, F.g, F.cx, F.cy, F.cz, F.wd,
                          Cl.g, Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd);
             UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_diag<DIM, T>), vec_grid(Cl.g), dim3(32, 8), Cl.g,
-                         Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd, Cl.dg, Cl.rdg);
+                         Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd, Cl.dg);
         }
         for (int l = 0; l < nl; ++l)
             UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_codes<DIM>, vec_grid(lv_[l].g), dim3(32, 8),
@@ -483,72 +524,95 @@ private:
         }
     }
 
-    VLevel<T> vlevel(int l) const {
+    MLevel<T> mlevel(int l) const {
         const LevelBuf<T>& L = lv_[l];
-        VLevel<T> v;
+        MLevel<T> v;
         v.g = L.g;
-        v.cx = l == 0 ? nullptr : L.cx;
-        v.cy = L.cy; v.cz = L.cz;
-        v.dg = L.dg;
-        v.rdg = L.rdg;
+        v.cg = l + 1 < (int)lv_.size() ? lv_[l + 1].g : L.g;
         v.idx2 = (T)(1.0 / (L.hx * L.hx));
         v.idy2 = (T)(1.0 / (L.hy * L.hy));
         v.idz2 = L.g.nz ? (T)(1.0 / (L.hz * L.hz)) : T(0);
         v.dirichlet = dirichlet_;
+        v.zc = L.zc;
         return v;
     }
 
+    // Tensor maps of a march over level l: value slots b, [x], [cx, cy, (cz), dg]
+    // (coefficients on coarse levels), the codes and, for the prolongation, the
+    // next-coarser level's x as parent boxes.
     template <int DIM>
-    void tiles(const Geom& g, int& ntx, int& nty, int& nt, int& grid, int per_sm) const {
-        ntx = (g.nx + VTile<DIM>::X - 1) / VTile<DIM>::X;
-        nty = (g.ny + VTile<DIM>::Y - 1) / VTile<DIM>::Y;
-        const int ntz = DIM == 3 ? (g.nz + VTile<DIM>::Z - 1) / VTile<DIM>::Z : 1;
-        nt = ntx * nty * ntz;
-        grid = nt < per_sm * num_sms_ ? nt : per_sm * num_sms_;
+    MarchMaps maps(int l, bool hasx, bool parent) const {
+        const LevelBuf<T>& L = lv_[l];
+        MarchMaps m;
+        int q = 0;
+        m.v[q++] = L.mb;
+        if (hasx) m.v[q++] = L.mx;
+        if (l > 0) {
+            m.v[q++] = L.mcx;
+            m.v[q++] = L.mcy;
+            if (DIM == 3) m.v[q++] = L.mcz;
+            m.v[q++] = L.mdg;
+        }
+        m.code = L.mcode;
+        if (parent) m.xc = lv_[l + 1].mxq;
+        return m;
     }
 
-    // z = M^{-1} r_ (r_ is the TMA-mapped level-0 b) with one fused kernel per level
-    // down and one per level up (fused.cuh); the finest up kernel also reduces the
-    // CG's z sums when zdot is set.
+    template <int DIM, bool FINE>
+    void down_level(int l, const int* done) {
+        const LevelBuf<T>& L = lv_[l];
+        const LevelBuf<T>& Cl = lv_[l + 1];
+        const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
+        const double coef = FINE ? 0.0 : (DIM + 1.0) * t;
+        const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kMX, kMY);
+        T* x = l == 0 ? z_ : L.x;
+        UAAMG_LAUNCH_SMEM((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_smooth<DIM, T, FINE>),
+                          grid, blk, (FwdCfg<DIM, T, FINE>::BYTES), maps<DIM>(l, false, false),
+                          mlevel(l), x, done, err_);
+        UAAMG_LAUNCH_SMEM((KTag{K_RES, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
+                          (k_restrict_res<DIM, T, FINE>), grid, blk, (ResCfg<DIM, T, FINE>::BYTES),
+                          maps<DIM>(l, true, false), mlevel(l), Cl.code, Cl.b, done, err_);
+    }
+
+    template <int DIM, bool FINE>
+    void up_level(int l, const int* done, bool zdot) {
+        const LevelBuf<T>& L = lv_[l];
+        const LevelBuf<T>& Cl = lv_[l + 1];
+        const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
+        const double coef = FINE ? 0.0 : (DIM + 1.0) * t;
+        const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kMX, kMY);
+        T* x = l == 0 ? z_ : L.x;
+        UAAMG_LAUNCH_SMEM((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
+                          (k_up_even<DIM, T, FINE>), grid, blk, (UpeCfg<DIM, T, FINE>::BYTES),
+                          maps<DIM>(l, false, true), mlevel(l), x, done, err_);
+        if (zdot)
+            UAAMG_LAUNCH_SMEM((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
+                              (k_up_odd<DIM, T, FINE, true>), grid, blk, (UpoCfg<DIM, T, FINE>::BYTES),
+                              maps<DIM>(l, true, false), mlevel(l), x, done, err_, partials_, cg_);
+        else
+            UAAMG_LAUNCH_SMEM((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
+                              (k_up_odd<DIM, T, FINE, false>), grid, blk, (UpoCfg<DIM, T, FINE>::BYTES),
+                              maps<DIM>(l, true, false), mlevel(l), x, done, err_, partials_, cg_);
+    }
+
+    // z_ = M^{-1} r_ with four z marches per level (march.cuh); the finest level's
+    // last march also reduces the CG's z sums when zdot is set.
     template <int DIM>
-    void vcycle_fused(T* z, const int* done, bool zdot) {
-        constexpr int TX = VTile<DIM>::X, TY = VTile<DIM>::Y, TZ = VTile<DIM>::Z;
-        using VP = VPlan<DIM, T, TX, TY, TZ>;
+    void vcycle_march(const int* done, bool zdot) {
         const int nl = (int)lv_.size();
-        const int per_sm = VP::BYTES > 110000 ? 1 : (VP::BYTES > 74000 ? 2 : 3);
         for (int l = 0; l + 1 < nl; ++l) {
-            const LevelBuf<T>& L = lv_[l];
-            const LevelBuf<T>& Cl = lv_[l + 1];
-            int ntx, nty, nt, grid;
-            tiles<DIM>(L.g, ntx, nty, nt, grid, per_sm);
-            const double bytes = cells(L.g) * (sizeof(T) + 1.0 + (l ? (DIM + 1.0) * sizeof(T) : 0.0)) +
-                                 cells(Cl.g) * sizeof(T);
-            UAAMG_LAUNCH_SMEM((KTag{K_VDOWN, l, bytes}), (k_vdown<DIM, T, TX, TY, TZ>), grid, 256,
-                              VP::BYTES, L.map_b, L.map_c, vlevel(l), Cl.g, Cl.solid, Cl.b, ntx, nty,
-                              nt, done, err_);
+            if (l == 0) down_level<DIM, true>(l, done);
+            else down_level<DIM, false>(l, done);
         }
-        coarsest<DIM>(r_, z, done);
+        coarsest<DIM>(r_, z_, done);
         if (nl == 1 && zdot) {
             const Geom& g = lv_[0].g;
             UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>),
-                         vec_grid(g), dim3(32, 8), g, lv_[0].solid, r_, z, partials_, cg_);
+                         vec_grid(g), dim3(32, 8), g, lv_[0].solid, r_, z_, partials_, cg_);
         }
         for (int l = nl - 2; l >= 0; --l) {
-            const LevelBuf<T>& L = lv_[l];
-            const LevelBuf<T>& Cl = lv_[l + 1];
-            int ntx, nty, nt, grid;
-            tiles<DIM>(L.g, ntx, nty, nt, grid, per_sm);
-            const double bytes = cells(L.g) * (2.0 * sizeof(T) + 1.0 + (l ? (DIM + 1.0) * sizeof(T) : 0.0)) +
-                                 cells(Cl.g) * (sizeof(T) + 1.0);
-            T* x = l == 0 ? z : L.x;
-            if (l == 0 && zdot)
-                UAAMG_LAUNCH_SMEM((KTag{K_VUP, l, bytes}), (k_vup<DIM, T, TX, TY, TZ, true>), grid, 256,
-                                  VP::BYTES, L.map_b, L.map_c, vlevel(l), Cl.g, Cl.solid, Cl.x, x, ntx,
-                                  nty, nt, done, err_, partials_, cg_);
-            else
-                UAAMG_LAUNCH_SMEM((KTag{K_VUP, l, bytes}), (k_vup<DIM, T, TX, TY, TZ, false>), grid, 256,
-                                  VP::BYTES, L.map_b, L.map_c, vlevel(l), Cl.g, Cl.solid, Cl.x, x, ntx,
-                                  nty, nt, done, err_, partials_, cg_);
+            if (l == 0) up_level<DIM, true>(l, done, zdot);
+            else up_level<DIM, false>(l, done, false);
         }
     }
 
@@ -563,7 +627,7 @@ private:
                              vec_grid(g), dim3(32, 8), g, lv_[0].solid, r_, z, partials_, cg_);
             }
         } else {
-            vcycle_fused<DIM>(z, done, zdot);
+            vcycle_march<DIM>(done, zdot);
         }
     }
 
@@ -579,8 +643,6 @@ private:
 
     template <int DIM>
     int solve_impl(const SolveArgs& a) {
-        constexpr int TX = VTile<DIM>::X, TY = VTile<DIM>::Y, TZ = VTile<DIM>::Z;
-        using PP = PPlan<DIM, T, TX, TY, TZ>;
         const Geom g = lv_[0].g;
         const uint8_t* s = lv_[0].solid;
         const dim3 vb(32, 8);
@@ -633,8 +695,13 @@ private:
                              g, s, r_, z_, partials_, cg_);
             }
         };
-        int ntx, nty, nt, pgrid;
-        tiles<DIM>(g, ntx, nty, nt, pgrid, 4);
+        const dim3 pgrid = march_grid<DIM>(g, lv_[0].zc);
+        MarchMaps pm[2];  // z and the current search direction (p_, p2_), codes
+        for (int q = 0; q < 2; ++q) {
+            pm[q] = maps<DIM>(0, true, false);
+            pm[q].v[0] = lv_[0].mx;
+            pm[q].v[1] = q == 0 ? map_p_ : map_p2_;
+        }
         const long long nvec = (long long)n / Vec16<T>::N;
         const int ugrid = max_reduce_blocks();
         precond();
@@ -643,9 +710,8 @@ private:
         auto iteration = [&](bool from_p) {
             T* pnew = from_p ? p2_ : p_;
             UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
-                              (k_pmatvec_tile<DIM, T, TX, TY, TZ>), pgrid, 256, PP::BYTES, map_z_,
-                              from_p ? map_p_ : map_p2_, map_c1_, g, pnew, ap_, st, ntx, nty, nt,
-                              partials_, cg_, err_);
+                              (k_pmatvec<DIM, T>), pgrid, dim3(kMX, kMY), (PmvCfg<DIM, T>::BYTES),
+                              pm[from_p ? 0 : 1], g, lv_[0].zc, pnew, ap_, st, partials_, cg_, err_);
             UAAMG_LAUNCH((KTag{K_UPDATE, 0, cells(g) * (6.0 * sizeof(T))}), k_update_flat<T>, ugrid, 256,
                          nvec, xlo_, r_, pnew, ap_, partials_, cg_, a.hist);
             if (mixed_) {

@@ -1,0 +1,161 @@
+// CG vector kernels over whole padded arrays, layout conversions between the
+// caller's layout and the pitched one, and the per-level set-up of cell codes and
+// coarse diagonals.
+#pragma once
+#include "march.cuh"
+
+namespace uaamg {
+namespace {
+
+// x += alpha p, r -= alpha Ap over the whole padded array with 16-byte vectors
+// (p and Ap are 0 outside fluid cells, r starts at 0 there), then r.r; the last
+// block applies the stopping rule sqrt(r.r) < tol_abs (pcg_3d.cpp:99-110).  In
+// mixed mode meeting the rule only marks a candidate for the FP64 residual
+// replacement to confirm.
+template <class T>
+struct Vec16;
+template <> struct Vec16<float> { using V = float4; static constexpr int N = 4; };
+template <> struct Vec16<double> { using V = double2; static constexpr int N = 2; };
+
+template <class T>
+__device__ __forceinline__ void vaxpy_rr(typename Vec16<T>::V& x, typename Vec16<T>::V& r,
+                                         const typename Vec16<T>::V& p,
+                                         const typename Vec16<T>::V& a, T alpha, double& rr);
+template <>
+__device__ __forceinline__ void vaxpy_rr<float>(float4& x, float4& r, const float4& p,
+                                                const float4& a, float alpha, double& rr) {
+    x.x += alpha * p.x; x.y += alpha * p.y; x.z += alpha * p.z; x.w += alpha * p.w;
+    r.x = r.x - alpha * a.x; r.y = r.y - alpha * a.y; r.z = r.z - alpha * a.z; r.w = r.w - alpha * a.w;
+    rr += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
+    rr += (double)r.z * (double)r.z + (double)r.w * (double)r.w;
+}
+template <>
+__device__ __forceinline__ void vaxpy_rr<double>(double2& x, double2& r, const double2& p,
+                                                 const double2& a, double alpha, double& rr) {
+    x.x += alpha * p.x; x.y += alpha * p.y;
+    r.x = r.x - alpha * a.x; r.y = r.y - alpha * a.y;
+    rr += r.x * r.x;
+    rr += r.y * r.y;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
+                                                     const T* __restrict__ p,
+                                                     const T* __restrict__ ap, double* partials,
+                                                     CGState* cg, double* hist) {
+    if (cg->done) return;
+    using V = typename Vec16<T>::V;
+    const T alpha = (T)cg->alpha;
+    V* xv = reinterpret_cast<V*>(x);
+    V* rv = reinterpret_cast<V*>(r);
+    const V* pv = reinterpret_cast<const V*>(p);
+    const V* av = reinterpret_cast<const V*>(ap);
+    double acc[1] = {0.0};
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nvec; t += stride) {
+        V xx = xv[t], rr_ = rv[t];
+        const V pp = __ldg(&pv[t]), aa = __ldg(&av[t]);
+        vaxpy_rr<T>(xx, rr_, pp, aa, alpha, acc[0]);
+        xv[t] = xx;
+        rv[t] = rr_;
+    }
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[1], tot)) {
+        const double rr = tot[0];
+        cg->rr = rr;
+        cg->iter += 1;
+        if (hist) {
+            if (cg->iter == 1) hist[0] = cg->r0;
+            hist[cg->iter] = sqrt(rr);
+        }
+        if (!(rr == rr)) { cg->status = CG_NAN; cg->done = 1; }
+        else if (sqrt(rr) < cg->tol_abs) {
+            if (cg->replace_every > 0) cg->cand = 1;
+            else { cg->status = CG_CONVERGED; cg->done = 1; }
+        } else if (cg->iter >= cg->max_iter && cg->replace_every == 0) {
+            cg->status = CG_MAXITER; cg->done = 1;
+        }
+    }
+}
+
+// Mixed mode fold over the whole padded array (x_lo is 0 outside fluid cells).
+template <class T>
+__global__ void k_fold_flat(long long n, double* xhi, T* xlo, const CGState* cg, int force) {
+    if (!force) {
+        if (cg->done) return;
+        if (!(cg->cand || (cg->replace_every > 0 && cg->iter > 0 &&
+                           cg->iter % cg->replace_every == 0)))
+            return;
+    }
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        const T v = xlo[t];
+        if (v != T(0)) {
+            xhi[t] += (double)v;
+            xlo[t] = T(0);
+        }
+    }
+}
+
+// Layout conversions between the reference's layout (gr) and the pitched one (g).
+template <int DIM, class T>
+__global__ void k_import(Geom g, Geom gr, const double* __restrict__ src, T* dst) {
+    for_cells<DIM>(g, [&](int i, int j, int k, int id) { dst[id] = (T)src[cidx(gr, i, j, k)]; });
+}
+template <int DIM>
+__global__ void k_import_mask(Geom g, Geom gr, const uint8_t* __restrict__ src, uint8_t* dst) {
+    for_cells<DIM>(g, [&](int i, int j, int k, int id) {
+        dst[id] = src[cidx(gr, i, j, k)] ? 1 : 0;
+    });
+}
+// dst (reference layout) = src on interior cells (overwrite) or += src (accumulate).
+template <int DIM, class T>
+__global__ void k_export(Geom g, Geom gr, const T* __restrict__ src, double* dst, int accumulate) {
+    for_cells<DIM>(g, [&](int i, int j, int k, int id) {
+        const int rid = cidx(gr, i, j, k);
+        dst[rid] = accumulate ? dst[rid] + (double)src[id] : (double)src[id];
+    });
+}
+
+// Cell codes of a level, one byte per cell: bit 6 the cell is an interior fluid
+// cell, bit 7 its colour ((i+j+k) odd), and on the finest level (fine = 1) bits
+// 0-5 whether its +x,-x,+y,-y,+z,-z neighbour is an interior fluid cell --
+// exactly when the reference's coupling exists (uaamg_preconditioner_3d.cpp:50-66).
+template <int DIM>
+__global__ void k_codes(Geom g, const uint8_t* __restrict__ s, uint8_t* code, int fine) {
+    for_cells<DIM>(g, [&](int i, int j, int k, int id) {
+        uint32_t c = ((i + j + k) & 1) ? kOdd : 0u;
+        if (!s[id]) {
+            c |= kActive;
+            if (fine) {
+                if (i < g.nx && !s[id + 1]) c |= 1u;
+                if (i > 1 && !s[id - 1]) c |= 2u;
+                if (j < g.ny && !s[id + g.sx]) c |= 4u;
+                if (j > 1 && !s[id - g.sx]) c |= 8u;
+                if (DIM == 3) {
+                    if (k < g.nz && !s[id + g.sxy]) c |= 16u;
+                    if (k > 1 && !s[id - g.sxy]) c |= 32u;
+                }
+            }
+        }
+        code[id] = (uint8_t)c;
+    });
+}
+
+// Diagonal of every fluid cell of a coarse level, in the reference's summation
+// order (uaamg_preconditioner_3d.cpp:113-119), plus the Dirichlet wall channel.
+template <int DIM, class T>
+__global__ void k_diag(Geom g, const uint8_t* __restrict__ s, const T* __restrict__ cx,
+                       const T* __restrict__ cy, const T* __restrict__ cz,
+                       const T* __restrict__ wd, T* dg) {
+    for_cells<DIM>(g, [&](int, int, int, int id) {
+        if (s[id]) return;
+        T d = cx[id] + cx[id - 1] + cy[id] + cy[id - g.sx];
+        if (DIM == 3) d = d + cz[id] + cz[id - g.sxy];
+        if (wd) d = d + wd[id];
+        dg[id] = d;
+    });
+}
+
+}  // namespace
+}  // namespace uaamg

@@ -115,7 +115,7 @@ class Handle:
         self._check(self.lib.uaamg_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
 
     def set_vcycle_kernels(self, sweeps: bool):
-        """False: fused V-cycle kernels (default); True: per-colour sweep kernels."""
+        """False: z-march V-cycle kernels (default); True: per-colour sweep kernels."""
         self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(bool(sweeps))), "vcycle")
 
     def set_dirichlet_walls(self, on: bool):
