@@ -40,14 +40,15 @@ uaamg_status cuda_fail(uaamg_handle* h, cudaError_t e, const char* where) {
     return fail(h, UAAMG_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-uaamg_status map_engine(uaamg_handle* h, int e, const char* where) {
+uaamg_status map_engine(uaamg_handle* h, int e, const char* where,
+                        const uaamg::Engine* eng = nullptr) {
     switch (e) {
         case uaamg::E_OK: return UAAMG_OK;
         case uaamg::E_OOM: return fail(h, UAAMG_OOM, std::string(where) + ": device allocation failed");
         case uaamg::E_ARG: return fail(h, UAAMG_INVALID_ARG, std::string(where) + ": invalid argument");
         case uaamg::E_NOPROB: return fail(h, UAAMG_NO_PROBLEM, std::string(where) + ": no problem set");
         default: {
-            cudaError_t ce = cudaGetLastError();
+            cudaError_t ce = eng && eng->cuda_error != cudaSuccess ? eng->cuda_error : cudaGetLastError();
             return fail(h, UAAMG_CUDA_ERROR, std::string(where) + ": CUDA error " +
                                                  (ce != cudaSuccess ? cudaGetErrorString(ce) : ""));
         }
@@ -81,7 +82,7 @@ uaamg_status engine_for(uaamg_handle* h, int p, uaamg::Engine** out) {
     if (!h->ready[p]) {
         int e = h->eng[p]->set_problem(h->dim, h->nx, h->ny, h->nz, h->dx, h->dy, h->dz,
                                        h->d_solid, h->dirichlet);
-        if (e != uaamg::E_OK) return map_engine(h, e, "hierarchy set-up");
+        if (e != uaamg::E_OK) return map_engine(h, e, "hierarchy set-up", h->eng[p]);
         h->ready[p] = true;
     }
     *out = h->eng[p];
@@ -162,7 +163,7 @@ uaamg_status solve_dev(uaamg_handle* h, const double* d_rhs, double* d_p, const 
     uaamg::SolveResult r;
     std::memset(&r, 0, sizeof(r));
     int e = eng->solve(a, &r);
-    if (e != uaamg::E_OK) return map_engine(h, e, "solve");
+    if (e != uaamg::E_OK) return map_engine(h, e, "solve", eng);
     if (eng->timed_out())
         return fail(h, UAAMG_TIMEOUT, "solve: a kernel gave up waiting for its tile loads");
     h->last_iters = r.iterations;
@@ -310,7 +311,7 @@ uaamg_status uaamg_precond_apply(uaamg_handle* h, int precision, const double* r
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_p, 0, bytes, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "upload");
     int ee = eng->precond_apply(h->d_rhs, h->d_p);
-    if (ee != uaamg::E_OK) return map_engine(h, ee, "precond_apply");
+    if (ee != uaamg::E_OK) return map_engine(h, ee, "precond_apply", eng);
     if (eng->timed_out())
         return fail(h, UAAMG_TIMEOUT, "precond_apply: a kernel gave up waiting for its tile loads");
     e = cudaMemcpyAsync(z, h->d_p, bytes, cudaMemcpyDeviceToHost, h->stream);

@@ -300,8 +300,11 @@ private:
     }
 
     int sync_check() {
-        cudaError_t e = cudaStreamSynchronize(st_);
+        cudaError_t e = cudaGetLastError();
+        const cudaError_t es = cudaStreamSynchronize(st_);
+        if (e == cudaSuccess) e = es;
         if (e == cudaSuccess) e = cudaGetLastError();
+        if (e != cudaSuccess) cuda_error = e;
         return e == cudaSuccess ? E_OK : E_CUDA;
     }
 
@@ -564,7 +567,7 @@ private:
         const LevelBuf<T>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : (DIM + 1.0) * t;
-        const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kMX, kMY);
+        const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
         UAAMG_LAUNCH_SMEM((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_smooth<DIM, T, FINE>),
                           grid, blk, (FwdCfg<DIM, T, FINE>::BYTES), maps<DIM>(l, false, false),
@@ -580,7 +583,7 @@ private:
         const LevelBuf<T>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : (DIM + 1.0) * t;
-        const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kMX, kMY);
+        const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
         UAAMG_LAUNCH_SMEM((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
                           (k_up_even<DIM, T, FINE>), grid, blk, (UpeCfg<DIM, T, FINE>::BYTES),
@@ -710,7 +713,7 @@ private:
         auto iteration = [&](bool from_p) {
             T* pnew = from_p ? p2_ : p_;
             UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
-                              (k_pmatvec<DIM, T>), pgrid, dim3(kMX, kMY), (PmvCfg<DIM, T>::BYTES),
+                              (k_pmatvec<DIM, T>), pgrid, dim3(kThreads), (PmvCfg<DIM, T>::BYTES),
                               pm[from_p ? 0 : 1], g, lv_[0].zc, pnew, ap_, st, partials_, cg_, err_);
             UAAMG_LAUNCH((KTag{K_UPDATE, 0, cells(g) * (6.0 * sizeof(T))}), k_update_flat<T>, ugrid, 256,
                          nvec, xlo_, r_, pnew, ap_, partials_, cg_, a.hist);
@@ -746,7 +749,7 @@ private:
                     ce = cudaStreamEndCapture(cap_, &graph);
                 }
                 st_ = saved;
-                if (ce != cudaSuccess || !graph) return E_CUDA;
+                if (ce != cudaSuccess || !graph) { cuda_error = ce != cudaSuccess ? ce : cudaErrorUnknown; return E_CUDA; }
                 ce = cudaGraphInstantiate(&gexec_, graph, 0);
                 cudaGraphDestroy(graph);
                 if (ce != cudaSuccess) { gexec_ = nullptr; return E_CUDA; }

@@ -54,6 +54,8 @@ struct KernelTime {
 class Engine {
 public:
     virtual ~Engine() {}
+    // The CUDA error behind the last E_CUDA result (cudaSuccess when none).
+    cudaError_t cuda_error = cudaSuccess;
     // Builds the level hierarchy for a padded level-0 mask already on the device.
     virtual int set_problem(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
                             const uint8_t* d_solid, int dirichlet) = 0;

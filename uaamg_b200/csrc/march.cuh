@@ -1,11 +1,14 @@
-// Stencil kernels that march along z through a level: a block owns a 32 x 8
-// column tile of (i, j) cells and walks a chunk of z planes; each plane of every
-// input array arrives as one TMA box (the tile plus a 1-cell ring) in a ring of
-// shared-memory stages, kept several planes ahead of the compute so that the
-// block always has loads in flight.  A z neighbour is the same column one
-// stage up or down, so nothing along z is loaded twice, and a cell's value
-// that needs a division (a pre-smoothed value) is computed once per plane into
-// a shared plane buffer that the in-plane neighbours read.
+// Stencil kernels that march along z through a level: a block owns a 32 x 16
+// column tile of (i, j) cells (256 threads, each owning an x-pair of cells -- one
+// of each colour -- so a warp never splits on the red-black parity) and walks a
+// chunk of z planes; each plane of every input array arrives as one TMA box (the tile plus
+// a 1-cell ring) in a ring of shared-memory stages, issued several planes ahead
+// of the compute so that the block always has loads in flight.  One thread waits
+// on the stage's mbarrier for the plane the next step needs and the step's block
+// barrier hands it to everyone.  A z neighbour is the same column one stage up
+// or down, so nothing along z is loaded twice, and a value that needs a division
+// (a pre-smoothed cell) is computed once per plane into a shared plane buffer
+// that the in-plane neighbours read.
 //
 // One V-cycle level = four marches (uaamg_preconditioner_3d.cpp:183-196):
 //   k_fwd_smooth   forward red-black sweep from x = 0 (smooth(L,1,false),
@@ -22,8 +25,9 @@
 // Finest level: the couplings are the constants 1/h^2 wherever the neighbour is
 // an interior fluid cell (uaamg_preconditioner_3d.cpp:50-66), and every other
 // neighbour holds x = 0, so c_n x_n = (1/h^2) x_n for every neighbour; the
-// diagonal comes from the cell-code bits in the reference's summation order.
-// Coarse levels read their Galerkin coefficients and diagonal from TMA boxes.
+// diagonal is a 64-entry table indexed by the cell-code neighbour bits, summed
+// in the reference's order.  Coarse levels read their Galerkin coefficients and
+// diagonal from TMA boxes.
 //
 // Arithmetic: every per-cell expression is the reference's, operand for operand
 // and in its order, including the division by the diagonal; with the FP64
@@ -37,13 +41,14 @@ namespace uaamg {
 namespace {
 
 constexpr uint32_t kActive = 64u, kOdd = 128u;
-constexpr int kMX = 32, kMY = 8;                   // column tile; one thread per column
-constexpr int kHalo = 2 * (kMX + 2) + 2 * kMY;     // cells of the 1-cell ring: 84
+constexpr int kMX = 32, kMY = 16;                  // column tile
+constexpr int kThreads = 256;                      // one thread per x-pair of the tile
+constexpr int kHaloOdd = 2 * (kMX / 2 + 1) + kMY;  // odd cells of the 1-cell ring: 50
 
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
 
-// Plane box of a level array: cells i in [i0-1, i0+32], j in [j0-1, j0+8] of one
-// plane, where i0 = 1 + 32 bx, j0 = 1 + 8 by.  The start column i0-1 = 32 bx sits
+// Plane box of a level array: cells i in [i0-1, i0+32], j in [j0-1, j0+16] of one
+// plane, where i0 = 1 + 32 bx, j0 = 1 + 16 by.  The start column i0-1 = 32 bx sits
 // on a 16-byte boundary for every element size; the width is padded to 16 bytes.
 template <class E>
 struct PBox {
@@ -53,7 +58,7 @@ struct PBox {
     static constexpr uint32_t BYTES = (uint32_t)(N * sizeof(E));
 };
 // Parent box: the next-coarser level's cells under a plane box, i.e. coarse
-// columns [16 bx, 16 bx + 17], rows [4 by, 4 by + 5] of coarse plane (k+1)/2.
+// columns [16 bx, 16 bx + 17], rows [8 by, 8 by + 9] of coarse plane (k+1)/2.
 template <class E>
 struct QBox {
     static constexpr int W = ((kMX / 2 + 2) * (int)sizeof(E) + 15) / 16 * 16 / (int)sizeof(E);
@@ -76,6 +81,15 @@ struct MPlan {
     static constexpr size_t STAGE = OFF_XC + (XC ? align128(QBox<T>::BYTES) : 0);
     static constexpr uint32_t TX_BYTES =
         NV * PBox<T>::BYTES + PBox<uint8_t>::BYTES + (XC ? QBox<T>::BYTES : 0);
+};
+
+// Shared memory of a march: 128 B of barriers, the diagonal table, S stages, then
+// `extra` bytes of plane buffers (plus 128 B of alignment slack up front).
+template <class T, int S, class P>
+struct MLayout {
+    static constexpr size_t OFF_LUT = 128;
+    static constexpr size_t OFF_RING = OFF_LUT + align128(64 * sizeof(T));
+    static constexpr size_t OFF_EXTRA = OFF_RING + S * P::STAGE;
 };
 
 // Tensor maps of one march, in the stage's slot order.
@@ -104,22 +118,29 @@ __device__ __forceinline__ E boxv(const unsigned char* st, size_t off, int q) {
     return reinterpret_cast<const E*>(st + off)[q];
 }
 
-// Ring position of the h-th cell of the 1-cell ring (h < kHalo).
-__device__ __forceinline__ void halo_cell(int h, int& a, int& r) {
-    if (h < kMX + 2) { a = h; r = 0; }
-    else if (h < 2 * (kMX + 2)) { a = h - (kMX + 2); r = kMY + 1; }
-    else if (h < 2 * (kMX + 2) + kMY) { a = 0; r = 1 + h - 2 * (kMX + 2); }
-    else { a = kMX + 1; r = 1 + h - 2 * (kMX + 2) - kMY; }
+// Box position of the h-th odd cell of the 1-cell ring (h < kHaloOdd), where the
+// box's corner cell (i0-1, j0-1, k) has parity s0: the odd cells of the bottom and
+// top rows (17 each), then of the left and right columns (8 each).
+__device__ __forceinline__ void halo_odd(int h, int s0, int& a, int& r) {
+    constexpr int R = kMX / 2 + 1;
+    if (h < R) { r = 0; a = 2 * h + (1 - s0); }
+    else if (h < 2 * R) { r = kMY + 1; a = 2 * (h - R) + s0; }
+    else if (h < 2 * R + kMY / 2) { a = 0; r = 1 + 2 * (h - 2 * R) + s0; }
+    else { a = kMX + 1; r = 1 + 2 * (h - 2 * R - kMY / 2) + (1 - s0); }
 }
 
-// Finest-level diagonal from the neighbour bits, summed in the reference's order
-// (uaamg_preconditioner_3d.cpp:72-74).
+// Finest-level diagonal table: entry c is the diagonal of a cell whose neighbour
+// bits are c, summed in the reference's order (uaamg_preconditioner_3d.cpp:72-74).
 template <int DIM, class T>
-__device__ __forceinline__ T fine_diag(uint32_t c, T idx2, T idy2, T idz2) {
-    T d = ((c & 1u) ? idx2 : T(0)) + ((c & 2u) ? idx2 : T(0)) + ((c & 4u) ? idy2 : T(0)) +
-          ((c & 8u) ? idy2 : T(0));
-    if (DIM == 3) d = d + ((c & 16u) ? idz2 : T(0)) + ((c & 32u) ? idz2 : T(0));
-    return d;
+__device__ __forceinline__ void build_lut(T* lut, T idx2, T idy2, T idz2) {
+    const int t = threadIdx.x + blockDim.x * threadIdx.y;
+    if (t < 64) {
+        const uint32_t c = (uint32_t)t;
+        T d = ((c & 1u) ? idx2 : T(0)) + ((c & 2u) ? idx2 : T(0)) + ((c & 4u) ? idy2 : T(0)) +
+              ((c & 8u) ? idy2 : T(0));
+        if (DIM == 3) d = d + ((c & 16u) ? idz2 : T(0)) + ((c & 32u) ? idz2 : T(0));
+        lut[t] = d;
+    }
 }
 
 // Dirichlet wall diagonal of a finest-level cell (as k_fine_coeffs).
@@ -135,12 +156,12 @@ __device__ __forceinline__ T wall_diag_at(const MLevel<T>& L, int i, int j, int 
     return w;
 }
 
-// Diagonal of the cell at box position q of stage st (cell (i, j, k)).
+// Diagonal of the cell with code c at box position q of stage st (cell (i, j, k)).
 template <int DIM, class T, class P, bool FINE>
-__device__ __forceinline__ T mdiag(const MLevel<T>& L, const unsigned char* st, uint32_t c, int q,
-                                   int i, int j, int k) {
+__device__ __forceinline__ T mdiag(const MLevel<T>& L, const T* lut, const unsigned char* st,
+                                   uint32_t c, int q, int i, int j, int k) {
     if constexpr (FINE) {
-        T d = fine_diag<DIM, T>(c, L.idx2, L.idy2, L.idz2);
+        T d = lut[c & 63u];
         if (L.dirichlet) d = d + wall_diag_at<DIM, T>(L, i, j, k);
         return d;
     } else {
@@ -184,15 +205,16 @@ __device__ __forceinline__ T nbsum(const T (&c)[6], const T* v, int q, T vp, T v
     return nb;
 }
 
-// Pre-smoothed value of the cell at box position q: an odd active cell smoothed
-// from x = 0 has x = (b + 0)/d (skipped, x = 0, when d < 1e-30); every other cell 0.
+// Pre-smoothed value of the cell at box position (a, r): an odd active cell
+// smoothed from x = 0 has x = (b + 0)/d (skipped, x = 0, when d < 1e-30); every
+// other cell 0.
 template <int DIM, class T, class P, bool FINE>
-__device__ __forceinline__ T presmooth(const MLevel<T>& L, const unsigned char* st, int a, int r,
-                                       int i, int j, int k) {
+__device__ __forceinline__ T presmooth(const MLevel<T>& L, const T* lut, const unsigned char* st,
+                                       int a, int r, int i, int j, int k) {
     const uint32_t c = st[P::OFF_CODE + r * PBox<uint8_t>::W + a];
     if ((c & (kActive | kOdd)) != (kActive | kOdd)) return T(0);
     const int q = r * PBox<T>::W + a;
-    const T d = mdiag<DIM, T, P, FINE>(L, st, c, q, i, j, k);
+    const T d = mdiag<DIM, T, P, FINE>(L, lut, st, c, q, i, j, k);
     if (d < T(1e-30)) return T(0);
     return (boxv<T>(st, P::QB * P::VB, q) + T(0)) / d;
 }
@@ -203,21 +225,6 @@ template <class T, class P>
 __device__ __forceinline__ T prolong_at(const unsigned char* st, int a, int r) {
     return T(2) * boxv<T>(st, P::OFF_XC, ((r + 1) >> 1) * QBox<T>::W + ((a + 1) >> 1));
 }
-
-// March bookkeeping shared by the kernels: planes p0 .. plast pass through S
-// stages; plane p uses stage (p - p0) % S for the ((p - p0) / S)-th time.
-template <int S>
-struct MRing {
-    uint64_t* bars;
-    unsigned char* base;
-    size_t stage;
-    int p0;
-    __device__ unsigned char* at(int p) const { return base + (size_t)((p - p0) % S) * stage; }
-    __device__ bool wait(int p) const {
-        const int u = p - p0;
-        return mbar_wait(&bars[u % S], (uint32_t)((u / S) & 1), kTmaWaitLimit);
-    }
-};
 
 template <int DIM, class P>
 __device__ __forceinline__ void issue_plane(const MarchMaps& M, unsigned char* st, uint64_t* bar,
@@ -231,65 +238,68 @@ __device__ __forceinline__ void issue_plane(const MarchMaps& M, unsigned char* s
     if constexpr (P::XCB) tma_load<DIM>(st + P::OFF_XC, &M.xc, x0 / 2, y0 / 2, (k + 1) >> 1, bar);
 }
 
-// Sets up the ring (thread 0 initialises the barriers and issues the first
-// planes) and returns it; all threads return after a barrier.
+// March bookkeeping: planes p0 .. plast pass through S stages; plane p uses stage
+// (p - p0) % S for the ((p - p0) / S)-th time.  Thread 0 issues every load and is
+// the only thread that waits on the stage barriers.
 template <int DIM, int S, class P>
-__device__ __forceinline__ MRing<S> ring_start(const MarchMaps& M, unsigned char* sm, int p0,
-                                               int plast) {
-    MRing<S> R;
-    R.bars = reinterpret_cast<uint64_t*>(sm);
-    R.base = sm + 128;
-    R.stage = P::STAGE;
-    R.p0 = p0;
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&R.bars[s], 1);
-        for (int p = p0; p < p0 + S && p <= plast; ++p)
-            issue_plane<DIM, P>(M, R.at(p), &R.bars[(p - p0) % S], p);
+struct MRing {
+    uint64_t* bars;
+    unsigned char* base;
+    int p0, plast;
+    __device__ unsigned char* at(int p) const { return base + (size_t)((p - p0) % S) * P::STAGE; }
+    __device__ bool wait(int p) const {
+        const int u = p - p0;
+        return mbar_wait(&bars[u % S], (uint32_t)((u / S) & 1), kTmaWaitLimit);
     }
-    __syncthreads();
-    return R;
+    // thread 0: barriers and the first S planes
+    __device__ void start(const MarchMaps& M) const {
+        for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        for (int p = p0; p < p0 + S && p <= plast; ++p) issue_plane<DIM, P>(M, at(p), &bars[(p - p0) % S], p);
+    }
+    // thread 0, after a block barrier: refill the stage of plane `freed`
+    __device__ void refill(const MarchMaps& M, int freed) const {
+        if (freed >= p0 && freed + S <= plast)
+            issue_plane<DIM, P>(M, at(freed + S), &bars[(freed - p0) % S], freed + S);
+    }
+};
+
+// Block-wide verdict on thread 0's waits; on a timeout the error word is set.
+__device__ __forceinline__ bool step_barrier(bool ok, int* err) {
+    if (__syncthreads_and(ok ? 1 : 0)) return true;
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(err, 1);
+    return false;
 }
 
-// End of a march step: one block-wide verdict on the waits of the step, then the
-// stage of plane `freed` is refilled with plane freed + S.
-template <int DIM, int S, class P>
-__device__ __forceinline__ bool ring_step(const MarchMaps& M, const MRing<S>& R, bool ok, int freed,
-                                          int plast, int* err) {
-    if (!__syncthreads_and(ok ? 1 : 0)) {
-        if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(err, 1);
-        return false;
-    }
-    if (threadIdx.x == 0 && threadIdx.y == 0 && freed >= R.p0 && freed + S <= plast)
-        issue_plane<DIM, P>(M, R.at(freed + S), &R.bars[(freed - R.p0) % S], freed + S);
-    return true;
-}
-
-// Dynamic shared memory of each march (ring + plane buffers + 128 B barriers + 128 B
-// alignment slack).
+// Per-march ring depth and dynamic shared-memory size.
 template <int DIM, class T, bool FINE> struct FwdCfg {
     using P = MPlan<DIM, T, false, !FINE, false>;
-    static constexpr int S = FINE ? 6 : 4;
-    static constexpr size_t BYTES = 256 + S * P::STAGE + 2 * align128(PBox<T>::BYTES);
+    static constexpr int S = FINE ? 8 : 4;
+    using Lay = MLayout<T, S, P>;
+    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
 template <int DIM, class T, bool FINE> struct ResCfg {
     using P = MPlan<DIM, T, true, !FINE, false>;
-    static constexpr int S = FINE ? 5 : 4;
-    static constexpr size_t BYTES = 256 + S * P::STAGE + align128(2 * kMX * kMY * sizeof(T));
+    static constexpr int S = FINE ? 6 : 4;
+    using Lay = MLayout<T, S, P>;
+    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA;
 };
 template <int DIM, class T, bool FINE> struct UpeCfg {
     using P = MPlan<DIM, T, false, !FINE, true>;
-    static constexpr int S = FINE ? 6 : 4;
-    static constexpr size_t BYTES = 256 + S * P::STAGE + 2 * align128(PBox<T>::BYTES);
+    static constexpr int S = FINE ? 8 : 4;
+    using Lay = MLayout<T, S, P>;
+    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
 template <int DIM, class T, bool FINE> struct UpoCfg {
     using P = MPlan<DIM, T, true, !FINE, false>;
-    static constexpr int S = FINE ? 5 : 4;
-    static constexpr size_t BYTES = 256 + S * P::STAGE;
+    static constexpr int S = FINE ? 6 : 4;
+    using Lay = MLayout<T, S, P>;
+    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA;
 };
 template <int DIM, class T> struct PmvCfg {
     using P = MPlan<DIM, T, true, false, false>;
-    static constexpr int S = 5;
-    static constexpr size_t BYTES = 256 + S * P::STAGE;
+    static constexpr int S = 6;
+    using Lay = MLayout<T, S, P>;
+    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA;
 };
 
 // z range of this block: planes kb .. ke-1 (3D); the single plane 0 (2D).
@@ -304,155 +314,223 @@ __device__ __forceinline__ void zrange(const Geom& g, int zc, int& kb, int& ke) 
     }
 }
 
+// The thread's x-pair: cells A = (i, j) and B = (i + 1, j) of tile row r (lanes
+// 0-15 of warp w take row 2w, lanes 16-31 row 2w + 1).  i is odd, so A and B have
+// opposite colours on every plane.
+struct Pair {
+    int i, j, w, pp;  // cell A; warp; pair index within the row
+    int a, rb;        // box column of A, box row
+    int qa, ca;       // box positions of A in the value and code boxes (B: +1)
+    bool ina, inb;    // inside the level
+    int gid;          // cidx(g, i, j, 0)
+};
+
+template <class T>
+__device__ __forceinline__ Pair own_pair(const Geom& g) {
+    Pair o;
+    const int t = threadIdx.x, l = t & 31;
+    o.w = t >> 5;
+    o.pp = l & 15;
+    const int r = 2 * o.w + (l >> 4);
+    o.i = 1 + kMX * (int)blockIdx.x + 2 * o.pp;
+    o.j = 1 + kMY * (int)blockIdx.y + r;
+    o.a = 2 * o.pp + 1;
+    o.rb = r + 1;
+    o.qa = o.rb * PBox<T>::W + o.a;
+    o.ca = o.rb * PBox<uint8_t>::W + o.a;
+    o.ina = o.i <= g.nx && o.j <= g.ny;
+    o.inb = o.i + 1 <= g.nx && o.j <= g.ny;
+    o.gid = o.i + o.j * g.sx;
+    return o;
+}
+
 // ---------------------------------------------------------------------------
 // Forward sweep from x = 0: x = (b + 0)/d on odd cells, then
 // x = (b + sum c_n x_n)/d on even cells; writes x on every interior cell.
+// Step k builds plane k+1's odd values (own pair + the ring's odd cells) into a
+// plane buffer and smooths the even cells of plane k from plane k's buffer and the
+// odd values of the cell's own column one plane up and down (registers).
 template <int DIM, class T, bool FINE>
-__global__ void __launch_bounds__(256) k_fwd_smooth(const __grid_constant__ MarchMaps M,
-                                                    MLevel<T> L, T* __restrict__ x,
-                                                    const int* __restrict__ done, int* err) {
+__global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__ MarchMaps M,
+                                                         MLevel<T> L, T* __restrict__ x,
+                                                         const int* __restrict__ done, int* err) {
     if (done && *done) return;
     using C = FwdCfg<DIM, T, FINE>;
     using P = typename C::P;
-    constexpr int S = C::S, W = PBox<T>::W, N = PBox<T>::N;
+    using Lay = typename C::Lay;
+    constexpr int S = C::S, N = PBox<T>::N, W = PBox<T>::W;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* sm = aligned_smem(smem_raw);
-    T* Yb = reinterpret_cast<T*>(sm + 128 + S * P::STAGE);
+    T* lut = reinterpret_cast<T*>(sm + Lay::OFF_LUT);
+    T* Yb = reinterpret_cast<T*>(sm + Lay::OFF_EXTRA);
     const Geom& g = L.g;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kMX * ty;
-    const int i = 1 + kMX * (int)blockIdx.x + tx, j = 1 + kMY * (int)blockIdx.y + ty;
-    const bool own = i <= g.nx && j <= g.ny;
-    const int q = (ty + 1) * W + tx + 1;
-    int ha = 0, hr = 0;
-    if (tid < kHalo) halo_cell(tid, ha, hr);
-    const int hq = hr * W + ha, hi = i - tx - 1 + ha, hj = j - ty - 1 + hr;
+    const int tid = threadIdx.x;
+    const Pair o = own_pair<T>(g);
+    const int ib = kMX * (int)blockIdx.x, jb = kMY * (int)blockIdx.y;  // box corner cell
     int kb, ke;
     zrange<DIM>(g, L.zc, kb, ke);
-    const int p0 = DIM == 3 ? kb - 1 : 0, plast = DIM == 3 ? ke : 0;
-    MRing<S> R = ring_start<DIM, S, P>(M, sm, p0, plast);
-    bool ok = R.wait(p0);
-    // y: pre-smoothed values of this column at planes k-1, k, k+1
-    T ym = T(0), y0 = T(0), yp = T(0);
-    if (DIM == 3) y0 = presmooth<DIM, T, P, FINE>(L, R.at(p0), tx + 1, ty + 1, i, j, p0);
+    MRing<DIM, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING,
+                       DIM == 3 ? kb - 1 : 0, DIM == 3 ? ke : 0};
+    if (FINE) build_lut<DIM, T>(lut, L.idx2, L.idy2, L.idz2);
+    bool ok = true;
+    if (tid == 0) {
+        R.start(M);
+        ok = R.wait(R.p0) && (DIM == 2 || R.wait(R.p0 + 1));
+    }
+    if (!step_barrier(ok, err)) return;
+    // odd value of the pair at plane p, placed in its column (0: A, 1: B)
+    auto odd_pair = [&](int p, T (&y)[2]) -> T {
+        const int bo = 1 - ((o.i + o.j + p) & 1);
+        const T v = presmooth<DIM, T, P, FINE>(L, lut, R.at(p), o.a + bo, o.rb, o.i + bo, o.j, p);
+        y[0] = bo ? T(0) : v;
+        y[1] = bo ? v : T(0);
+        return v;
+    };
+    T ym[2] = {T(0), T(0)}, y0[2] = {T(0), T(0)}, yp[2] = {T(0), T(0)};
+    if (DIM == 3) odd_pair(R.p0, y0);
 #pragma unroll 1
-    for (int k = p0; k < ke; ++k) {
-        const int kn = DIM == 3 ? k + 1 : 0;  // plane whose y plane is built this step
-        if (DIM == 3) ok &= R.wait(kn);
+    for (int k = R.p0; k < ke; ++k) {
+        const int kn = DIM == 3 ? k + 1 : 0;  // plane whose odd values are built this step
         {
-            const unsigned char* sn = R.at(kn);
             T* Yn = Yb + (kn & 1) * N;
-            yp = presmooth<DIM, T, P, FINE>(L, sn, tx + 1, ty + 1, i, j, kn);
-            Yn[q] = yp;
-            if (tid < kHalo) Yn[hq] = presmooth<DIM, T, P, FINE>(L, sn, ha, hr, hi, hj, kn);
+            const T v = odd_pair(kn, yp);
+            Yn[o.qa + (1 - ((o.i + o.j + kn) & 1))] = v;
+            if (tid < kHaloOdd) {
+                int a, r;
+                halo_odd(tid, (ib + jb + kn) & 1, a, r);
+                Yn[r * W + a] = presmooth<DIM, T, P, FINE>(L, lut, R.at(kn), a, r, ib + a, jb + r, kn);
+            }
         }
         if (DIM == 2) {
-            y0 = yp;
+            y0[0] = yp[0];
+            y0[1] = yp[1];
             __syncthreads();
         }
         if (k >= kb) {
             const unsigned char* sc = R.at(k);
-            const uint32_t c = sc[P::OFF_CODE + (ty + 1) * PBox<uint8_t>::W + tx + 1];
-            T xv = T(0);
+            const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
+            const T* Yc = Yb + (k & 1) * N;
+            const int e = (o.i + o.j + k) & 1;  // column of the even cell
+            const int q = o.qa + e;
+            const uint32_t c = sc[P::OFF_CODE + o.ca + e];
+            T xe = T(0);
             if (c & kActive) {
-                if (c & kOdd) {
-                    xv = y0;
-                } else {
-                    const T d = mdiag<DIM, T, P, FINE>(L, sc, c, q, i, j, k);
-                    if (!(d < T(1e-30))) {
-                        T cc[6];
-                        mcoup<DIM, T, P, FINE>(L, sc, DIM == 3 ? R.at(k - 1) : sc, q, cc);
-                        const T* Yc = Yb + (k & 1) * N;
-                        xv = (boxv<T>(sc, P::QB * P::VB, q) + nbsum<DIM, T>(cc, Yc, q, yp, ym)) / d;
-                    }
+                const T d = mdiag<DIM, T, P, FINE>(L, lut, sc, c, q, o.i + e, o.j, k);
+                if (!(d < T(1e-30))) {
+                    T cc[6];
+                    mcoup<DIM, T, P, FINE>(L, sc, sb, q, cc);
+                    xe = (boxv<T>(sc, P::QB * P::VB, q) +
+                          nbsum<DIM, T>(cc, Yc, q, e ? yp[1] : yp[0], e ? ym[1] : ym[0])) / d;
                 }
             }
-            if (own) x[cidx(g, i, j, k)] = xv;
+            const int base = o.gid + k * g.sxy;
+            if (o.ina) x[base] = e ? y0[0] : xe;
+            if (o.inb) x[base + 1] = e ? xe : y0[1];
         }
         if (DIM == 2) break;
-        ym = y0;
-        y0 = yp;
-        if (!ring_step<DIM, S, P>(M, R, ok, k - 1, plast, err)) return;
+        ym[0] = y0[0]; ym[1] = y0[1];
+        y0[0] = yp[0]; y0[1] = yp[1];
+        if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
+        if (!step_barrier(ok, err)) return;
+        if (tid == 0) R.refill(M, k - 1);
     }
-    if (DIM == 2 && !__syncthreads_and(ok ? 1 : 0) && tid == 0) atomicExch(err, 1);
 }
 
 // Residual r = b - A x of every fluid cell and its restriction
-// b_c = sum over the 2x2(x2) children, in the reference's (di, dj, dk) order; the
-// children of a coarse cell sit in two adjacent columns, two adjacent rows and
-// two consecutive planes of one block, and meet in shared memory.
+// b_c = sum over the 2x2(x2) children in the reference's (di, dj, dk) order.  A
+// thread's pair is the di = 0, 1 children of one coarse column; the dj = 1 row is
+// the same lane of the other half-warp; dk = 0, 1 are consecutive planes.
 template <int DIM, class T, bool FINE>
-__global__ void __launch_bounds__(256) k_restrict_res(const __grid_constant__ MarchMaps M,
-                                                      MLevel<T> L, const uint8_t* __restrict__ ccode,
-                                                      T* __restrict__ cb,
-                                                      const int* __restrict__ done, int* err) {
+__global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant__ MarchMaps M,
+                                                           MLevel<T> L,
+                                                           const uint8_t* __restrict__ ccode,
+                                                           T* __restrict__ cb,
+                                                           const int* __restrict__ done, int* err) {
     if (done && *done) return;
     using C = ResCfg<DIM, T, FINE>;
     using P = typename C::P;
+    using Lay = typename C::Lay;
     constexpr int S = C::S, W = PBox<T>::W;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* sm = aligned_smem(smem_raw);
-    T* Rb = reinterpret_cast<T*>(sm + 128 + S * P::STAGE);  // [ty][tx][dk]
+    T* lut = reinterpret_cast<T*>(sm + Lay::OFF_LUT);
     const Geom& g = L.g;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kMX * ty;
-    const int i = 1 + kMX * (int)blockIdx.x + tx, j = 1 + kMY * (int)blockIdx.y + ty;
-    const int q = (ty + 1) * W + tx + 1;
+    const int tid = threadIdx.x;
+    const Pair o = own_pair<T>(g);
     int kb, ke;
     zrange<DIM>(g, L.zc, kb, ke);
-    const int p0 = DIM == 3 ? kb - 1 : 0, plast = DIM == 3 ? ke : 0;
-    MRing<S> R = ring_start<DIM, S, P>(M, sm, p0, plast);
-    bool ok = R.wait(p0);
-    if (DIM == 3) ok &= R.wait(kb);
-    T rlo = T(0);
+    MRing<DIM, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING,
+                       DIM == 3 ? kb - 1 : 0, DIM == 3 ? ke : 0};
+    if (FINE) build_lut<DIM, T>(lut, L.idx2, L.idy2, L.idz2);
+    bool ok = true;
+    if (tid == 0) {
+        R.start(M);
+        ok = R.wait(R.p0) && (DIM == 2 || (R.wait(kb) && R.wait(kb + 1)));
+    }
+    if (!step_barrier(ok, err)) return;
+    const int ic = kMX / 2 * (int)blockIdx.x + 1 + o.pp;
+    const int jc = kMY / 2 * (int)blockIdx.y + 1 + o.w;
+    const bool writer = (threadIdx.x & 16) == 0 && ic <= L.cg.nx && jc <= L.cg.ny;
+    T rlo[2] = {T(0), T(0)};
 #pragma unroll 1
     for (int k = kb; k < ke; ++k) {
-        if (DIM == 3) ok &= R.wait(k + 1);
         const unsigned char* sc = R.at(k);
-        const uint32_t c = sc[P::OFF_CODE + (ty + 1) * PBox<uint8_t>::W + tx + 1];
-        T rv = T(0);
-        if (c & kActive) {
-            const T* xb = reinterpret_cast<const T*>(sc + P::QX * P::VB);
-            const T d = mdiag<DIM, T, P, FINE>(L, sc, c, q, i, j, k);
-            T cc[6];
-            mcoup<DIM, T, P, FINE>(L, sc, DIM == 3 ? R.at(k - 1) : sc, q, cc);
-            T ax = d * xb[q] - cc[0] * xb[q + 1] - cc[1] * xb[q - 1] - cc[2] * xb[q + W] -
-                   cc[3] * xb[q - W];
-            if (DIM == 3)
-                ax = ax - cc[4] * boxv<T>(R.at(k + 1), P::QX * P::VB, q) -
-                     cc[5] * boxv<T>(R.at(k - 1), P::QX * P::VB, q);
-            rv = boxv<T>(sc, P::QB * P::VB, q) - ax;
+        const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
+        const unsigned char* su = DIM == 3 ? R.at(k + 1) : sc;
+        const T* xb = reinterpret_cast<const T*>(sc + P::QX * P::VB);
+        T rv[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int q = o.qa + e;
+            const uint32_t c = sc[P::OFF_CODE + o.ca + e];
+            rv[e] = T(0);
+            if (c & kActive) {
+                const T d = mdiag<DIM, T, P, FINE>(L, lut, sc, c, q, o.i + e, o.j, k);
+                T cc[6];
+                mcoup<DIM, T, P, FINE>(L, sc, sb, q, cc);
+                T ax = d * xb[q] - cc[0] * xb[q + 1] - cc[1] * xb[q - 1] - cc[2] * xb[q + W] -
+                       cc[3] * xb[q - W];
+                if (DIM == 3)
+                    ax = ax - cc[4] * boxv<T>(su, P::QX * P::VB, q) -
+                         cc[5] * boxv<T>(sb, P::QX * P::VB, q);
+                rv[e] = boxv<T>(sc, P::QB * P::VB, q) - ax;
+            }
         }
-        // children with dk = 0 live on odd planes (k = 2 kc - 1); the pair is complete
+        // children with dk = 0 live on odd planes (k = 2 kc - 1); the set is complete
         // on the even plane that follows
-        const bool pair = DIM == 2 || (k & 1) == 0;
-        if (DIM == 3 && !pair) rlo = rv;
-        if (pair) {
-            Rb[2 * tid] = DIM == 3 ? rlo : rv;
-            Rb[2 * tid + 1] = rv;
-        }
-        if (DIM == 3) {
-            if (!ring_step<DIM, S, P>(M, R, ok, k - 1, plast, err)) return;
-        } else if (!__syncthreads_and(ok ? 1 : 0)) {
-            if (tid == 0) atomicExch(err, 1);
-            return;
-        }
-        if (pair && tid < (kMX / 2) * (kMY / 2)) {
-            const int ca = tid % (kMX / 2), cr = tid / (kMX / 2);
-            const int ic = kMX / 2 * (int)blockIdx.x + 1 + ca;
-            const int jc = kMY / 2 * (int)blockIdx.y + 1 + cr;
-            const int kc = DIM == 3 ? k / 2 : 0;
-            if (ic <= L.cg.nx && jc <= L.cg.ny) {
+        if (DIM == 3 && (k & 1)) {
+            rlo[0] = rv[0];
+            rlo[1] = rv[1];
+        } else {
+            T pr[2][2];  // the dj = 1 partner's values [di][dk]
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                pr[e][0] = __shfl_down_sync(0xffffffffu, DIM == 3 ? rlo[e] : rv[e], 16);
+                pr[e][1] = __shfl_down_sync(0xffffffffu, rv[e], 16);
+            }
+            if (writer) {
+                const int kc = DIM == 3 ? k / 2 : 0;
                 const int cid = cidx(L.cg, ic, jc, kc);
                 T s = T(0);
-                for (int di = 0; di < 2; ++di)
-                    for (int dj = 0; dj < 2; ++dj) {
-                        const int t = (2 * cr + dj) * kMX + 2 * ca + di;
-                        s += Rb[2 * t];
-                        if (DIM == 3) s += Rb[2 * t + 1];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    if (DIM == 3) {
+                        s += rlo[e];
+                        s += rv[e];
+                        s += pr[e][0];
+                        s += pr[e][1];
+                    } else {
+                        s += rv[e];
+                        s += pr[e][1];
                     }
+                }
                 cb[cid] = (ccode[cid] & kActive) ? s : T(0);
             }
         }
-        // Rb is rewritten two steps later, after another block-wide barrier
+        if (DIM == 2) break;
+        if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
+        if (!step_barrier(ok, err)) return;
+        if (tid == 0) R.refill(M, k - 1);
     }
 }
 
@@ -461,143 +539,177 @@ __global__ void __launch_bounds__(256) k_restrict_res(const __grid_constant__ Ma
 // smoothed from those: x = (b + sum c_n x_n)/d (a skipped even cell keeps
 // 0 + 2 x_c).  Writes x on every interior cell.
 template <int DIM, class T, bool FINE>
-__global__ void __launch_bounds__(256) k_up_even(const __grid_constant__ MarchMaps M, MLevel<T> L,
-                                                 T* __restrict__ x, const int* __restrict__ done,
-                                                 int* err) {
+__global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ MarchMaps M,
+                                                      MLevel<T> L, T* __restrict__ x,
+                                                      const int* __restrict__ done, int* err) {
     if (done && *done) return;
     using C = UpeCfg<DIM, T, FINE>;
     using P = typename C::P;
-    constexpr int S = C::S, W = PBox<T>::W, N = PBox<T>::N;
+    using Lay = typename C::Lay;
+    constexpr int S = C::S, N = PBox<T>::N, W = PBox<T>::W;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* sm = aligned_smem(smem_raw);
-    T* Yb = reinterpret_cast<T*>(sm + 128 + S * P::STAGE);
+    T* lut = reinterpret_cast<T*>(sm + Lay::OFF_LUT);
+    T* Yb = reinterpret_cast<T*>(sm + Lay::OFF_EXTRA);
     const Geom& g = L.g;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kMX * ty;
-    const int i = 1 + kMX * (int)blockIdx.x + tx, j = 1 + kMY * (int)blockIdx.y + ty;
-    const bool own = i <= g.nx && j <= g.ny;
-    const int q = (ty + 1) * W + tx + 1;
-    int ha = 0, hr = 0;
-    if (tid < kHalo) halo_cell(tid, ha, hr);
-    const int hq = hr * W + ha, hi = i - tx - 1 + ha, hj = j - ty - 1 + hr;
-    // odd cells: pre-smoothed value + prolongation; others 0
-    auto oddval = [&](const unsigned char* st, int qq, int a, int r, int ci, int cj, int ck) -> T {
+    const int tid = threadIdx.x;
+    const Pair o = own_pair<T>(g);
+    const int ib = kMX * (int)blockIdx.x, jb = kMY * (int)blockIdx.y;
+    // odd cell at box position (a, r): pre-smoothed value + prolongation (0 if not
+    // an active odd cell)
+    auto oddval = [&](const unsigned char* st, int a, int r, int ci, int cj, int ck) -> T {
         const uint32_t c = st[P::OFF_CODE + r * PBox<uint8_t>::W + a];
         if ((c & (kActive | kOdd)) != (kActive | kOdd)) return T(0);
-        const T d = mdiag<DIM, T, P, FINE>(L, st, c, qq, ci, cj, ck);
+        const int qq = r * W + a;
+        const T d = mdiag<DIM, T, P, FINE>(L, lut, st, c, qq, ci, cj, ck);
         const T pre = d < T(1e-30) ? T(0) : (boxv<T>(st, P::QB * P::VB, qq) + T(0)) / d;
         return pre + prolong_at<T, P>(st, a, r);
     };
     int kb, ke;
     zrange<DIM>(g, L.zc, kb, ke);
-    const int p0 = DIM == 3 ? kb - 1 : 0, plast = DIM == 3 ? ke : 0;
-    MRing<S> R = ring_start<DIM, S, P>(M, sm, p0, plast);
-    bool ok = R.wait(p0);
-    T ym = T(0), y0 = T(0), yp = T(0);
-    if (DIM == 3) y0 = oddval(R.at(p0), q, tx + 1, ty + 1, i, j, p0);
+    MRing<DIM, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING,
+                       DIM == 3 ? kb - 1 : 0, DIM == 3 ? ke : 0};
+    if (FINE) build_lut<DIM, T>(lut, L.idx2, L.idy2, L.idz2);
+    bool ok = true;
+    if (tid == 0) {
+        R.start(M);
+        ok = R.wait(R.p0) && (DIM == 2 || R.wait(R.p0 + 1));
+    }
+    if (!step_barrier(ok, err)) return;
+    auto odd_pair = [&](int p, T (&y)[2]) -> T {
+        const int bo = 1 - ((o.i + o.j + p) & 1);
+        const T v = oddval(R.at(p), o.a + bo, o.rb, o.i + bo, o.j, p);
+        y[0] = bo ? T(0) : v;
+        y[1] = bo ? v : T(0);
+        return v;
+    };
+    T ym[2] = {T(0), T(0)}, y0[2] = {T(0), T(0)}, yp[2] = {T(0), T(0)};
+    if (DIM == 3) odd_pair(R.p0, y0);
 #pragma unroll 1
-    for (int k = p0; k < ke; ++k) {
+    for (int k = R.p0; k < ke; ++k) {
         const int kn = DIM == 3 ? k + 1 : 0;
-        if (DIM == 3) ok &= R.wait(kn);
         {
-            const unsigned char* sn = R.at(kn);
             T* Yn = Yb + (kn & 1) * N;
-            yp = oddval(sn, q, tx + 1, ty + 1, i, j, kn);
-            Yn[q] = yp;
-            if (tid < kHalo) Yn[hq] = oddval(sn, hq, ha, hr, hi, hj, kn);
+            const T v = odd_pair(kn, yp);
+            Yn[o.qa + (1 - ((o.i + o.j + kn) & 1))] = v;
+            if (tid < kHaloOdd) {
+                int a, r;
+                halo_odd(tid, (ib + jb + kn) & 1, a, r);
+                Yn[r * W + a] = oddval(R.at(kn), a, r, ib + a, jb + r, kn);
+            }
         }
         if (DIM == 2) {
-            y0 = yp;
+            y0[0] = yp[0];
+            y0[1] = yp[1];
             __syncthreads();
         }
         if (k >= kb) {
             const unsigned char* sc = R.at(k);
-            const uint32_t c = sc[P::OFF_CODE + (ty + 1) * PBox<uint8_t>::W + tx + 1];
-            T xv = T(0);
+            const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
+            const T* Yc = Yb + (k & 1) * N;
+            const int e = (o.i + o.j + k) & 1;
+            const int q = o.qa + e;
+            const uint32_t c = sc[P::OFF_CODE + o.ca + e];
+            T xe = T(0);
             if (c & kActive) {
-                if (c & kOdd) {
-                    xv = y0;
+                const T d = mdiag<DIM, T, P, FINE>(L, lut, sc, c, q, o.i + e, o.j, k);
+                if (d < T(1e-30)) {
+                    xe = T(0) + prolong_at<T, P>(sc, o.a + e, o.rb);
                 } else {
-                    const T d = mdiag<DIM, T, P, FINE>(L, sc, c, q, i, j, k);
-                    if (d < T(1e-30)) {
-                        xv = T(0) + prolong_at<T, P>(sc, tx + 1, ty + 1);
-                    } else {
-                        T cc[6];
-                        mcoup<DIM, T, P, FINE>(L, sc, DIM == 3 ? R.at(k - 1) : sc, q, cc);
-                        const T* Yc = Yb + (k & 1) * N;
-                        xv = (boxv<T>(sc, P::QB * P::VB, q) + nbsum<DIM, T>(cc, Yc, q, yp, ym)) / d;
-                    }
+                    T cc[6];
+                    mcoup<DIM, T, P, FINE>(L, sc, sb, q, cc);
+                    xe = (boxv<T>(sc, P::QB * P::VB, q) +
+                          nbsum<DIM, T>(cc, Yc, q, e ? yp[1] : yp[0], e ? ym[1] : ym[0])) / d;
                 }
             }
-            if (own) x[cidx(g, i, j, k)] = xv;
+            const int base = o.gid + k * g.sxy;
+            if (o.ina) x[base] = e ? y0[0] : xe;
+            if (o.inb) x[base + 1] = e ? xe : y0[1];
         }
         if (DIM == 2) break;
-        ym = y0;
-        y0 = yp;
-        if (!ring_step<DIM, S, P>(M, R, ok, k - 1, plast, err)) return;
+        ym[0] = y0[0]; ym[1] = y0[1];
+        y0[0] = yp[0]; y0[1] = yp[1];
+        if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
+        if (!step_barrier(ok, err)) return;
+        if (tid == 0) R.refill(M, k - 1);
     }
-    if (DIM == 2 && !__syncthreads_and(ok ? 1 : 0) && tid == 0) atomicExch(err, 1);
 }
 
 // Second (odd) colour of the reverse sweep, in place: odd cells read only even
 // neighbours, which this kernel does not write.  ZDOT (finest level): also the
 // fluid sums of z, r*z and r (r = this level's b) and the CG's projection / beta.
 template <int DIM, class T, bool FINE, bool ZDOT>
-__global__ void __launch_bounds__(256) k_up_odd(const __grid_constant__ MarchMaps M, MLevel<T> L,
-                                                T* x, const int* __restrict__ done, int* err,
-                                                double* partials, CGState* cg) {
+__global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ MarchMaps M,
+                                                     MLevel<T> L, T* x,
+                                                     const int* __restrict__ done, int* err,
+                                                     double* partials, CGState* cg) {
     if (done && *done) return;
     using C = UpoCfg<DIM, T, FINE>;
     using P = typename C::P;
-    constexpr int S = C::S, W = PBox<T>::W;
+    using Lay = typename C::Lay;
+    constexpr int S = C::S;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* sm = aligned_smem(smem_raw);
+    T* lut = reinterpret_cast<T*>(sm + Lay::OFF_LUT);
     const Geom& g = L.g;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i = 1 + kMX * (int)blockIdx.x + tx, j = 1 + kMY * (int)blockIdx.y + ty;
-    const bool own = i <= g.nx && j <= g.ny;
-    const int q = (ty + 1) * W + tx + 1;
+    const int tid = threadIdx.x;
+    const Pair o = own_pair<T>(g);
     double acc[3] = {0.0, 0.0, 0.0};
     int kb, ke;
     zrange<DIM>(g, L.zc, kb, ke);
-    const int p0 = DIM == 3 ? kb - 1 : 0, plast = DIM == 3 ? ke : 0;
-    MRing<S> R = ring_start<DIM, S, P>(M, sm, p0, plast);
-    bool ok = R.wait(p0);
-    if (DIM == 3) ok &= R.wait(kb);
-    bool failed = false;
+    MRing<DIM, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING,
+                       DIM == 3 ? kb - 1 : 0, DIM == 3 ? ke : 0};
+    if (FINE) build_lut<DIM, T>(lut, L.idx2, L.idy2, L.idz2);
+    bool ok = true;
+    if (tid == 0) {
+        R.start(M);
+        ok = R.wait(R.p0) && (DIM == 2 || (R.wait(kb) && R.wait(kb + 1)));
+    }
+    if (!step_barrier(ok, err)) return;
 #pragma unroll 1
     for (int k = kb; k < ke; ++k) {
-        if (DIM == 3) ok &= R.wait(k + 1);
         const unsigned char* sc = R.at(k);
-        const uint32_t c = sc[P::OFF_CODE + (ty + 1) * PBox<uint8_t>::W + tx + 1];
-        if (c & kActive) {
-            const T* xb = reinterpret_cast<const T*>(sc + P::QX * P::VB);
-            T xv = xb[q];
-            if (c & kOdd) {
-                const T d = mdiag<DIM, T, P, FINE>(L, sc, c, q, i, j, k);
+        const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
+        const unsigned char* su = DIM == 3 ? R.at(k + 1) : sc;
+        const T* xb = reinterpret_cast<const T*>(sc + P::QX * P::VB);
+        const int od = 1 - ((o.i + o.j + k) & 1);  // column of the odd cell
+        T za = xb[o.qa], zb = xb[o.qa + 1];
+        const uint32_t ca = sc[P::OFF_CODE + o.ca], cbb = sc[P::OFF_CODE + o.ca + 1];
+        {
+            const int q = o.qa + od;
+            const uint32_t c = od ? cbb : ca;
+            if (c & kActive) {
+                const T d = mdiag<DIM, T, P, FINE>(L, lut, sc, c, q, o.i + od, o.j, k);
                 if (!(d < T(1e-30))) {
                     T cc[6];
-                    mcoup<DIM, T, P, FINE>(L, sc, DIM == 3 ? R.at(k - 1) : sc, q, cc);
-                    const T vp = DIM == 3 ? boxv<T>(R.at(k + 1), P::QX * P::VB, q) : T(0);
-                    const T vm = DIM == 3 ? boxv<T>(R.at(k - 1), P::QX * P::VB, q) : T(0);
-                    xv = (boxv<T>(sc, P::QB * P::VB, q) + nbsum<DIM, T>(cc, xb, q, vp, vm)) / d;
-                    if (own) x[cidx(g, i, j, k)] = xv;
+                    mcoup<DIM, T, P, FINE>(L, sc, sb, q, cc);
+                    const T vp = DIM == 3 ? boxv<T>(su, P::QX * P::VB, q) : T(0);
+                    const T vm = DIM == 3 ? boxv<T>(sb, P::QX * P::VB, q) : T(0);
+                    const T xv = (boxv<T>(sc, P::QB * P::VB, q) + nbsum<DIM, T>(cc, xb, q, vp, vm)) / d;
+                    if (od) zb = xv; else za = xv;
+                    if (od ? o.inb : o.ina) x[o.gid + k * g.sxy + od] = xv;
                 }
             }
-            if (ZDOT && own) {
-                const double zv = (double)xv, rv = (double)boxv<T>(sc, P::QB * P::VB, q);
-                acc[0] += zv;
-                acc[1] += rv * zv;
-                acc[2] += rv;
+        }
+        if (ZDOT) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const uint32_t c = e ? cbb : ca;
+                if ((c & kActive) && (e ? o.inb : o.ina)) {
+                    const double zv = (double)(e ? zb : za);
+                    const double rv = (double)boxv<T>(sc, P::QB * P::VB, o.qa + e);
+                    acc[0] += zv;
+                    acc[1] += rv * zv;
+                    acc[2] += rv;
+                }
             }
         }
-        if (DIM == 3) {
-            if (!ring_step<DIM, S, P>(M, R, ok, k - 1, plast, err)) { failed = true; break; }
-        } else if (!__syncthreads_and(ok ? 1 : 0)) {
-            if (tx == 0 && ty == 0) atomicExch(err, 1);
-            failed = true;
-        }
+        if (DIM == 2) break;
+        if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
+        if (!step_barrier(ok, err)) return;
+        if (tid == 0) R.refill(M, k - 1);
     }
-    if (ZDOT && !failed) {
+    if (ZDOT) {
         double tot[3];
         if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
     }
@@ -610,68 +722,74 @@ __global__ void __launch_bounds__(256) k_up_odd(const __grid_constant__ MarchMap
 // reduced and the last block sets alpha = rz_old / p.Ap or stops on breakdown
 // (pcg_3d.cpp:94-99).  p_old and p_new are distinct buffers.
 template <int DIM, class T>
-__global__ void __launch_bounds__(256) k_pmatvec(const __grid_constant__ MarchMaps M, Geom g,
-                                                 int zc, T* __restrict__ pnew, T* __restrict__ ap,
-                                                 Stencil st, double* partials, CGState* cg,
-                                                 int* err) {
+__global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ MarchMaps M, Geom g,
+                                                      int zc, T* __restrict__ pnew,
+                                                      T* __restrict__ ap, Stencil st,
+                                                      double* partials, CGState* cg, int* err) {
     if (cg->done) return;
     using C = PmvCfg<DIM, T>;
     using P = typename C::P;
+    using Lay = typename C::Lay;
     constexpr int S = C::S, W = PBox<T>::W;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* sm = aligned_smem(smem_raw);
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i = 1 + kMX * (int)blockIdx.x + tx, j = 1 + kMY * (int)blockIdx.y + ty;
-    const bool own = i <= g.nx && j <= g.ny;
-    const int q = (ty + 1) * W + tx + 1;
+    const int tid = threadIdx.x;
+    const Pair o = own_pair<T>(g);
     const T m = (T)cg->mean_z, beta = (T)cg->beta;
     const T idx2 = (T)st.idx2, idy2 = (T)st.idy2, idz2 = (T)st.idz2, diag = (T)st.diag;
     double acc[1] = {0.0};
     int kb, ke;
     zrange<DIM>(g, zc, kb, ke);
-    const int p0 = DIM == 3 ? kb - 1 : 0, plast = DIM == 3 ? ke : 0;
-    MRing<S> R = ring_start<DIM, S, P>(M, sm, p0, plast);
-    bool ok = R.wait(p0);
-    if (DIM == 3) ok &= R.wait(kb);
-    bool failed = false;
+    MRing<DIM, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING,
+                       DIM == 3 ? kb - 1 : 0, DIM == 3 ? ke : 0};
+    bool ok = true;
+    if (tid == 0) {
+        R.start(M);
+        ok = R.wait(R.p0) && (DIM == 2 || (R.wait(kb) && R.wait(kb + 1)));
+    }
+    if (!step_barrier(ok, err)) return;
     auto pv = [&](const unsigned char* s_, int qq) -> T {
         return (boxv<T>(s_, P::QB * P::VB, qq) - m) + beta * boxv<T>(s_, P::QX * P::VB, qq);
     };
 #pragma unroll 1
     for (int k = kb; k < ke; ++k) {
-        if (DIM == 3) ok &= R.wait(k + 1);
         const unsigned char* sc = R.at(k);
-        const uint32_t c = sc[P::OFF_CODE + (ty + 1) * PBox<uint8_t>::W + tx + 1];
-        T pc = T(0), a_ = T(0);
-        if (c & kActive) {
-            pc = pv(sc, q);
-            const T wall = st.dirichlet ? -pc : pc;
-            const T vL = (c & 2u) ? pv(sc, q - 1) : (i > 1 ? pc : wall);
-            const T vR = (c & 1u) ? pv(sc, q + 1) : (i < g.nx ? pc : wall);
-            const T vB = (c & 8u) ? pv(sc, q - W) : (j > 1 ? pc : wall);
-            const T vT = (c & 4u) ? pv(sc, q + W) : (j < g.ny ? pc : wall);
-            if (DIM == 3) {
-                const T vF = (c & 32u) ? pv(R.at(k - 1), q) : (k > 1 ? pc : wall);
-                const T vK = (c & 16u) ? pv(R.at(k + 1), q) : (k < g.nz ? pc : wall);
-                a_ = diag * pc - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
-            } else {
-                a_ = diag * pc - (vL + vR) * idx2 - (vB + vT) * idy2;
+        const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
+        const unsigned char* su = DIM == 3 ? R.at(k + 1) : sc;
+        const uint32_t cc[2] = {sc[P::OFF_CODE + o.ca], sc[P::OFF_CODE + o.ca + 1]};
+        T pc[2], a_[2] = {T(0), T(0)};
+#pragma unroll
+        for (int e = 0; e < 2; ++e) pc[e] = (cc[e] & kActive) ? pv(sc, o.qa + e) : T(0);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const uint32_t c = cc[e];
+            if (c & kActive) {
+                const int q = o.qa + e, i = o.i + e, j = o.j;
+                const T p0 = pc[e];
+                const T wall = st.dirichlet ? -p0 : p0;
+                // the pair's other cell is the +x (A) or -x (B) neighbour
+                const T vL = (c & 2u) ? (e ? pc[0] : pv(sc, q - 1)) : (i > 1 ? p0 : wall);
+                const T vR = (c & 1u) ? (e ? pv(sc, q + 1) : pc[1]) : (i < g.nx ? p0 : wall);
+                const T vB = (c & 8u) ? pv(sc, q - W) : (j > 1 ? p0 : wall);
+                const T vT = (c & 4u) ? pv(sc, q + W) : (j < g.ny ? p0 : wall);
+                if (DIM == 3) {
+                    const T vF = (c & 32u) ? pv(sb, q) : (k > 1 ? p0 : wall);
+                    const T vK = (c & 16u) ? pv(su, q) : (k < g.nz ? p0 : wall);
+                    a_[e] = diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
+                } else {
+                    a_[e] = diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2;
+                }
+                acc[0] += (double)p0 * (double)a_[e];
             }
-            acc[0] += (double)pc * (double)a_;
         }
-        if (own) {
-            const int id = cidx(g, i, j, k);
-            pnew[id] = pc;
-            ap[id] = a_;
-        }
-        if (DIM == 3) {
-            if (!ring_step<DIM, S, P>(M, R, ok, k - 1, plast, err)) { failed = true; break; }
-        } else if (!__syncthreads_and(ok ? 1 : 0)) {
-            if (tx == 0 && ty == 0) atomicExch(err, 1);
-            failed = true;
-        }
+        const int id = o.gid + k * g.sxy;
+        if (o.ina) { pnew[id] = pc[0]; ap[id] = a_[0]; }
+        if (o.inb) { pnew[id + 1] = pc[1]; ap[id + 1] = a_[1]; }
+        if (DIM == 2) break;
+        if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
+        if (!step_barrier(ok, err)) return;
+        if (tid == 0) R.refill(M, k - 1);
     }
-    if (failed) return;
     double tot[1];
     if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
         const double pap = tot[0];
