@@ -1,7 +1,7 @@
 // Stencil kernels that march along z through a level: a block owns a 32 x 16
-// column tile of (i, j) cells (256 threads, each owning an x-pair of cells -- one
-// of each colour -- so a warp never splits on the red-black parity) and walks a
-// chunk of z planes; each plane of every input array arrives as one TMA box (the tile plus
+// column tile of (i, j) cells (256 threads, each owning a pair of cells (i, j),
+// (i, j+1) -- one of each colour, so a warp never splits on the red-black
+// parity) and walks a chunk of z planes; each plane of every input array arrives as one TMA box (the tile plus
 // a 1-cell ring) in a ring of shared-memory stages, issued several planes ahead
 // of the compute so that the block always has loads in flight.  One thread waits
 // on the stage's mbarrier for the plane the next step needs and the step's block
@@ -84,7 +84,7 @@ struct MPlan {
 };
 
 // Shared memory of a march: 128 B of barriers, the diagonal table, S stages, then
-// `extra` bytes of plane buffers (plus 128 B of alignment slack up front).
+// the plane buffers.
 template <class T, int S, class P>
 struct MLayout {
     static constexpr size_t OFF_LUT = 128;
@@ -108,10 +108,18 @@ struct MLevel {
     int zc;          // planes per block (even)
 };
 
-__device__ __forceinline__ unsigned char* aligned_smem(unsigned char* raw) {
-    const uintptr_t p = reinterpret_cast<uintptr_t>(raw);
-    return reinterpret_cast<unsigned char*>((p + 127) & ~uintptr_t(127));
-}
+// The dynamic shared memory of a march, declared 128-byte aligned (every TMA box
+// sits at a multiple of 128 bytes from it).  Used directly -- never through an
+// integer -- so that every access compiles to a 32-bit shared-memory address.  A
+// base that is not 128-byte aligned sets the error word to 2 and the block returns
+// before it issues a load.
+#define UAAMG_MARCH_SMEM(sm, err)                                                 \
+    extern __shared__ __align__(128) unsigned char smem_raw[];                   \
+    unsigned char* sm = smem_raw;                                                \
+    if (smem_u32(sm) & 127u) {                                                   \
+        if (threadIdx.x == 0) atomicExch(err, 2);                                \
+        return;                                                                  \
+    }
 
 template <class E>
 __device__ __forceinline__ E boxv(const unsigned char* st, size_t off, int q) {
@@ -275,31 +283,31 @@ template <int DIM, class T, bool FINE> struct FwdCfg {
     using P = MPlan<DIM, T, false, !FINE, false>;
     static constexpr int S = FINE ? 8 : 4;
     using Lay = MLayout<T, S, P>;
-    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
+    static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
 template <int DIM, class T, bool FINE> struct ResCfg {
     using P = MPlan<DIM, T, true, !FINE, false>;
-    static constexpr int S = FINE ? 6 : 4;
+    static constexpr int S = FINE && sizeof(T) == 4 ? 6 : 4;
     using Lay = MLayout<T, S, P>;
-    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA;
+    static constexpr size_t BYTES = Lay::OFF_EXTRA;
 };
 template <int DIM, class T, bool FINE> struct UpeCfg {
     using P = MPlan<DIM, T, false, !FINE, true>;
     static constexpr int S = FINE ? 8 : 4;
     using Lay = MLayout<T, S, P>;
-    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
+    static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
 template <int DIM, class T, bool FINE> struct UpoCfg {
     using P = MPlan<DIM, T, true, !FINE, false>;
-    static constexpr int S = FINE ? 6 : 4;
+    static constexpr int S = FINE && sizeof(T) == 4 ? 6 : 4;
     using Lay = MLayout<T, S, P>;
-    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA;
+    static constexpr size_t BYTES = Lay::OFF_EXTRA;
 };
 template <int DIM, class T> struct PmvCfg {
     using P = MPlan<DIM, T, true, false, false>;
-    static constexpr int S = 6;
+    static constexpr int S = sizeof(T) == 4 ? 6 : 4;
     using Lay = MLayout<T, S, P>;
-    static constexpr size_t BYTES = 128 + Lay::OFF_EXTRA;
+    static constexpr size_t BYTES = Lay::OFF_EXTRA;
 };
 
 // z range of this block: planes kb .. ke-1 (3D); the single plane 0 (2D).
@@ -314,42 +322,62 @@ __device__ __forceinline__ void zrange(const Geom& g, int zc, int& kb, int& ke) 
     }
 }
 
-// The thread's x-pair: cells A = (i, j) and B = (i + 1, j) of tile row r (lanes
-// 0-15 of warp w take row 2w, lanes 16-31 row 2w + 1).  i is odd, so A and B have
-// opposite colours on every plane.
+// The thread's pair: cells A = (i, j) and B = (i, j + 1), lane = column, warp w =
+// tile rows 2w and 2w + 1.  A and B have opposite colours on every plane; the
+// lanes of a warp read consecutive words of a box row.
 struct Pair {
-    int i, j, w, pp;  // cell A; warp; pair index within the row
-    int a, rb;        // box column of A, box row
-    int qa, ca;       // box positions of A in the value and code boxes (B: +1)
-    bool ina, inb;    // inside the level
-    int gid;          // cidx(g, i, j, 0)
+    int i, j, lane, w;
+    int a, rb;         // box column and row of A (B: row rb + 1)
+    int qa, ca;        // box positions of A in the value and code boxes
+    bool ina, inb;     // inside the level
+    int gid;           // cidx(g, i, j, 0)
 };
 
 template <class T>
 __device__ __forceinline__ Pair own_pair(const Geom& g) {
     Pair o;
-    const int t = threadIdx.x, l = t & 31;
+    const int t = threadIdx.x;
+    o.lane = t & 31;
     o.w = t >> 5;
-    o.pp = l & 15;
-    const int r = 2 * o.w + (l >> 4);
-    o.i = 1 + kMX * (int)blockIdx.x + 2 * o.pp;
-    o.j = 1 + kMY * (int)blockIdx.y + r;
-    o.a = 2 * o.pp + 1;
-    o.rb = r + 1;
+    o.i = 1 + kMX * (int)blockIdx.x + o.lane;
+    o.j = 1 + kMY * (int)blockIdx.y + 2 * o.w;
+    o.a = o.lane + 1;
+    o.rb = 2 * o.w + 1;
     o.qa = o.rb * PBox<T>::W + o.a;
     o.ca = o.rb * PBox<uint8_t>::W + o.a;
     o.ina = o.i <= g.nx && o.j <= g.ny;
-    o.inb = o.i + 1 <= g.nx && o.j <= g.ny;
+    o.inb = o.i <= g.nx && o.j + 1 <= g.ny;
     o.gid = o.i + o.j * g.sx;
     return o;
+}
+
+// Stage pointers of planes k-1, k, k+1, advanced once per step.
+struct Stages {
+    const unsigned char *m, *c, *n;
+};
+
+template <int DIM, int S, class P>
+__device__ __forceinline__ Stages stages_at(const MRing<DIM, S, P>& R, int k) {
+    Stages s;
+    s.c = R.at(k);
+    s.m = DIM == 3 && k > R.p0 ? R.at(k - 1) : s.c;
+    s.n = DIM == 3 ? R.at(k + 1) : s.c;
+    return s;
+}
+
+template <int DIM, int S, class P>
+__device__ __forceinline__ void stages_next(const MRing<DIM, S, P>& R, Stages& s, int k) {
+    s.m = s.c;
+    s.c = s.n;
+    s.n = R.at(k + 2);  // k: the step just finished
 }
 
 // ---------------------------------------------------------------------------
 // Forward sweep from x = 0: x = (b + 0)/d on odd cells, then
 // x = (b + sum c_n x_n)/d on even cells; writes x on every interior cell.
-// Step k builds plane k+1's odd values (own pair + the ring's odd cells) into a
-// plane buffer and smooths the even cells of plane k from plane k's buffer and the
-// odd values of the cell's own column one plane up and down (registers).
+// Step k builds plane k+1's odd values (the pair's odd cell and the ring's odd
+// cells) into a plane buffer and smooths plane k's even cells from plane k's
+// buffer and the odd values of their own column one plane up and down (registers).
 template <int DIM, class T, bool FINE>
 __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__ MarchMaps M,
                                                          MLevel<T> L, T* __restrict__ x,
@@ -358,15 +386,22 @@ __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__
     using C = FwdCfg<DIM, T, FINE>;
     using P = typename C::P;
     using Lay = typename C::Lay;
-    constexpr int S = C::S, N = PBox<T>::N, W = PBox<T>::W;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char* sm = aligned_smem(smem_raw);
+    constexpr int S = C::S, N = PBox<T>::N, W = PBox<T>::W, WC = PBox<uint8_t>::W;
+    UAAMG_MARCH_SMEM(sm, err)
     T* lut = reinterpret_cast<T*>(sm + Lay::OFF_LUT);
     T* Yb = reinterpret_cast<T*>(sm + Lay::OFF_EXTRA);
     const Geom& g = L.g;
     const int tid = threadIdx.x;
     const Pair o = own_pair<T>(g);
     const int ib = kMX * (int)blockIdx.x, jb = kMY * (int)blockIdx.y;  // box corner cell
+    // the last warps also build the odd cells of the plane buffer's ring; their box
+    // positions for a corner cell of either parity
+    const bool hal = tid >= kThreads - kHaloOdd;
+    int ha0 = 0, hr0 = 0, ha1 = 0, hr1 = 0;
+    if (hal) {
+        halo_odd(tid - (kThreads - kHaloOdd), 0, ha0, hr0);
+        halo_odd(tid - (kThreads - kHaloOdd), 1, ha1, hr1);
+    }
     int kb, ke;
     zrange<DIM>(g, L.zc, kb, ke);
     MRing<DIM, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING,
@@ -378,68 +413,70 @@ __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__
         ok = R.wait(R.p0) && (DIM == 2 || R.wait(R.p0 + 1));
     }
     if (!step_barrier(ok, err)) return;
-    // odd value of the pair at plane p, placed in its column (0: A, 1: B)
-    auto odd_pair = [&](int p, T (&y)[2]) -> T {
-        const int bo = 1 - ((o.i + o.j + p) & 1);
-        const T v = presmooth<DIM, T, P, FINE>(L, lut, R.at(p), o.a + bo, o.rb, o.i + bo, o.j, p);
-        y[0] = bo ? T(0) : v;
-        y[1] = bo ? v : T(0);
+    // odd value of the pair at plane p (stage st), placed in its column (0: A, 1: B);
+    // bo = 1 when B is the odd cell
+    auto odd_pair = [&](const unsigned char* st, int p, int bo, T& ya, T& yb) -> T {
+        const T v = presmooth<DIM, T, P, FINE>(L, lut, st, o.a, o.rb + bo, o.i, o.j + bo, p);
+        ya = bo ? T(0) : v;
+        yb = bo ? v : T(0);
         return v;
     };
-    T ym[2] = {T(0), T(0)}, y0[2] = {T(0), T(0)}, yp[2] = {T(0), T(0)};
-    if (DIM == 3) odd_pair(R.p0, y0);
+    Stages sg = stages_at<DIM, S, P>(R, R.p0);
+    int par = (o.i + o.j + R.p0) & 1;  // 1: A is odd at plane k
+    T yma = T(0), ymb = T(0), y0a = T(0), y0b = T(0), ypa = T(0), ypb = T(0);
+    if (DIM == 3) odd_pair(sg.c, R.p0, par ^ 1, y0a, y0b);
 #pragma unroll 1
     for (int k = R.p0; k < ke; ++k) {
         const int kn = DIM == 3 ? k + 1 : 0;  // plane whose odd values are built this step
+        const int pn = DIM == 3 ? par ^ 1 : par;
         {
             T* Yn = Yb + (kn & 1) * N;
-            const T v = odd_pair(kn, yp);
-            Yn[o.qa + (1 - ((o.i + o.j + kn) & 1))] = v;
-            if (tid < kHaloOdd) {
-                int a, r;
-                halo_odd(tid, (ib + jb + kn) & 1, a, r);
-                Yn[r * W + a] = presmooth<DIM, T, P, FINE>(L, lut, R.at(kn), a, r, ib + a, jb + r, kn);
+            const T v = odd_pair(sg.n, kn, pn ^ 1, ypa, ypb);
+            Yn[o.qa + (pn ? 0 : W)] = v;
+            if (hal) {
+                const int s0 = (ib + jb + kn) & 1, a = s0 ? ha1 : ha0, r = s0 ? hr1 : hr0;
+                Yn[r * W + a] = presmooth<DIM, T, P, FINE>(L, lut, sg.n, a, r, ib + a, jb + r, kn);
             }
         }
         if (DIM == 2) {
-            y0[0] = yp[0];
-            y0[1] = yp[1];
+            y0a = ypa;
+            y0b = ypb;
             __syncthreads();
         }
         if (k >= kb) {
-            const unsigned char* sc = R.at(k);
-            const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
             const T* Yc = Yb + (k & 1) * N;
-            const int e = (o.i + o.j + k) & 1;  // column of the even cell
-            const int q = o.qa + e;
-            const uint32_t c = sc[P::OFF_CODE + o.ca + e];
+            const int e = par;  // 1: B is the even cell
+            const int q = o.qa + (e ? W : 0);
+            const uint32_t c = sg.c[P::OFF_CODE + o.ca + (e ? WC : 0)];
             T xe = T(0);
             if (c & kActive) {
-                const T d = mdiag<DIM, T, P, FINE>(L, lut, sc, c, q, o.i + e, o.j, k);
+                const T d = mdiag<DIM, T, P, FINE>(L, lut, sg.c, c, q, o.i, o.j + e, k);
                 if (!(d < T(1e-30))) {
                     T cc[6];
-                    mcoup<DIM, T, P, FINE>(L, sc, sb, q, cc);
-                    xe = (boxv<T>(sc, P::QB * P::VB, q) +
-                          nbsum<DIM, T>(cc, Yc, q, e ? yp[1] : yp[0], e ? ym[1] : ym[0])) / d;
+                    mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
+                    xe = (boxv<T>(sg.c, P::QB * P::VB, q) +
+                          nbsum<DIM, T>(cc, Yc, q, e ? ypb : ypa, e ? ymb : yma)) / d;
                 }
             }
             const int base = o.gid + k * g.sxy;
-            if (o.ina) x[base] = e ? y0[0] : xe;
-            if (o.inb) x[base + 1] = e ? xe : y0[1];
+            if (o.ina) x[base] = e ? y0a : xe;
+            if (o.inb) x[base + g.sx] = e ? xe : y0b;
         }
         if (DIM == 2) break;
-        ym[0] = y0[0]; ym[1] = y0[1];
-        y0[0] = yp[0]; y0[1] = yp[1];
+        yma = y0a; ymb = y0b;
+        y0a = ypa; y0b = ypb;
+        par ^= 1;
         if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
         if (!step_barrier(ok, err)) return;
         if (tid == 0) R.refill(M, k - 1);
+        stages_next<DIM, S, P>(R, sg, k);
     }
 }
 
 // Residual r = b - A x of every fluid cell and its restriction
 // b_c = sum over the 2x2(x2) children in the reference's (di, dj, dk) order.  A
-// thread's pair is the di = 0, 1 children of one coarse column; the dj = 1 row is
-// the same lane of the other half-warp; dk = 0, 1 are consecutive planes.
+// thread's pair is the dj = 0, 1 children of one coarse column, the di = 1 children
+// are the next lane's pair, dk = 0, 1 are consecutive planes.
 template <int DIM, class T, bool FINE>
 __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant__ MarchMaps M,
                                                            MLevel<T> L,
@@ -450,9 +487,8 @@ __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant
     using C = ResCfg<DIM, T, FINE>;
     using P = typename C::P;
     using Lay = typename C::Lay;
-    constexpr int S = C::S, W = PBox<T>::W;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char* sm = aligned_smem(smem_raw);
+    constexpr int S = C::S, W = PBox<T>::W, WC = PBox<uint8_t>::W;
+    UAAMG_MARCH_SMEM(sm, err)
     T* lut = reinterpret_cast<T*>(sm + Lay::OFF_LUT);
     const Geom& g = L.g;
     const int tid = threadIdx.x;
@@ -468,32 +504,30 @@ __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant
         ok = R.wait(R.p0) && (DIM == 2 || (R.wait(kb) && R.wait(kb + 1)));
     }
     if (!step_barrier(ok, err)) return;
-    const int ic = kMX / 2 * (int)blockIdx.x + 1 + o.pp;
+    const int ic = kMX / 2 * (int)blockIdx.x + 1 + (o.lane >> 1);
     const int jc = kMY / 2 * (int)blockIdx.y + 1 + o.w;
-    const bool writer = (threadIdx.x & 16) == 0 && ic <= L.cg.nx && jc <= L.cg.ny;
+    const bool writer = (o.lane & 1) == 0 && ic <= L.cg.nx && jc <= L.cg.ny;
+    Stages sg = stages_at<DIM, S, P>(R, kb);
     T rlo[2] = {T(0), T(0)};
 #pragma unroll 1
     for (int k = kb; k < ke; ++k) {
-        const unsigned char* sc = R.at(k);
-        const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
-        const unsigned char* su = DIM == 3 ? R.at(k + 1) : sc;
-        const T* xb = reinterpret_cast<const T*>(sc + P::QX * P::VB);
+        const T* xb = reinterpret_cast<const T*>(sg.c + P::QX * P::VB);
         T rv[2];
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            const int q = o.qa + e;
-            const uint32_t c = sc[P::OFF_CODE + o.ca + e];
+            const int q = o.qa + e * W;
+            const uint32_t c = sg.c[P::OFF_CODE + o.ca + e * WC];
             rv[e] = T(0);
             if (c & kActive) {
-                const T d = mdiag<DIM, T, P, FINE>(L, lut, sc, c, q, o.i + e, o.j, k);
+                const T d = mdiag<DIM, T, P, FINE>(L, lut, sg.c, c, q, o.i, o.j + e, k);
                 T cc[6];
-                mcoup<DIM, T, P, FINE>(L, sc, sb, q, cc);
+                mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
                 T ax = d * xb[q] - cc[0] * xb[q + 1] - cc[1] * xb[q - 1] - cc[2] * xb[q + W] -
                        cc[3] * xb[q - W];
                 if (DIM == 3)
-                    ax = ax - cc[4] * boxv<T>(su, P::QX * P::VB, q) -
-                         cc[5] * boxv<T>(sb, P::QX * P::VB, q);
-                rv[e] = boxv<T>(sc, P::QB * P::VB, q) - ax;
+                    ax = ax - cc[4] * boxv<T>(sg.n, P::QX * P::VB, q) -
+                         cc[5] * boxv<T>(sg.m, P::QX * P::VB, q);
+                rv[e] = boxv<T>(sg.c, P::QB * P::VB, q) - ax;
             }
         }
         // children with dk = 0 live on odd planes (k = 2 kc - 1); the set is complete
@@ -502,27 +536,22 @@ __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant
             rlo[0] = rv[0];
             rlo[1] = rv[1];
         } else {
-            T pr[2][2];  // the dj = 1 partner's values [di][dk]
+            T pr[2][2];  // the di = 1 partner's values [dj][dk]
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
-                pr[e][0] = __shfl_down_sync(0xffffffffu, DIM == 3 ? rlo[e] : rv[e], 16);
-                pr[e][1] = __shfl_down_sync(0xffffffffu, rv[e], 16);
+                pr[e][0] = __shfl_down_sync(0xffffffffu, DIM == 3 ? rlo[e] : rv[e], 1);
+                pr[e][1] = __shfl_down_sync(0xffffffffu, rv[e], 1);
             }
             if (writer) {
                 const int kc = DIM == 3 ? k / 2 : 0;
                 const int cid = cidx(L.cg, ic, jc, kc);
                 T s = T(0);
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    if (DIM == 3) {
-                        s += rlo[e];
-                        s += rv[e];
-                        s += pr[e][0];
-                        s += pr[e][1];
-                    } else {
-                        s += rv[e];
-                        s += pr[e][1];
-                    }
+                if (DIM == 3) {
+                    s += rlo[0]; s += rv[0]; s += rlo[1]; s += rv[1];
+                    s += pr[0][0]; s += pr[0][1]; s += pr[1][0]; s += pr[1][1];
+                } else {
+                    s += rv[0]; s += rv[1];
+                    s += pr[0][1]; s += pr[1][1];
                 }
                 cb[cid] = (ccode[cid] & kActive) ? s : T(0);
             }
@@ -531,6 +560,7 @@ __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant
         if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
         if (!step_barrier(ok, err)) return;
         if (tid == 0) R.refill(M, k - 1);
+        stages_next<DIM, S, P>(R, sg, k);
     }
 }
 
@@ -546,19 +576,24 @@ __global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ Ma
     using C = UpeCfg<DIM, T, FINE>;
     using P = typename C::P;
     using Lay = typename C::Lay;
-    constexpr int S = C::S, N = PBox<T>::N, W = PBox<T>::W;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char* sm = aligned_smem(smem_raw);
+    constexpr int S = C::S, N = PBox<T>::N, W = PBox<T>::W, WC = PBox<uint8_t>::W;
+    UAAMG_MARCH_SMEM(sm, err)
     T* lut = reinterpret_cast<T*>(sm + Lay::OFF_LUT);
     T* Yb = reinterpret_cast<T*>(sm + Lay::OFF_EXTRA);
     const Geom& g = L.g;
     const int tid = threadIdx.x;
     const Pair o = own_pair<T>(g);
     const int ib = kMX * (int)blockIdx.x, jb = kMY * (int)blockIdx.y;
+    const bool hal = tid >= kThreads - kHaloOdd;
+    int ha0 = 0, hr0 = 0, ha1 = 0, hr1 = 0;
+    if (hal) {
+        halo_odd(tid - (kThreads - kHaloOdd), 0, ha0, hr0);
+        halo_odd(tid - (kThreads - kHaloOdd), 1, ha1, hr1);
+    }
     // odd cell at box position (a, r): pre-smoothed value + prolongation (0 if not
     // an active odd cell)
     auto oddval = [&](const unsigned char* st, int a, int r, int ci, int cj, int ck) -> T {
-        const uint32_t c = st[P::OFF_CODE + r * PBox<uint8_t>::W + a];
+        const uint32_t c = st[P::OFF_CODE + r * WC + a];
         if ((c & (kActive | kOdd)) != (kActive | kOdd)) return T(0);
         const int qq = r * W + a;
         const T d = mdiag<DIM, T, P, FINE>(L, lut, st, c, qq, ci, cj, ck);
@@ -576,62 +611,64 @@ __global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ Ma
         ok = R.wait(R.p0) && (DIM == 2 || R.wait(R.p0 + 1));
     }
     if (!step_barrier(ok, err)) return;
-    auto odd_pair = [&](int p, T (&y)[2]) -> T {
-        const int bo = 1 - ((o.i + o.j + p) & 1);
-        const T v = oddval(R.at(p), o.a + bo, o.rb, o.i + bo, o.j, p);
-        y[0] = bo ? T(0) : v;
-        y[1] = bo ? v : T(0);
+    auto odd_pair = [&](const unsigned char* st, int p, int bo, T& ya, T& yb) -> T {
+        const T v = oddval(st, o.a, o.rb + bo, o.i, o.j + bo, p);
+        ya = bo ? T(0) : v;
+        yb = bo ? v : T(0);
         return v;
     };
-    T ym[2] = {T(0), T(0)}, y0[2] = {T(0), T(0)}, yp[2] = {T(0), T(0)};
-    if (DIM == 3) odd_pair(R.p0, y0);
+    Stages sg = stages_at<DIM, S, P>(R, R.p0);
+    int par = (o.i + o.j + R.p0) & 1;
+    T yma = T(0), ymb = T(0), y0a = T(0), y0b = T(0), ypa = T(0), ypb = T(0);
+    if (DIM == 3) odd_pair(sg.c, R.p0, par ^ 1, y0a, y0b);
 #pragma unroll 1
     for (int k = R.p0; k < ke; ++k) {
         const int kn = DIM == 3 ? k + 1 : 0;
+        const int pn = DIM == 3 ? par ^ 1 : par;
         {
             T* Yn = Yb + (kn & 1) * N;
-            const T v = odd_pair(kn, yp);
-            Yn[o.qa + (1 - ((o.i + o.j + kn) & 1))] = v;
-            if (tid < kHaloOdd) {
-                int a, r;
-                halo_odd(tid, (ib + jb + kn) & 1, a, r);
-                Yn[r * W + a] = oddval(R.at(kn), a, r, ib + a, jb + r, kn);
+            const T v = odd_pair(sg.n, kn, pn ^ 1, ypa, ypb);
+            Yn[o.qa + (pn ? 0 : W)] = v;
+            if (hal) {
+                const int s0 = (ib + jb + kn) & 1, a = s0 ? ha1 : ha0, r = s0 ? hr1 : hr0;
+                Yn[r * W + a] = oddval(sg.n, a, r, ib + a, jb + r, kn);
             }
         }
         if (DIM == 2) {
-            y0[0] = yp[0];
-            y0[1] = yp[1];
+            y0a = ypa;
+            y0b = ypb;
             __syncthreads();
         }
         if (k >= kb) {
-            const unsigned char* sc = R.at(k);
-            const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
             const T* Yc = Yb + (k & 1) * N;
-            const int e = (o.i + o.j + k) & 1;
-            const int q = o.qa + e;
-            const uint32_t c = sc[P::OFF_CODE + o.ca + e];
+            const int e = par;
+            const int q = o.qa + (e ? W : 0);
+            const uint32_t c = sg.c[P::OFF_CODE + o.ca + (e ? WC : 0)];
             T xe = T(0);
             if (c & kActive) {
-                const T d = mdiag<DIM, T, P, FINE>(L, lut, sc, c, q, o.i + e, o.j, k);
+                const T d = mdiag<DIM, T, P, FINE>(L, lut, sg.c, c, q, o.i, o.j + e, k);
                 if (d < T(1e-30)) {
-                    xe = T(0) + prolong_at<T, P>(sc, o.a + e, o.rb);
+                    // a skipped even cell keeps its pre-smoothed 0 plus the prolongation
+                    xe = T(0) + prolong_at<T, P>(sg.c, o.a, o.rb + e);
                 } else {
                     T cc[6];
-                    mcoup<DIM, T, P, FINE>(L, sc, sb, q, cc);
-                    xe = (boxv<T>(sc, P::QB * P::VB, q) +
-                          nbsum<DIM, T>(cc, Yc, q, e ? yp[1] : yp[0], e ? ym[1] : ym[0])) / d;
+                    mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
+                    xe = (boxv<T>(sg.c, P::QB * P::VB, q) +
+                          nbsum<DIM, T>(cc, Yc, q, e ? ypb : ypa, e ? ymb : yma)) / d;
                 }
             }
             const int base = o.gid + k * g.sxy;
-            if (o.ina) x[base] = e ? y0[0] : xe;
-            if (o.inb) x[base + 1] = e ? xe : y0[1];
+            if (o.ina) x[base] = e ? y0a : xe;
+            if (o.inb) x[base + g.sx] = e ? xe : y0b;
         }
         if (DIM == 2) break;
-        ym[0] = y0[0]; ym[1] = y0[1];
-        y0[0] = yp[0]; y0[1] = yp[1];
+        yma = y0a; ymb = y0b;
+        y0a = ypa; y0b = ypb;
+        par ^= 1;
         if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
         if (!step_barrier(ok, err)) return;
         if (tid == 0) R.refill(M, k - 1);
+        stages_next<DIM, S, P>(R, sg, k);
     }
 }
 
@@ -647,9 +684,8 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
     using C = UpoCfg<DIM, T, FINE>;
     using P = typename C::P;
     using Lay = typename C::Lay;
-    constexpr int S = C::S;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char* sm = aligned_smem(smem_raw);
+    constexpr int S = C::S, W = PBox<T>::W, WC = PBox<uint8_t>::W;
+    UAAMG_MARCH_SMEM(sm, err)
     T* lut = reinterpret_cast<T*>(sm + Lay::OFF_LUT);
     const Geom& g = L.g;
     const int tid = threadIdx.x;
@@ -666,28 +702,27 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
         ok = R.wait(R.p0) && (DIM == 2 || (R.wait(kb) && R.wait(kb + 1)));
     }
     if (!step_barrier(ok, err)) return;
+    Stages sg = stages_at<DIM, S, P>(R, kb);
+    int par = (o.i + o.j + kb) & 1;  // 1: A is odd
 #pragma unroll 1
     for (int k = kb; k < ke; ++k) {
-        const unsigned char* sc = R.at(k);
-        const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
-        const unsigned char* su = DIM == 3 ? R.at(k + 1) : sc;
-        const T* xb = reinterpret_cast<const T*>(sc + P::QX * P::VB);
-        const int od = 1 - ((o.i + o.j + k) & 1);  // column of the odd cell
-        T za = xb[o.qa], zb = xb[o.qa + 1];
-        const uint32_t ca = sc[P::OFF_CODE + o.ca], cbb = sc[P::OFF_CODE + o.ca + 1];
+        const T* xb = reinterpret_cast<const T*>(sg.c + P::QX * P::VB);
+        const int od = par ^ 1;  // 1: B is the odd cell
+        T za = xb[o.qa], zb = xb[o.qa + W];
+        const uint32_t ca = sg.c[P::OFF_CODE + o.ca], cbb = sg.c[P::OFF_CODE + o.ca + WC];
         {
-            const int q = o.qa + od;
+            const int q = o.qa + (od ? W : 0);
             const uint32_t c = od ? cbb : ca;
             if (c & kActive) {
-                const T d = mdiag<DIM, T, P, FINE>(L, lut, sc, c, q, o.i + od, o.j, k);
+                const T d = mdiag<DIM, T, P, FINE>(L, lut, sg.c, c, q, o.i, o.j + od, k);
                 if (!(d < T(1e-30))) {
                     T cc[6];
-                    mcoup<DIM, T, P, FINE>(L, sc, sb, q, cc);
-                    const T vp = DIM == 3 ? boxv<T>(su, P::QX * P::VB, q) : T(0);
-                    const T vm = DIM == 3 ? boxv<T>(sb, P::QX * P::VB, q) : T(0);
-                    const T xv = (boxv<T>(sc, P::QB * P::VB, q) + nbsum<DIM, T>(cc, xb, q, vp, vm)) / d;
+                    mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
+                    const T vp = DIM == 3 ? boxv<T>(sg.n, P::QX * P::VB, q) : T(0);
+                    const T vm = DIM == 3 ? boxv<T>(sg.m, P::QX * P::VB, q) : T(0);
+                    const T xv = (boxv<T>(sg.c, P::QB * P::VB, q) + nbsum<DIM, T>(cc, xb, q, vp, vm)) / d;
                     if (od) zb = xv; else za = xv;
-                    if (od ? o.inb : o.ina) x[o.gid + k * g.sxy + od] = xv;
+                    if (od ? o.inb : o.ina) x[o.gid + k * g.sxy + (od ? g.sx : 0)] = xv;
                 }
             }
         }
@@ -697,7 +732,7 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
                 const uint32_t c = e ? cbb : ca;
                 if ((c & kActive) && (e ? o.inb : o.ina)) {
                     const double zv = (double)(e ? zb : za);
-                    const double rv = (double)boxv<T>(sc, P::QB * P::VB, o.qa + e);
+                    const double rv = (double)boxv<T>(sg.c, P::QB * P::VB, o.qa + e * W);
                     acc[0] += zv;
                     acc[1] += rv * zv;
                     acc[2] += rv;
@@ -705,9 +740,11 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
             }
         }
         if (DIM == 2) break;
+        par ^= 1;
         if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
         if (!step_barrier(ok, err)) return;
         if (tid == 0) R.refill(M, k - 1);
+        stages_next<DIM, S, P>(R, sg, k);
     }
     if (ZDOT) {
         double tot[3];
@@ -730,9 +767,8 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
     using C = PmvCfg<DIM, T>;
     using P = typename C::P;
     using Lay = typename C::Lay;
-    constexpr int S = C::S, W = PBox<T>::W;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char* sm = aligned_smem(smem_raw);
+    constexpr int S = C::S, W = PBox<T>::W, WC = PBox<uint8_t>::W;
+    UAAMG_MARCH_SMEM(sm, err)
     const int tid = threadIdx.x;
     const Pair o = own_pair<T>(g);
     const T m = (T)cg->mean_z, beta = (T)cg->beta;
@@ -751,30 +787,28 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
     auto pv = [&](const unsigned char* s_, int qq) -> T {
         return (boxv<T>(s_, P::QB * P::VB, qq) - m) + beta * boxv<T>(s_, P::QX * P::VB, qq);
     };
+    Stages sg = stages_at<DIM, S, P>(R, kb);
 #pragma unroll 1
     for (int k = kb; k < ke; ++k) {
-        const unsigned char* sc = R.at(k);
-        const unsigned char* sb = DIM == 3 ? R.at(k - 1) : sc;
-        const unsigned char* su = DIM == 3 ? R.at(k + 1) : sc;
-        const uint32_t cc[2] = {sc[P::OFF_CODE + o.ca], sc[P::OFF_CODE + o.ca + 1]};
+        const uint32_t cc[2] = {sg.c[P::OFF_CODE + o.ca], sg.c[P::OFF_CODE + o.ca + WC]};
         T pc[2], a_[2] = {T(0), T(0)};
 #pragma unroll
-        for (int e = 0; e < 2; ++e) pc[e] = (cc[e] & kActive) ? pv(sc, o.qa + e) : T(0);
+        for (int e = 0; e < 2; ++e) pc[e] = (cc[e] & kActive) ? pv(sg.c, o.qa + e * W) : T(0);
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const uint32_t c = cc[e];
             if (c & kActive) {
-                const int q = o.qa + e, i = o.i + e, j = o.j;
+                const int q = o.qa + e * W, i = o.i, j = o.j + e;
                 const T p0 = pc[e];
                 const T wall = st.dirichlet ? -p0 : p0;
-                // the pair's other cell is the +x (A) or -x (B) neighbour
-                const T vL = (c & 2u) ? (e ? pc[0] : pv(sc, q - 1)) : (i > 1 ? p0 : wall);
-                const T vR = (c & 1u) ? (e ? pv(sc, q + 1) : pc[1]) : (i < g.nx ? p0 : wall);
-                const T vB = (c & 8u) ? pv(sc, q - W) : (j > 1 ? p0 : wall);
-                const T vT = (c & 4u) ? pv(sc, q + W) : (j < g.ny ? p0 : wall);
+                const T vL = (c & 2u) ? pv(sg.c, q - 1) : (i > 1 ? p0 : wall);
+                const T vR = (c & 1u) ? pv(sg.c, q + 1) : (i < g.nx ? p0 : wall);
+                // the pair's other cell is the +y (A) or -y (B) neighbour
+                const T vB = (c & 8u) ? (e ? pc[0] : pv(sg.c, q - W)) : (j > 1 ? p0 : wall);
+                const T vT = (c & 4u) ? (e ? pv(sg.c, q + W) : pc[1]) : (j < g.ny ? p0 : wall);
                 if (DIM == 3) {
-                    const T vF = (c & 32u) ? pv(sb, q) : (k > 1 ? p0 : wall);
-                    const T vK = (c & 16u) ? pv(su, q) : (k < g.nz ? p0 : wall);
+                    const T vF = (c & 32u) ? pv(sg.m, q) : (k > 1 ? p0 : wall);
+                    const T vK = (c & 16u) ? pv(sg.n, q) : (k < g.nz ? p0 : wall);
                     a_[e] = diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
                 } else {
                     a_[e] = diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2;
@@ -784,11 +818,12 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
         }
         const int id = o.gid + k * g.sxy;
         if (o.ina) { pnew[id] = pc[0]; ap[id] = a_[0]; }
-        if (o.inb) { pnew[id + 1] = pc[1]; ap[id + 1] = a_[1]; }
+        if (o.inb) { pnew[id + g.sx] = pc[1]; ap[id + g.sx] = a_[1]; }
         if (DIM == 2) break;
         if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
         if (!step_barrier(ok, err)) return;
         if (tid == 0) R.refill(M, k - 1);
+        stages_next<DIM, S, P>(R, sg, k);
     }
     double tot[1];
     if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
@@ -799,6 +834,8 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
         else cg->alpha = cg->rz_old / pap;
     }
 }
+
+#undef UAAMG_MARCH_SMEM
 
 }  // namespace
 }  // namespace uaamg

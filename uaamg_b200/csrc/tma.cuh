@@ -92,18 +92,21 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Waits for the barrier's phase `parity` to complete, at most `limit` polls
-// (each poll may suspend the thread briefly).  Returns false on timeout.
+// Waits for the barrier's phase `parity` to complete, at most `limit` polls; each
+// poll suspends the thread in hardware for up to kTmaPollNs (it resumes as soon as
+// the phase completes), so a waiting thread issues almost nothing.  Returns false
+// on timeout.
+constexpr uint32_t kTmaPollNs = 20000;
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit) {
     const uint32_t a = smem_u32(bar);
     for (long long it = 0; it < limit; ++it) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred P;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, P;\n\t}"
             : "=r"(ok)
-            : "r"(a), "r"(parity)
+            : "r"(a), "r"(parity), "r"(kTmaPollNs)
             : "memory");
         if (ok) return true;
     }
@@ -134,7 +137,7 @@ __device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, int 
     }
 }
 
-// Polls before a TMA wait is declared stuck (several seconds on B200).
-constexpr long long kTmaWaitLimit = 1LL << 24;
+// Polls before a TMA wait is declared stuck: at most 250000 x 20 us = 5 s.
+constexpr long long kTmaWaitLimit = 250000;
 
 }  // namespace uaamg
