@@ -199,6 +199,96 @@ UAAMG_API uaamg_status uaamg_device_bytes(uaamg_handle* h, size_t* bytes);
 UAAMG_API const char* uaamg_last_error(uaamg_handle* h);
 UAAMG_API const char* uaamg_status_string(int status);
 
+/* ---- Batched uneven solves (uaamg_solve_batch) -------------------
+ * One problem of a batch: HOST arrays in the reference layout of Grid / Grid3D
+ * (include/core/mesh.h:35, mesh_3d.h:38), padded, column-major i-fastest.  p
+ * follows Solver::solve (include/solver/solver.h:18-34): 0 on entry, or the
+ * initial guess when options.warm_start is set; the result is written into it. */
+typedef struct uaamg_problem {
+    int dim, nx, ny, nz;  /* nz ignored for dim = 2 */
+    double dx, dy, dz;
+    const uint8_t* solid;
+    const double* rhs;
+    double* p;
+} uaamg_problem;
+
+/* Solves n independent problems of any mix of sizes together on the handle's
+ * device: each problem keeps its own hierarchy, CG state and stream (reused by
+ * the next batch when its shape matches), and the host interleaves the problems'
+ * two-iteration CUDA graphs so that small problems fill the GPU together.  The
+ * handle's own problem (uaamg_set_problem_*) is untouched.  stats[i] (may be
+ * NULL) receives problem i's statistics.  Returns UAAMG_OK when every problem
+ * converged, else the first non-OK status in problem order.  The reference has
+ * no batch entry point; each problem matches uaamg_solve on it alone bit for bit. */
+UAAMG_API uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_problem* problems,
+                                         const uaamg_options* opts, uaamg_stats* stats);
+
+/* 1: before its first solve, every hierarchy times its V-cycle marches at each
+ * level for a few z-chunk lengths (planes per block) and keeps the fastest;
+ * results are cached per level shape for the process.  0 (default): fixed rule.
+ * No reference counterpart (the reference's kernels have fixed shapes). */
+UAAMG_API uaamg_status uaamg_set_autotune(uaamg_handle* h, int on);
+
+/* ---- Serving (uaamg_server_{start,submit,poll,stop}) ------------
+ * A device-resident request loop on one GPU.  Requests carry a simulation id; the
+ * server keeps each id's hierarchy and FP64 pressure on the device and
+ * warm-starts the id's next request from it.  Requests are admitted while fewer
+ * than max_active solves run and the device bytes of all resident ids stay within
+ * hbm_budget_bytes (idle ids are evicted least-recently-used first); admitted
+ * solves run concurrently, each on its own stream, and new requests join as
+ * slots free up (continuous batching).  A request of an id waits for that id's
+ * previous request. */
+typedef struct uaamg_server uaamg_server;
+
+typedef struct uaamg_server_config {
+    int device;
+    int precision;            /* uaamg_precision */
+    double tol;               /* relative to ||b|| (UAAMG_TOL_REL) */
+    int max_iter;
+    int replace_every;        /* mixed precision residual replacement period */
+    int warm_start;           /* 1: start from the id's previous pressure */
+    int max_active;           /* concurrent solves */
+    size_t hbm_budget_bytes;  /* device bytes all resident ids may hold */
+} uaamg_server_config;
+
+typedef struct uaamg_request {
+    long long sim_id;
+    int dim, nx, ny, nz;
+    double dx, dy, dz;
+    const uint8_t* solid;     /* host, copied by submit */
+    const double* rhs;        /* host, copied by submit */
+    double* p_out;            /* host, may be NULL: receives the padded pressure (reference
+                                 layout) when the solve finishes; must stay valid until then */
+} uaamg_request;
+
+typedef struct uaamg_result {
+    long long ticket;
+    long long sim_id;
+    int status;               /* uaamg_status */
+    int iterations;
+    double rel_residual;      /* FP64 true ||b - A p|| / ||b|| */
+    double wait_ms;           /* submit -> admitted */
+    double latency_ms;        /* submit -> result on the host */
+    int warm;                 /* 1 when warm-started from the id's previous pressure */
+} uaamg_result;
+
+UAAMG_API void uaamg_server_default_config(uaamg_server_config* cfg);
+UAAMG_API uaamg_status uaamg_server_start(uaamg_server** out, const uaamg_server_config* cfg);
+/* Copies the request's arrays and queues it; *ticket identifies it. */
+UAAMG_API uaamg_status uaamg_server_submit(uaamg_server* s, const uaamg_request* req,
+                                           long long* ticket);
+/* *done = 1 once the ticket's solve finished (its p_out is written): res is
+ * filled and the ticket is released.  Non-blocking; an unknown or already
+ * released ticket is UAAMG_INVALID_ARG. */
+UAAMG_API uaamg_status uaamg_server_poll(uaamg_server* s, long long ticket, uaamg_result* res,
+                                         int* done);
+/* Blocks until every submitted request has finished. */
+UAAMG_API uaamg_status uaamg_server_drain(uaamg_server* s);
+/* Device bytes held by resident ids, resident id count, completed requests. */
+UAAMG_API uaamg_status uaamg_server_info(uaamg_server* s, size_t* device_bytes, int* resident,
+                                         long long* completed);
+UAAMG_API uaamg_status uaamg_server_stop(uaamg_server* s);
+
 #ifdef __cplusplus
 }
 #endif

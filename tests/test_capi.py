@@ -66,3 +66,23 @@ def test_python_mirror_fails_loudly_without_library(tmp_path):
             _capi.load(str(tmp_path / "nope.so"))
         finally:
             _capi._lib = _capi._lib_saved
+
+
+def test_batch_and_server_reject_bad_arguments_without_a_gpu():
+    lib = _capi.load()
+    assert lib.uaamg_solve_batch(None, 0, None, None, None) == _capi.INVALID_ARG
+    assert lib.uaamg_set_autotune(None, 1) == _capi.INVALID_ARG
+    cfg = _capi.ServerConfig()
+    lib.uaamg_server_default_config(C.byref(cfg))
+    assert (cfg.precision, cfg.tol, cfg.warm_start, cfg.max_active) == (_capi.MIXED, 1e-6, 1, 16)
+    assert cfg.hbm_budget_bytes == 150 << 30
+    s = C.c_void_p()
+    assert lib.uaamg_server_start(None, None) == _capi.INVALID_ARG
+    cfg.max_active = 0
+    assert lib.uaamg_server_start(C.byref(s), C.byref(cfg)) == _capi.INVALID_ARG
+    t = C.c_longlong()
+    assert lib.uaamg_server_submit(None, None, C.byref(t)) == _capi.INVALID_ARG
+    assert lib.uaamg_server_poll(None, 1, None, None) == _capi.INVALID_ARG
+    assert lib.uaamg_server_drain(None) == _capi.INVALID_ARG
+    assert lib.uaamg_server_info(None, None, None, None) == _capi.INVALID_ARG
+    assert lib.uaamg_server_stop(None) == _capi.INVALID_ARG

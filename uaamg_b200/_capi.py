@@ -32,7 +32,10 @@ EXPORTS = [
     "uaamg_set_dirichlet_walls", "uaamg_solve", "uaamg_solve_device", "uaamg_precond_apply",
     "uaamg_residual_history", "uaamg_num_levels", "uaamg_level_dims", "uaamg_copy_level",
     "uaamg_device_bytes", "uaamg_last_error", "uaamg_status_string", "uaamg_profile_solve",
-    "uaamg_set_vcycle_kernels", "uaamg_residual_noalloc",
+    "uaamg_set_vcycle_kernels", "uaamg_residual_noalloc", "uaamg_solve_batch",
+    "uaamg_set_autotune", "uaamg_server_default_config", "uaamg_server_start",
+    "uaamg_server_submit", "uaamg_server_poll", "uaamg_server_drain", "uaamg_server_info",
+    "uaamg_server_stop",
 ]
 
 
@@ -71,6 +74,43 @@ class Stats(C.Structure):
         ("rhs_norm", C.c_double),
         ("solve_ms", C.c_double),
         ("kernel_launches", C.c_longlong),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Problem(C.Structure):
+    """uaamg_problem: one problem of uaamg_solve_batch (host arrays)."""
+    _fields_ = [
+        ("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("solid", C.c_void_p), ("rhs", C.c_void_p), ("p", C.c_void_p),
+    ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_int), ("precision", C.c_int), ("tol", C.c_double),
+        ("max_iter", C.c_int), ("replace_every", C.c_int), ("warm_start", C.c_int),
+        ("max_active", C.c_int), ("hbm_budget_bytes", C.c_size_t),
+    ]
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("sim_id", C.c_longlong),
+        ("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("solid", C.c_void_p), ("rhs", C.c_void_p), ("p_out", C.c_void_p),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_longlong), ("sim_id", C.c_longlong), ("status", C.c_int),
+        ("iterations", C.c_int), ("rel_residual", C.c_double), ("wait_ms", C.c_double),
+        ("latency_ms", C.c_double), ("warm", C.c_int),
     ]
 
     def as_dict(self):
@@ -118,12 +158,22 @@ def load(path: str | None = None):
     L.uaamg_device_bytes.argtypes = [p, C.POINTER(C.c_size_t)]
     L.uaamg_profile_solve.argtypes = [p, p, p, C.POINTER(Options), C.POINTER(Stats),
                                       C.POINTER(KernelTime), i, C.POINTER(i)]
+    L.uaamg_solve_batch.argtypes = [p, i, C.POINTER(Problem), C.POINTER(Options), C.POINTER(Stats)]
+    L.uaamg_set_autotune.argtypes = [p, i]
+    L.uaamg_server_default_config.argtypes = [C.POINTER(ServerConfig)]
+    L.uaamg_server_start.argtypes = [C.POINTER(p), C.POINTER(ServerConfig)]
+    L.uaamg_server_submit.argtypes = [p, C.POINTER(Request), C.POINTER(C.c_longlong)]
+    L.uaamg_server_poll.argtypes = [p, C.c_longlong, C.POINTER(Result), C.POINTER(i)]
+    L.uaamg_server_drain.argtypes = [p]
+    L.uaamg_server_info.argtypes = [p, C.POINTER(C.c_size_t), C.POINTER(i), C.POINTER(C.c_longlong)]
+    L.uaamg_server_stop.argtypes = [p]
     L.uaamg_last_error.argtypes = [p]
     L.uaamg_last_error.restype = C.c_char_p
     L.uaamg_status_string.argtypes = [i]
     L.uaamg_status_string.restype = C.c_char_p
     for name in EXPORTS:
-        if name not in ("uaamg_default_options", "uaamg_last_error", "uaamg_status_string"):
+        if name not in ("uaamg_default_options", "uaamg_last_error", "uaamg_status_string",
+                        "uaamg_server_default_config"):
             getattr(L, name).restype = i
     _lib = L
     return L

@@ -28,9 +28,10 @@ UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_f32.cu", []),
     ("api.cpp", ["-x", "cu"]),
+    ("runtime.cpp", ["-x", "cu"]),
     ("noalloc.cu", ["-fmad=false"]),
 ]
-HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "vec.cuh", "tma.cuh", "engine.cuh", "engine.h"]
+HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "vec.cuh", "tma.cuh", "engine.cuh", "engine.h", "handle.h"]
 
 
 def _nvcc() -> str:

@@ -9,27 +9,10 @@
 #include <vector>
 
 #include "engine.h"
+#include "handle.h"
 
-struct uaamg_handle {
-    int device = 0;
-    cudaStream_t stream = 0;
-    int dirichlet = 0;
-    int dim = 0, nx = 0, ny = 0, nz = 0;
-    double dx = 1, dy = 1, dz = 1;
-    size_t n = 0;
-    uint8_t* d_solid = nullptr;
-    double* d_rhs = nullptr;  // staging for the host-array entry points
-    double* d_p = nullptr;
-    double* d_hist = nullptr;
-    int hist_cap = 0;
-    int last_iters = 0;
-    uaamg::Engine* eng[3] = {nullptr, nullptr, nullptr};
-    bool ready[3] = {false, false, false};
-    int sweeps = 0;
-    std::string err;
-};
-
-namespace {
+namespace uaamg {
+namespace api {
 
 uaamg_status fail(uaamg_handle* h, uaamg_status s, const std::string& msg) {
     if (h) h->err = msg;
@@ -40,8 +23,7 @@ uaamg_status cuda_fail(uaamg_handle* h, cudaError_t e, const char* where) {
     return fail(h, UAAMG_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-uaamg_status map_engine(uaamg_handle* h, int e, const char* where,
-                        const uaamg::Engine* eng = nullptr) {
+uaamg_status map_engine(uaamg_handle* h, int e, const char* where, const uaamg::Engine* eng) {
     switch (e) {
         case uaamg::E_OK: return UAAMG_OK;
         case uaamg::E_OOM: return fail(h, UAAMG_OOM, std::string(where) + ": device allocation failed");
@@ -54,6 +36,37 @@ uaamg_status map_engine(uaamg_handle* h, int e, const char* where,
         }
     }
 }
+
+uaamg_status fill_stats(const uaamg::Engine* eng, const uaamg::SolveResult& r, uaamg_stats* st) {
+    uaamg_status out;
+    switch (r.status) {
+        case 1: out = UAAMG_OK; break;            // CG_CONVERGED
+        case 3: out = UAAMG_BREAKDOWN; break;
+        case 4: out = UAAMG_NAN; break;
+        default: out = UAAMG_NOT_CONVERGED; break; // CG_MAXITER / never started
+    }
+    if (st) {
+        st->status = out;
+        st->iterations = r.iterations;
+        st->replacements = r.replacements;
+        st->levels = eng->nlevels();
+        st->residual = r.rr_true >= 0 ? __builtin_sqrt(r.rr_true) : 0.0;
+        st->rhs_norm = r.bnorm;
+        st->rel_residual = r.bnorm > 0 ? st->residual / r.bnorm : st->residual;
+        st->recursive_residual = r.rr >= 0 ? __builtin_sqrt(r.rr) : 0.0;
+        st->kernel_launches = eng->launches();
+    }
+    return out;
+}
+
+}  // namespace api
+}  // namespace uaamg
+
+namespace {
+
+using uaamg::api::fail;
+using uaamg::api::cuda_fail;
+using uaamg::api::map_engine;
 
 void free_problem(uaamg_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
@@ -167,25 +180,7 @@ uaamg_status solve_dev(uaamg_handle* h, const double* d_rhs, double* d_p, const 
     if (eng->timed_out())
         return fail(h, UAAMG_TIMEOUT, "solve: a kernel gave up waiting for its tile loads");
     h->last_iters = r.iterations;
-    uaamg_status out;
-    switch (r.status) {
-        case 1: out = UAAMG_OK; break;            // CG_CONVERGED
-        case 3: out = UAAMG_BREAKDOWN; break;
-        case 4: out = UAAMG_NAN; break;
-        default: out = UAAMG_NOT_CONVERGED; break; // CG_MAXITER / never started
-    }
-    if (st) {
-        st->status = out;
-        st->iterations = r.iterations;
-        st->replacements = r.replacements;
-        st->levels = eng->nlevels();
-        st->residual = r.rr_true >= 0 ? __builtin_sqrt(r.rr_true) : 0.0;
-        st->rhs_norm = r.bnorm;
-        st->rel_residual = r.bnorm > 0 ? st->residual / r.bnorm : st->residual;
-        st->recursive_residual = r.rr >= 0 ? __builtin_sqrt(r.rr) : 0.0;
-        st->kernel_launches = eng->launches();
-    }
-    return out;
+    return uaamg::api::fill_stats(eng, r, st);
 }
 
 }  // namespace
@@ -224,6 +219,7 @@ uaamg_status uaamg_destroy(uaamg_handle* h) {
     if (!h) return UAAMG_INVALID_ARG;
     cudaSetDevice(h->device);
     free_problem(h);
+    uaamg::api::free_batch(h);
     for (auto*& e : h->eng) { delete e; e = nullptr; }
     delete h;
     return UAAMG_OK;

@@ -97,21 +97,56 @@ public:
         return sync_check();
     }
 
-    int solve(const SolveArgs& a, SolveResult* res) override {
+    int solve_begin(const SolveArgs& a) override {
         if (lv_.empty()) return E_NOPROB;
         launches_ = 0;
-        int e = dim_ == 3 ? solve_impl<3>(a) : solve_impl<2>(a);
-        if (e != E_OK) return e;
-        const CGState& c = *cg_host_;
-        res->status = c.status;
-        res->iterations = c.iter;
-        res->replacements = c.replacements;
-        res->rr = c.rr;
-        res->rr_true = c.rr_true;
-        res->bnorm = c.bnorm;
-        res->r0 = c.r0;
-        res->tol_abs = c.tol_abs;
+        return dim_ == 3 ? begin_impl<3>(a) : begin_impl<2>(a);
+    }
+
+    int solve_step() override {
+        if (stopped_) return E_OK;
+        return dim_ == 3 ? step_impl<3>() : step_impl<2>();
+    }
+
+    // The device is known to have stopped once the flag copied after some step
+    // reads 1, or once every queued step has finished after max_iter was reached.
+    int solve_poll(bool wait, bool* stopped) override {
+        while (!stopped_ && seen_ < nstep_) {
+            const int slot = seen_ & 1;
+            if (wait) {
+                if (cudaEventSynchronize(ev_[slot]) != cudaSuccess) return E_CUDA;
+            } else {
+                const cudaError_t q = cudaEventQuery(ev_[slot]);
+                if (q == cudaErrorNotReady) break;
+                if (q != cudaSuccess) return E_CUDA;
+            }
+            if (flag_host_[slot]) stopped_ = true;
+            ++seen_;
+        }
+        if (!stopped_ && seen_ == nstep_ && it_ >= cur_.max_iter) stopped_ = true;
+        *stopped = stopped_;
         return E_OK;
+    }
+
+    // Steps queued but not yet seen by solve_poll (at most two are useful).
+    int solve_inflight() const override { return nstep_ - seen_; }
+
+    int solve_end(SolveResult* res) override {
+        return dim_ == 3 ? end_impl<3>(res) : end_impl<2>(res);
+    }
+
+    // The whole solve: the host keeps two steps queued and polls one behind, so it
+    // never idles the GPU waiting for a scalar.
+    int solve(const SolveArgs& a, SolveResult* res) override {
+        int e = solve_begin(a);
+        if (e != E_OK) return e;
+        bool stopped = false;
+        while (!stopped) {
+            if ((e = solve_step()) != E_OK) return e;
+            if ((e = solve_poll(solve_inflight() >= 2 || it_ >= cur_.max_iter, &stopped)) != E_OK)
+                return e;
+        }
+        return solve_end(res);
     }
 
     int nlevels() const override { return (int)lv_.size(); }
@@ -160,6 +195,7 @@ public:
     long launches() const override { return launches_; }
     void set_vcycle_sweeps(bool on) override { sweeps_ = on; }
     void set_graphs(bool on) override { graphs_ = on; }
+    void set_autotune(bool on) override { autotune_ = on; }
 
     void set_profiling(bool on) override {
         prof_on_ = on;
@@ -211,6 +247,11 @@ private:
     double *b64_ = nullptr, *xd_ = nullptr, *partials_ = nullptr;
     int* err_ = nullptr;             // set by a kernel whose TMA wait gave up
     CUtensorMap map_p_, map_p2_;     // plane boxes of the two search-direction buffers
+    SolveArgs cur_{};                // the solve in progress
+    bool use_graph_ = false;
+    int it_ = 0;                     // iterations queued
+    int nstep_ = 0, seen_ = 0;       // steps queued / steps whose flag was read
+    bool stopped_ = false;
     long long reduce_blocks_ = 0;    // partials_ capacity in blocks (4 doubles each)
     CGState* cg_ = nullptr;
     CGState* cg_host_ = nullptr;  // pinned
@@ -223,6 +264,7 @@ private:
     int num_sms_ = 148;
     bool sweeps_ = false;  // V-cycle as per-colour sweeps (cross-check) instead of the marches
     bool graphs_ = true;   // replay the PCG step as a CUDA graph
+    bool autotune_ = false;  // time the marches' z-chunk lengths at set-up
     cudaStream_t cap_ = nullptr;      // capture stream
     cudaGraphExec_t gexec_ = nullptr; // two PCG iterations
     long long gkey_ = -1;
@@ -644,19 +686,71 @@ private:
                      dim3(32, 8), g, gref_, z_, d_z, 0);
     }
 
+    // ---- PCG solve, in four stages so that many engines can interleave (batch and
+    // serving): begin (right-hand side, initial residual, first preconditioner
+    // application, graph capture), step (queue two iterations), poll (has the
+    // device stopped?), end (solution out, exit diagnostics).
+
+    Stencil stencil() const {
+        Stencil st;
+        st.idx2 = 1.0 / (dx_ * dx_);
+        st.idy2 = 1.0 / (dy_ * dy_);
+        st.idz2 = dim_ == 3 ? 1.0 / (dz_ * dz_) : 0.0;
+        st.diag = dim_ == 3 ? 2.0 * (st.idx2 + st.idy2 + st.idz2) : 2.0 * (st.idx2 + st.idy2);
+        st.dirichlet = dirichlet_;
+        return st;
+    }
+
+    // z = M r (or z = r), then the z sums -> mean, r.z, beta
     template <int DIM>
-    int solve_impl(const SolveArgs& a) {
+    void cg_precond() {
+        const Geom& g = lv_[0].g;
+        if (cur_.precond) {
+            vcycle<DIM>(z_, &cg_->done, true);
+        } else {
+            cudaMemcpyAsync(z_, r_, (size_t)g.n * sizeof(T), cudaMemcpyDeviceToDevice, st_);
+            UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>),
+                         vec_grid(g), dim3(32, 8), g, lv_[0].solid, r_, z_, partials_, cg_);
+        }
+    }
+
+    // One PCG iteration (pcg_3d.cpp:93-124); the search direction alternates between
+    // p_ and p2_ (from_p: the current one lives in p_).
+    template <int DIM>
+    void cg_iteration(bool from_p) {
+        const Geom& g = lv_[0].g;
+        const Stencil st = stencil();
+        T* pnew = from_p ? p2_ : p_;
+        MarchMaps pm = maps<DIM>(0, true, false);  // z and the current search direction
+        pm.v[0] = lv_[0].mx;
+        pm.v[1] = from_p ? map_p_ : map_p2_;
+        UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
+                          (k_pmatvec<DIM, T>), march_grid<DIM>(g, lv_[0].zc), dim3(kThreads),
+                          (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st, partials_, cg_,
+                          err_);
+        const long long nvec = (long long)g.n / Vec16<T>::N;
+        UAAMG_LAUNCH((KTag{K_UPDATE, 0, cells(g) * (6.0 * sizeof(T))}), k_update_flat<T>,
+                     max_reduce_blocks(), 256, nvec, xlo_, r_, pnew, ap_, partials_, cg_, cur_.hist);
+        if (mixed_) {
+            UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T))}), k_fold_flat<T>,
+                         max_reduce_blocks(), 256, (long long)g.n, xd_, xlo_, cg_, 0);
+            UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (17.0 + sizeof(T))}),
+                         (k_true_residual<DIM, T>), vec_grid(g), dim3(32, 8), g, lv_[0].solid, b64_,
+                         xd_, r_, st, partials_, cg_, 5, 1, cur_.tol, cur_.tol_mode);
+            UAAMG_LAUNCH((KTag{K_SCALAR, 0, 0.0}), k_maxiter_check, 1, 1, cg_);
+        }
+        cg_precond<DIM>();
+    }
+
+    template <int DIM>
+    int begin_impl(const SolveArgs& a) {
+        cur_ = a;
         const Geom g = lv_[0].g;
         const uint8_t* s = lv_[0].solid;
         const dim3 vb(32, 8);
         const dim3 vg = vec_grid(g);
         const int n = g.n;
-        Stencil st;
-        st.idx2 = 1.0 / (dx_ * dx_);
-        st.idy2 = 1.0 / (dy_ * dy_);
-        st.idz2 = DIM == 3 ? 1.0 / (dz_ * dz_) : 0.0;
-        st.diag = DIM == 3 ? 2.0 * (st.idx2 + st.idy2 + st.idz2) : 2.0 * (st.idx2 + st.idy2);
-        st.dirichlet = dirichlet_;
+        const Stencil st = stencil();
 
         CGState init = {};
         init.max_iter = a.max_iter;
@@ -686,53 +780,13 @@ private:
         cudaMemsetAsync(xlo_, 0, (size_t)n * sizeof(T), st_);
         cudaMemsetAsync(p_, 0, (size_t)n * sizeof(T), st_);
         cudaMemsetAsync(xd_, 0, (size_t)n * sizeof(double), st_);
+        cg_precond<DIM>();
 
-        const int* done = &cg_->done;
-        // z = M r (or z = r), then the z sums -> mean, r.z, beta
-        auto precond = [&]() {
-            if (a.precond) {
-                vcycle<DIM>(z_, done, true);
-            } else {
-                cudaMemcpyAsync(z_, r_, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, st_);
-                UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>), vg, vb,
-                             g, s, r_, z_, partials_, cg_);
-            }
-        };
-        const dim3 pgrid = march_grid<DIM>(g, lv_[0].zc);
-        MarchMaps pm[2];  // z and the current search direction (p_, p2_), codes
-        for (int q = 0; q < 2; ++q) {
-            pm[q] = maps<DIM>(0, true, false);
-            pm[q].v[0] = lv_[0].mx;
-            pm[q].v[1] = q == 0 ? map_p_ : map_p2_;
-        }
-        const long long nvec = (long long)n / Vec16<T>::N;
-        const int ugrid = max_reduce_blocks();
-        precond();
-        // One PCG iteration (pcg_3d.cpp:93-124); the search direction alternates
-        // between p_ and p2_ (from_p: the current one lives in p_).
-        auto iteration = [&](bool from_p) {
-            T* pnew = from_p ? p2_ : p_;
-            UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
-                              (k_pmatvec<DIM, T>), pgrid, dim3(kThreads), (PmvCfg<DIM, T>::BYTES),
-                              pm[from_p ? 0 : 1], g, lv_[0].zc, pnew, ap_, st, partials_, cg_, err_);
-            UAAMG_LAUNCH((KTag{K_UPDATE, 0, cells(g) * (6.0 * sizeof(T))}), k_update_flat<T>, ugrid, 256,
-                         nvec, xlo_, r_, pnew, ap_, partials_, cg_, a.hist);
-            if (mixed_) {
-                UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T))}), k_fold_flat<T>, ugrid,
-                             256, (long long)n, xd_, xlo_, cg_, 0);
-                UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (17.0 + sizeof(T))}), (k_true_residual<DIM, T>),
-                             vg, vb, g, s, b64_, xd_, r_, st, partials_, cg_, 5, 1, a.tol, a.tol_mode);
-                UAAMG_LAUNCH((KTag{K_SCALAR, 0, 0.0}), k_maxiter_check, 1, 1, cg_);
-            }
-            precond();
-        };
         // Two iterations form one step (the search direction is back in p_ after
         // it); outside profiling the step is a CUDA graph captured once per problem
-        // and options.  The host polls the device 'done' flag one step behind, so it
-        // never idles the GPU waiting for a scalar; kernels queued after the solve
-        // stopped return at once.
-        const bool use_graph = graphs_ && !prof_on_;
-        if (use_graph) {
+        // and options.
+        use_graph_ = graphs_ && !prof_on_;
+        if (use_graph_) {
             const long long key = ((long long)a.precond << 1) | (sweeps_ ? 1 : 0);
             if (!gexec_ || key != gkey_ || a.hist != ghist_) {
                 if (gexec_) { cudaGraphExecDestroy(gexec_); gexec_ = nullptr; }
@@ -744,49 +798,69 @@ private:
                 cudaGraph_t graph = nullptr;
                 cudaError_t ce = cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal);
                 if (ce == cudaSuccess) {
-                    iteration(true);
-                    iteration(false);
+                    cg_iteration<DIM>(true);
+                    cg_iteration<DIM>(false);
                     ce = cudaStreamEndCapture(cap_, &graph);
                 }
                 st_ = saved;
                 if (ce != cudaSuccess || !graph) { cuda_error = ce != cudaSuccess ? ce : cudaErrorUnknown; return E_CUDA; }
                 ce = cudaGraphInstantiate(&gexec_, graph, 0);
                 cudaGraphDestroy(graph);
-                if (ce != cudaSuccess) { gexec_ = nullptr; return E_CUDA; }
+                if (ce != cudaSuccess) { gexec_ = nullptr; cuda_error = ce; return E_CUDA; }
                 glaunches_ = launches_ - before;
                 launches_ = before;
                 gkey_ = key;
                 ghist_ = a.hist;
             }
         }
-        for (int it = 0, step = 0; it < a.max_iter; it += 2, ++step) {
-            if (use_graph) {
-                if (cudaGraphLaunch(gexec_, st_) != cudaSuccess) return E_CUDA;
-                launches_ += glaunches_;
-            } else {
-                iteration(true);
-                if (it + 1 < a.max_iter) iteration(false);
-            }
-            const int slot = step & 1;
-            cudaMemcpyAsync(&flag_host_[slot], done, sizeof(int), cudaMemcpyDeviceToHost, st_);
-            cudaEventRecord(ev_[slot], st_);
-            if (step > 0) {
-                if (cudaEventSynchronize(ev_[slot ^ 1]) != cudaSuccess) return E_CUDA;
-                if (flag_host_[slot ^ 1]) break;
-            }
-        }
+        it_ = 0;
+        nstep_ = 0;
+        seen_ = 0;
+        stopped_ = false;
+        return E_OK;
+    }
 
+    // Queues one step (two iterations) unless max_iter is reached, then the copy of
+    // the device 'done' flag into slot step % 2 and that slot's event.  Kernels
+    // queued after the solve stopped return at once.
+    template <int DIM>
+    int step_impl() {
+        // two flag slots: a third step waits until the oldest one has been polled
+        if (it_ >= cur_.max_iter || nstep_ - seen_ >= 2) return E_OK;
+        if (use_graph_) {
+            if (cudaGraphLaunch(gexec_, st_) != cudaSuccess) return E_CUDA;
+            launches_ += glaunches_;
+        } else {
+            cg_iteration<DIM>(true);
+            if (it_ + 1 < cur_.max_iter) cg_iteration<DIM>(false);
+        }
+        it_ += 2;
+        const int slot = nstep_ & 1;
+        cudaMemcpyAsync(&flag_host_[slot], &cg_->done, sizeof(int), cudaMemcpyDeviceToHost, st_);
+        cudaEventRecord(ev_[slot], st_);
+        ++nstep_;
+        return E_OK;
+    }
+
+    template <int DIM>
+    int end_impl(SolveResult* res) {
+        const Geom g = lv_[0].g;
+        const dim3 vb(32, 8);
+        const dim3 vg = vec_grid(g);
+        const int n = g.n;
+        const Stencil st = stencil();
+        const SolveArgs& a = cur_;
         if (mixed_) {
-            UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T))}), k_fold_flat<T>, ugrid, 256,
-                         (long long)n, xd_, xlo_, cg_, 1);
+            UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T))}), k_fold_flat<T>,
+                         max_reduce_blocks(), 256, (long long)n, xd_, xlo_, cg_, 1);
         } else if (sizeof(T) == sizeof(double)) {
             cudaMemcpyAsync(xd_, xlo_, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_);
         } else {
             UAAMG_LAUNCH((KTag{K_CAST, 0, 12.0 * n}), k_cast_to_f64<T>, (n + 255) / 256, 256, xlo_, xd_, n);
         }
         // exit diagnostics: FP64 true residual of the accumulated solution
-        UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * 17.0}), (k_true_residual<DIM, T>), vg, vb, g, s,
-                     b64_, xd_, (T*)nullptr, st, partials_, cg_, 5, 2, a.tol, a.tol_mode);
+        UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * 17.0}), (k_true_residual<DIM, T>), vg, vb, g,
+                     lv_[0].solid, b64_, xd_, (T*)nullptr, st, partials_, cg_, 5, 2, a.tol, a.tol_mode);
         UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 24.0}), (k_export<DIM, double>), vg, vb, g, gref_, xd_,
                      a.x, 1);
         if (a.project_mean && a.ref_solid) {
@@ -798,7 +872,18 @@ private:
         }
         if (cudaMemcpyAsync(cg_host_, cg_, sizeof(CGState), cudaMemcpyDeviceToHost, st_) != cudaSuccess)
             return E_CUDA;
-        return sync_check();
+        int e = sync_check();
+        if (e != E_OK) return e;
+        const CGState& c = *cg_host_;
+        res->status = c.status;
+        res->iterations = c.iter;
+        res->replacements = c.replacements;
+        res->rr = c.rr;
+        res->rr_true = c.rr_true;
+        res->bnorm = c.bnorm;
+        res->r0 = c.r0;
+        res->tol_abs = c.tol_abs;
+        return E_OK;
     }
 };
 

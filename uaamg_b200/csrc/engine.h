@@ -62,6 +62,16 @@ public:
     // z = M^{-1} r (one V(1,1) cycle); FP64 device arrays, padded.
     virtual int precond_apply(const double* d_r, double* d_z) = 0;
     virtual int solve(const SolveArgs& a, SolveResult* res) = 0;
+    // The solve in stages, for engines that share the GPU (batch, serving):
+    // begin queues the set-up and the first preconditioner application; step
+    // queues two iterations; poll reports whether the device has stopped (wait:
+    // block on the oldest queued step); end queues the output and blocks for the
+    // result.  All on the engine's stream.
+    virtual int solve_begin(const SolveArgs& a) = 0;
+    virtual int solve_step() = 0;
+    virtual int solve_poll(bool wait, bool* stopped) = 0;
+    virtual int solve_inflight() const = 0;
+    virtual int solve_end(SolveResult* res) = 0;
     virtual int nlevels() const = 0;
     virtual void level_dims(int l, int* nx, int* ny, int* nz) const = 0;
     // Host copies of level l: mask and FP64 views of cx, cy, cz (nullable).
@@ -74,6 +84,9 @@ public:
     virtual void set_vcycle_sweeps(bool on) = 0;
     // Replay each pair of PCG iterations as one CUDA graph (default on).
     virtual void set_graphs(bool on) = 0;
+    // 1: the next set_problem times each level's marches for a few z-chunk lengths
+    // and keeps the fastest (cached per level shape for the process).
+    virtual void set_autotune(bool on) = 0;
     // Per-launch CUDA-event timing of subsequent solves (adds two events per launch).
     virtual void set_profiling(bool on) = 0;
     virtual int profile_results(std::vector<KernelTime>& out) = 0;

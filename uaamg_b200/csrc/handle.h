@@ -1,0 +1,43 @@
+// The C-ABI handle (include/uaamg.h) and the helpers that api.cpp and runtime.cpp
+// share: error recording and the mapping of engine errors to uaamg_status.
+#pragma once
+#include <string>
+
+#include "../../include/uaamg.h"
+#include "engine.h"
+
+struct uaamg_handle {
+    int device = 0;
+    cudaStream_t stream = 0;
+    int dirichlet = 0;
+    int dim = 0, nx = 0, ny = 0, nz = 0;
+    double dx = 1, dy = 1, dz = 1;
+    size_t n = 0;
+    uint8_t* d_solid = nullptr;
+    double* d_rhs = nullptr;  // staging for the host-array entry points
+    double* d_p = nullptr;
+    double* d_hist = nullptr;
+    int hist_cap = 0;
+    int last_iters = 0;
+    uaamg::Engine* eng[3] = {nullptr, nullptr, nullptr};
+    bool ready[3] = {false, false, false};
+    int sweeps = 0;
+    int autotune = 0;
+    std::string err;
+    struct BatchPool* batch = nullptr;  // runtime.cpp: per-problem slots of uaamg_solve_batch
+};
+
+namespace uaamg {
+namespace api {
+
+uaamg_status fail(uaamg_handle* h, uaamg_status s, const std::string& msg);
+uaamg_status cuda_fail(uaamg_handle* h, cudaError_t e, const char* where);
+uaamg_status map_engine(uaamg_handle* h, int e, const char* where,
+                        const uaamg::Engine* eng = nullptr);
+// uaamg_stats from an engine result (CG_* status mapped to uaamg_status).
+uaamg_status fill_stats(const uaamg::Engine* eng, const uaamg::SolveResult& r, uaamg_stats* st);
+// Frees the batch slots of a handle (runtime.cpp).
+void free_batch(uaamg_handle* h);
+
+}  // namespace api
+}  // namespace uaamg

@@ -426,6 +426,11 @@ __global__ void k_true_residual(Geom g, const uint8_t* __restrict__ s, const dou
             cg->tol_abs = tol_mode ? tol * cg->bnorm : tol;
             if (rr == 0.0) { cg->status = CG_CONVERGED; cg->done = 1; }  // b = 0: x = 0 exactly
         } else if (mode == 1) {
+            // a true residual more than twice the recursive one means the FP32
+            // recurrence drifted: the next search direction restarts (beta = 0),
+            // since beta = r.z / r.z_old would mix the replaced residual with
+            // directions built for the drifted one
+            if (rr > 4.0 * cg->rr) cg->init = 1;
             cg->rr = rr;
             cg->replacements += 1;
             if (cg->cand) {

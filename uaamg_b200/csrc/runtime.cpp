@@ -1,0 +1,647 @@
+// Batched solves and the serving loop of the C-ABI (include/uaamg.h,
+// uaamg_solve_batch and uaamg_server_*).  Both run many independent engines on
+// one GPU at once: every problem owns an engine (hierarchy + CG state), device
+// staging buffers and a stream, and one host thread advances all of them through
+// the engine's staged solve (solve_begin / solve_step / solve_poll / solve_end),
+// so the problems' two-iteration CUDA graphs overlap on the device.
+//
+// There is no counterpart in the reference: its solvers run one problem at a time
+// on the legacy default stream (src/solver/cuda/cuda_pcg_solver.cu:21-63).  Each
+// problem's kernels, launch order and reductions are the ones uaamg_solve issues,
+// so a problem's result does not depend on what runs beside it.
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "engine.h"
+#include "handle.h"
+
+namespace uaamg {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_since(Clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+size_t padded_cells(int dim, int nx, int ny, int nz) {
+    return (size_t)(nx + 2) * (ny + 2) * (dim == 3 ? (size_t)(nz + 2) : 1);
+}
+
+// Device problem: an engine with its mask, FP64 right-hand side and pressure
+// staging buffers (reference layout) and a stream.
+struct DevProblem {
+    Engine* eng = nullptr;
+    int prec = -1, dim = 0, nx = 0, ny = 0, nz = 0, dirichlet = 0;
+    double dx = 0, dy = 0, dz = 0;
+    size_t n = 0;
+    uint8_t* d_solid = nullptr;
+    double* d_rhs = nullptr;
+    double* d_p = nullptr;
+    cudaStream_t stream = nullptr;
+    bool built = false;
+
+    size_t bytes() const { return (eng ? eng->device_bytes() : 0) + n * (1 + 16); }
+
+    void release() {
+        if (stream) cudaStreamSynchronize(stream);
+        delete eng;
+        eng = nullptr;
+        cudaFree(d_solid);
+        cudaFree(d_rhs);
+        cudaFree(d_p);
+        d_solid = nullptr;
+        d_rhs = d_p = nullptr;
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+        built = false;
+        n = 0;
+        prec = -1;
+    }
+
+    bool same_shape(int p, int d, int x, int y, int z, double hx, double hy, double hz,
+                    int dir) const {
+        return eng && prec == p && dim == d && nx == x && ny == y && (d == 2 || nz == z) &&
+               dx == hx && dy == hy && (d == 2 || dz == hz) && dirichlet == dir;
+    }
+
+    // Allocates for the shape (keeps what matches).  Returns an engine error code.
+    int prepare(int p, int d, int x, int y, int z, double hx, double hy, double hz, int dir) {
+        if (same_shape(p, d, x, y, z, hx, hy, hz, dir)) return E_OK;
+        release();
+        prec = p; dim = d; nx = x; ny = y; nz = d == 3 ? z : 0;
+        dx = hx; dy = hy; dz = d == 3 ? hz : 1.0; dirichlet = dir;
+        n = padded_cells(d, x, y, z);
+        if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            stream = nullptr;
+            return E_CUDA;
+        }
+        if (cudaMalloc(&d_solid, n) != cudaSuccess || cudaMalloc(&d_rhs, n * 8) != cudaSuccess ||
+            cudaMalloc(&d_p, n * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return E_OOM;
+        }
+        eng = p == PREC_FP64 ? create_engine_f64() : create_engine_f32(p == PREC_MIXED);
+        if (!eng) return E_OOM;
+        eng->set_stream(stream);
+        return E_OK;
+    }
+
+    // Mask upload + hierarchy (blocking on the problem's stream).
+    int build(const uint8_t* solid_host) {
+        if (cudaMemcpyAsync(d_solid, solid_host, n, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+            return E_CUDA;
+        built = false;
+        int e = eng->set_problem(dim, nx, ny, nz, dx, dy, dz, d_solid, dirichlet);
+        if (e == E_OK) built = true;
+        return e;
+    }
+
+    SolveArgs args(const uaamg_options& o) const {
+        SolveArgs a;
+        a.rhs = d_rhs;
+        a.x = d_p;
+        a.max_iter = o.max_iter;
+        a.tol = o.tol;
+        a.tol_mode = o.tol_mode;
+        a.warm = o.warm_start;
+        a.replace_every = o.replace_every;
+        a.project_mean = o.project_mean;
+        a.precond = o.preconditioner;
+        a.hist = nullptr;
+        a.ref_solid = d_solid;
+        return a;
+    }
+};
+
+}  // namespace
+}  // namespace uaamg
+
+// Per-problem slots of uaamg_solve_batch, kept on the handle between calls.
+struct BatchPool {
+    std::vector<uaamg::DevProblem> slots;
+};
+
+namespace uaamg {
+namespace api {
+
+void free_batch(uaamg_handle* h) {
+    if (!h || !h->batch) return;
+    for (auto& s : h->batch->slots) s.release();
+    delete h->batch;
+    h->batch = nullptr;
+}
+
+}  // namespace api
+}  // namespace uaamg
+
+extern "C" {
+
+uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_problem* probs,
+                               const uaamg_options* o, uaamg_stats* stats) {
+    using namespace uaamg;
+    using api::fail;
+    if (!h) return UAAMG_INVALID_ARG;
+    if (n < 0 || (n > 0 && !probs)) return fail(h, UAAMG_INVALID_ARG, "batch: bad problem list");
+    uaamg_options opts;
+    uaamg_default_options(&opts);
+    if (o) opts = *o;
+    if (opts.max_iter < 0 || !(opts.tol >= 0) || opts.tol_mode < 0 || opts.tol_mode > 1 ||
+        opts.precision < 0 || opts.precision > 2)
+        return fail(h, UAAMG_INVALID_ARG, "batch: bad options");
+    for (int i = 0; i < n; ++i) {
+        const uaamg_problem& p = probs[i];
+        const int nz = p.dim == 3 ? p.nz : 2;
+        if ((p.dim != 2 && p.dim != 3) || p.nx < 2 || p.ny < 2 || nz < 2 || !p.solid || !p.rhs ||
+            !p.p || !(p.dx > 0) || !(p.dy > 0) || (p.dim == 3 && !(p.dz > 0)) ||
+            padded_cells(p.dim, p.nx, p.ny, p.nz) >= ((size_t)1 << 31))
+            return fail(h, UAAMG_INVALID_ARG, "batch: problem " + std::to_string(i) + " is invalid");
+    }
+    cudaSetDevice(h->device);
+    if (!h->batch) h->batch = new (std::nothrow) BatchPool();
+    if (!h->batch) return fail(h, UAAMG_OOM, "batch: pool allocation failed");
+    auto& slots = h->batch->slots;
+    if ((int)slots.size() < n) slots.resize(n);
+    const auto t0 = Clock::now();
+    // set-up: buffers, mask, hierarchy, right-hand side and the first stage
+    for (int i = 0; i < n; ++i) {
+        const uaamg_problem& p = probs[i];
+        DevProblem& d = slots[i];
+        int e = d.prepare(opts.precision, p.dim, p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, h->dirichlet);
+        if (e == E_OK) {
+            d.eng->set_vcycle_sweeps(h->sweeps != 0);
+            d.eng->set_autotune(h->autotune != 0);
+            e = d.build(p.solid);
+        }
+        if (e != E_OK) {
+            const uaamg_status s =
+                api::map_engine(h, e, ("batch: problem " + std::to_string(i) + " set-up").c_str(), d.eng);
+            d.release();
+            return s;
+        }
+        // as uaamg_solve: the result is accumulated into the caller's p
+        cudaMemcpyAsync(d.d_rhs, p.rhs, d.n * 8, cudaMemcpyHostToDevice, d.stream);
+        cudaMemcpyAsync(d.d_p, p.p, d.n * 8, cudaMemcpyHostToDevice, d.stream);
+        if ((e = d.eng->solve_begin(d.args(opts))) != E_OK)
+            return api::map_engine(h, e, "batch: solve", d.eng);
+    }
+    // advance every unfinished problem: keep two steps queued, collect finished ones
+    std::vector<char> open(n, 1);
+    int left = n;
+    uaamg_status first_bad = UAAMG_OK;
+    while (left > 0) {
+        bool progressed = false;
+        for (int i = 0; i < n; ++i) {
+            if (!open[i]) continue;
+            DevProblem& d = slots[i];
+            bool stopped = false;
+            int e = d.eng->solve_step();
+            if (e == E_OK) e = d.eng->solve_poll(false, &stopped);
+            if (e != E_OK) return api::map_engine(h, e, "batch: solve", d.eng);
+            if (!stopped) continue;
+            SolveResult r;
+            std::memset(&r, 0, sizeof(r));
+            if ((e = d.eng->solve_end(&r)) != E_OK) return api::map_engine(h, e, "batch: solve", d.eng);
+            if (d.eng->timed_out())
+                return fail(h, UAAMG_TIMEOUT, "batch: a kernel gave up waiting for its tile loads");
+            cudaError_t ce = cudaMemcpyAsync(probs[i].p, d.d_p, d.n * 8, cudaMemcpyDeviceToHost, d.stream);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(d.stream);
+            if (ce != cudaSuccess) return api::cuda_fail(h, ce, "batch: download");
+            uaamg_stats st_local;
+            const uaamg_status s = api::fill_stats(d.eng, r, &st_local);
+            st_local.solve_ms = ms_since(t0);
+            if (stats) stats[i] = st_local;
+            if (s != UAAMG_OK && first_bad == UAAMG_OK) first_bad = s;
+            open[i] = 0;
+            --left;
+            progressed = true;
+        }
+        if (!progressed) std::this_thread::yield();
+    }
+    return first_bad;
+}
+
+uaamg_status uaamg_set_autotune(uaamg_handle* h, int on) {
+    if (!h) return UAAMG_INVALID_ARG;
+    h->autotune = on ? 1 : 0;
+    for (auto* e : h->eng)
+        if (e) e->set_autotune(on != 0);
+    for (int q = 0; q < 3; ++q) h->ready[q] = false;  // re-tune at the next set-up
+    return UAAMG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving loop.
+
+namespace uaamg {
+namespace {
+
+// One simulation id resident on the device: its engine and mask, and in d_p the
+// FP64 pressure of its last request (the next request's warm start).
+struct SimState {
+    DevProblem dp;
+    std::vector<uint8_t> mask;
+    bool has_p = false;
+    bool busy = false;
+    uint64_t last_used = 0;
+    size_t bytes = 0;
+};
+
+struct Ticket {
+    long long id = 0;
+    uaamg_request req{};
+    std::vector<uint8_t> solid;
+    std::vector<double> rhs;
+    Clock::time_point t_submit, t_admit;
+    uaamg_result res{};
+    bool done = false;
+    int slot = -1;
+    SimState* sim = nullptr;
+};
+
+// Pinned host staging of one concurrent solve.
+struct StageBuf {
+    double* h = nullptr;
+    size_t cap = 0;
+    bool used = false;
+    bool ensure(size_t n) {
+        if (n <= cap) return true;
+        if (h) cudaFreeHost(h);
+        h = nullptr;
+        cap = 0;
+        if (cudaHostAlloc(&h, n * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cap = n;
+        return true;
+    }
+};
+
+// Device bytes a new id of this shape is expected to hold (engine + staging),
+// used for admission before its hierarchy exists.
+size_t estimate_bytes(int prec, int dim, int nx, int ny, int nz) {
+    const size_t n = padded_cells(dim, nx, ny, nz);
+    return n * (prec == PREC_FP64 ? 200 : 120);
+}
+
+}  // namespace
+}  // namespace uaamg
+
+struct uaamg_server {
+    uaamg_server_config cfg{};
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv;
+    bool stopping = false;
+    long long next_ticket = 1;
+    long long outstanding = 0;  // submitted, not finished
+    long long completed = 0;
+    std::deque<uaamg::Ticket*> pending;
+    std::unordered_map<long long, uaamg::Ticket*> tickets;
+    // worker-owned (the counters below are also updated under mu for info)
+    std::unordered_map<long long, uaamg::SimState*> sims;
+    std::vector<uaamg::Ticket*> active;
+    std::vector<uaamg::StageBuf> stage;
+    size_t resident_bytes = 0;
+    int resident = 0;
+    uint64_t tick = 0;
+};
+
+namespace uaamg {
+namespace {
+
+void release_sim(uaamg_server* s, SimState* sim) {
+    sim->dp.release();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->resident_bytes -= sim->bytes;
+        s->resident -= 1;
+    }
+    delete sim;
+}
+
+// Evicts idle ids, least recently used first, until `need` more bytes fit in the
+// budget.  False when the idle ids are not enough.
+bool make_room(uaamg_server* s, size_t need) {
+    while (s->resident_bytes + need > s->cfg.hbm_budget_bytes) {
+        auto victim = s->sims.end();
+        for (auto it = s->sims.begin(); it != s->sims.end(); ++it)
+            if (!it->second->busy &&
+                (victim == s->sims.end() || it->second->last_used < victim->second->last_used))
+                victim = it;
+        if (victim == s->sims.end()) return false;
+        SimState* sim = victim->second;
+        s->sims.erase(victim);
+        release_sim(s, sim);
+    }
+    return true;
+}
+
+void finish(uaamg_server* s, Ticket* t, int status) {
+    t->res.ticket = t->id;
+    t->res.sim_id = t->req.sim_id;
+    t->res.status = status;
+    t->res.latency_ms = ms_since(t->t_submit);
+    if (t->slot >= 0) s->stage[t->slot].used = false;
+    t->slot = -1;
+    if (t->sim) {
+        t->sim->busy = false;
+        t->sim->last_used = ++s->tick;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    t->done = true;
+    s->outstanding -= 1;
+    s->completed += 1;
+    s->cv.notify_all();
+}
+
+// Starts an admitted request: its id's hierarchy (reused when the shape and mask
+// match), the right-hand side upload and the first solve stage.  Returns false if
+// it must wait (no device room yet).
+bool start_request(uaamg_server* s, Ticket* t) {
+    const uaamg_request& q = t->req;
+    const uaamg_server_config& c = s->cfg;
+    SimState* sim = nullptr;
+    auto it = s->sims.find(q.sim_id);
+    if (it != s->sims.end()) {
+        sim = it->second;
+        if (!sim->dp.same_shape(c.precision, q.dim, q.nx, q.ny, q.nz, q.dx, q.dy, q.dz, 0) ||
+            sim->mask != t->solid) {
+            s->sims.erase(it);
+            release_sim(s, sim);
+            sim = nullptr;
+        }
+    }
+    bool warm = false;
+    if (!sim) {
+        const size_t need = estimate_bytes(c.precision, q.dim, q.nx, q.ny, q.nz);
+        if (!make_room(s, need) && !s->active.empty()) return false;
+        sim = new (std::nothrow) SimState();
+        if (!sim) { finish(s, t, UAAMG_OOM); return true; }
+        int e = sim->dp.prepare(c.precision, q.dim, q.nx, q.ny, q.nz, q.dx, q.dy, q.dz, 0);
+        if (e == E_OK) e = sim->dp.build(t->solid.data());
+        if (e != E_OK) {
+            sim->dp.release();
+            delete sim;
+            finish(s, t, e == E_OOM ? UAAMG_OOM : UAAMG_CUDA_ERROR);
+            return true;
+        }
+        sim->mask = t->solid;
+        sim->bytes = sim->dp.bytes();
+        s->sims[q.sim_id] = sim;
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->resident_bytes += sim->bytes;
+        s->resident += 1;
+    } else {
+        warm = c.warm_start && sim->has_p;
+    }
+    int slot = -1;
+    for (int i = 0; i < (int)s->stage.size(); ++i)
+        if (!s->stage[i].used) { slot = i; break; }
+    if (slot < 0 || !s->stage[slot].ensure(sim->dp.n)) { finish(s, t, UAAMG_OOM); return true; }
+    StageBuf& b = s->stage[slot];
+    b.used = true;
+    t->slot = slot;
+    t->sim = sim;
+    sim->busy = true;
+    DevProblem& d = sim->dp;
+    std::memcpy(b.h, t->rhs.data(), d.n * sizeof(double));
+    cudaMemcpyAsync(d.d_rhs, b.h, d.n * sizeof(double), cudaMemcpyHostToDevice, d.stream);
+    if (!warm) cudaMemsetAsync(d.d_p, 0, d.n * sizeof(double), d.stream);
+    uaamg_options o;
+    uaamg_default_options(&o);
+    o.precision = c.precision;
+    o.tol = c.tol;
+    o.tol_mode = UAAMG_TOL_REL;
+    o.max_iter = c.max_iter;
+    o.replace_every = c.replace_every;
+    o.warm_start = warm ? 1 : 0;
+    t->res.warm = warm ? 1 : 0;
+    t->t_admit = Clock::now();
+    t->res.wait_ms = std::chrono::duration<double, std::milli>(t->t_admit - t->t_submit).count();
+    if (d.eng->solve_begin(d.args(o)) != E_OK) {
+        sim->has_p = false;
+        finish(s, t, UAAMG_CUDA_ERROR);
+        return true;
+    }
+    s->active.push_back(t);
+    return true;
+}
+
+// Advances one running request; true when it finished.
+bool advance(uaamg_server* s, Ticket* t) {
+    DevProblem& d = t->sim->dp;
+    bool stopped = false;
+    int e = d.eng->solve_step();
+    if (e == E_OK) e = d.eng->solve_poll(false, &stopped);
+    if (e == E_OK && !stopped) return false;
+    SolveResult r;
+    std::memset(&r, 0, sizeof(r));
+    if (e == E_OK) e = d.eng->solve_end(&r);
+    if (e != E_OK || d.eng->timed_out()) {
+        t->sim->has_p = false;
+        finish(s, t, e == E_OK ? UAAMG_TIMEOUT : UAAMG_CUDA_ERROR);
+        return true;
+    }
+    StageBuf& b = s->stage[t->slot];
+    cudaError_t ce = cudaSuccess;
+    if (t->req.p_out) {
+        ce = cudaMemcpyAsync(b.h, d.d_p, d.n * sizeof(double), cudaMemcpyDeviceToHost, d.stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(d.stream);
+        if (ce == cudaSuccess) std::memcpy(t->req.p_out, b.h, d.n * sizeof(double));
+    }
+    uaamg_stats st;
+    const uaamg_status status = api::fill_stats(d.eng, r, &st);
+    t->res.iterations = st.iterations;
+    t->res.rel_residual = st.rel_residual;
+    t->sim->has_p = ce == cudaSuccess;
+    finish(s, t, ce == cudaSuccess ? status : UAAMG_CUDA_ERROR);
+    return true;
+}
+
+void worker_main(uaamg_server* s) {
+    cudaSetDevice(s->cfg.device);
+    for (;;) {
+        // admission: FIFO over the queue; a request waits while its id is busy
+        std::vector<Ticket*> admit;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (s->pending.empty() && s->active.empty()) {
+                if (s->stopping) break;
+                s->cv.wait(lk, [&] { return s->stopping || !s->pending.empty(); });
+                continue;
+            }
+            int room = s->cfg.max_active - (int)s->active.size();
+            std::vector<long long> blocked;
+            for (auto it = s->pending.begin(); it != s->pending.end() && room > 0;) {
+                Ticket* t = *it;
+                const long long id = t->req.sim_id;
+                auto sim = s->sims.find(id);
+                bool busy = sim != s->sims.end() && sim->second->busy;
+                for (long long b : blocked) busy = busy || b == id;
+                for (Ticket* a : admit) busy = busy || a->req.sim_id == id;
+                if (busy) {
+                    blocked.push_back(id);
+                    ++it;
+                    continue;
+                }
+                admit.push_back(t);
+                it = s->pending.erase(it);
+                --room;
+            }
+        }
+        for (size_t i = 0; i < admit.size(); ++i) {
+            if (!start_request(s, admit[i])) {
+                // no device room until a running solve finishes: back to the queue front
+                std::lock_guard<std::mutex> lk(s->mu);
+                for (size_t j = admit.size(); j > i; --j) s->pending.push_front(admit[j - 1]);
+                break;
+            }
+        }
+        bool progressed = !admit.empty();
+        for (size_t i = 0; i < s->active.size();) {
+            if (advance(s, s->active[i])) {
+                s->active.erase(s->active.begin() + (long)i);
+                progressed = true;
+            } else {
+                ++i;
+            }
+        }
+        if (!progressed) std::this_thread::yield();
+    }
+}
+
+}  // namespace
+}  // namespace uaamg
+
+extern "C" {
+
+void uaamg_server_default_config(uaamg_server_config* c) {
+    if (!c) return;
+    c->device = 0;
+    c->precision = UAAMG_MIXED;
+    c->tol = 1e-6;
+    c->max_iter = 500;
+    c->replace_every = 10;
+    c->warm_start = 1;
+    c->max_active = 16;
+    c->hbm_budget_bytes = (size_t)150 << 30;
+}
+
+uaamg_status uaamg_server_start(uaamg_server** out, const uaamg_server_config* cfg) {
+    if (!out) return UAAMG_INVALID_ARG;
+    *out = nullptr;
+    uaamg_server_config c;
+    uaamg_server_default_config(&c);
+    if (cfg) c = *cfg;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || c.device < 0 || c.device >= count) {
+        cudaGetLastError();
+        return UAAMG_INVALID_ARG;
+    }
+    if (c.precision < 0 || c.precision > 2 || c.max_active < 1 || c.max_iter < 0 || !(c.tol >= 0) ||
+        c.hbm_budget_bytes == 0)
+        return UAAMG_INVALID_ARG;
+    uaamg_server* s = new (std::nothrow) uaamg_server();
+    if (!s) return UAAMG_OOM;
+    s->cfg = c;
+    s->stage.resize(c.max_active);
+    s->worker = std::thread(uaamg::worker_main, s);
+    *out = s;
+    return UAAMG_OK;
+}
+
+uaamg_status uaamg_server_submit(uaamg_server* s, const uaamg_request* q, long long* ticket) {
+    if (!s || !q || !ticket) return UAAMG_INVALID_ARG;
+    const int nz = q->dim == 3 ? q->nz : 2;
+    if ((q->dim != 2 && q->dim != 3) || q->nx < 2 || q->ny < 2 || nz < 2 || !q->solid || !q->rhs ||
+        !(q->dx > 0) || !(q->dy > 0) || (q->dim == 3 && !(q->dz > 0)))
+        return UAAMG_INVALID_ARG;
+    const size_t n = uaamg::padded_cells(q->dim, q->nx, q->ny, q->nz);
+    if (n >= ((size_t)1 << 31)) return UAAMG_INVALID_ARG;
+    uaamg::Ticket* t = new (std::nothrow) uaamg::Ticket();
+    if (!t) return UAAMG_OOM;
+    t->req = *q;
+    if (q->dim == 2) { t->req.nz = 0; t->req.dz = 1.0; }
+    t->solid.assign(q->solid, q->solid + n);
+    t->rhs.assign(q->rhs, q->rhs + n);
+    t->req.solid = nullptr;
+    t->req.rhs = nullptr;
+    t->t_submit = uaamg::Clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) { delete t; return UAAMG_INVALID_ARG; }
+    t->id = s->next_ticket++;
+    s->tickets[t->id] = t;
+    s->pending.push_back(t);
+    s->outstanding += 1;
+    *ticket = t->id;
+    s->cv.notify_all();
+    return UAAMG_OK;
+}
+
+uaamg_status uaamg_server_poll(uaamg_server* s, long long ticket, uaamg_result* res, int* done) {
+    if (!s || !done) return UAAMG_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->tickets.find(ticket);
+    if (it == s->tickets.end()) return UAAMG_INVALID_ARG;
+    uaamg::Ticket* t = it->second;
+    *done = t->done ? 1 : 0;
+    if (!t->done) return UAAMG_OK;
+    if (res) *res = t->res;
+    s->tickets.erase(it);
+    delete t;
+    return UAAMG_OK;
+}
+
+uaamg_status uaamg_server_drain(uaamg_server* s) {
+    if (!s) return UAAMG_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv.wait(lk, [&] { return s->outstanding == 0; });
+    return UAAMG_OK;
+}
+
+uaamg_status uaamg_server_info(uaamg_server* s, size_t* bytes, int* resident, long long* completed) {
+    if (!s) return UAAMG_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (bytes) *bytes = s->resident_bytes;
+    if (resident) *resident = s->resident;
+    if (completed) *completed = s->completed;
+    return UAAMG_OK;
+}
+
+uaamg_status uaamg_server_stop(uaamg_server* s) {
+    if (!s) return UAAMG_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+        s->cv.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->cfg.device);
+    for (auto& kv : s->sims) {
+        kv.second->dp.release();
+        delete kv.second;
+    }
+    s->sims.clear();
+    for (auto& b : s->stage)
+        if (b.h) cudaFreeHost(b.h);
+    // every ticket not yet released by a poll is in the map (queued or finished)
+    for (auto& kv : s->tickets) delete kv.second;
+    delete s;
+    return UAAMG_OK;
+}
+
+}  // extern "C"

@@ -236,6 +236,108 @@ class Handle:
         self._check(self.lib.uaamg_device_bytes(self.h, C.byref(b)), "device_bytes")
         return b.value
 
+    def set_autotune(self, on: bool):
+        self._check(self.lib.uaamg_set_autotune(self.h, int(bool(on))), "autotune")
+
+    def solve_batch(self, problems, opts: _capi.Options | None = None, strict: bool = False):
+        """uaamg_solve_batch over [(solid, rhs, p, dx, dy, dz), ...] (padded host
+        arrays; each p updated in place).  Returns the list of per-problem stats."""
+        keep, probs = [], (_capi.Problem * max(1, len(problems)))()
+        for q, (solid, rhs, p, dx, dy, dz) in enumerate(problems):
+            solid = np.ascontiguousarray(solid, dtype=np.uint8)
+            rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+            if p.dtype != np.float64 or not p.flags.c_contiguous or p.shape != solid.shape \
+                    or rhs.shape != solid.shape:
+                raise ValueError(f"problem {q}: arrays must share the padded shape, p float64")
+            keep += [solid, rhs]
+            pr = probs[q]
+            pr.dim = solid.ndim
+            if solid.ndim == 3:
+                pr.nz, pr.ny, pr.nx = (v - 2 for v in solid.shape)
+            else:
+                (pr.ny, pr.nx), pr.nz = (v - 2 for v in solid.shape), 0
+            pr.dx, pr.dy, pr.dz = float(dx), float(dy), float(dz)
+            pr.solid, pr.rhs, pr.p = solid.ctypes.data, rhs.ctypes.data, p.ctypes.data
+        stats = (_capi.Stats * max(1, len(problems)))()
+        s = self.lib.uaamg_solve_batch(self.h, len(problems), probs,
+                                       C.byref(opts or self.options()), stats)
+        self._check(s, "solve_batch", (_capi.OK,) if strict else self._SOLVE_OK)
+        return [stats[q] for q in range(len(problems))]
+
+
+class Server:
+    """The serving loop (uaamg_server_*): submit requests of any size; each
+    simulation id keeps its hierarchy and pressure on the device between requests."""
+
+    def __init__(self, device=0, precision="mixed", tol=1e-6, max_iter=500, replace_every=10,
+                 warm_start=True, max_active=16, hbm_budget_bytes=150 << 30):
+        self.lib = _capi.load()
+        cfg = _capi.ServerConfig()
+        self.lib.uaamg_server_default_config(C.byref(cfg))
+        cfg.device, cfg.precision = int(device), _capi.PRECISIONS[precision]
+        cfg.tol, cfg.max_iter, cfg.replace_every = float(tol), int(max_iter), int(replace_every)
+        cfg.warm_start, cfg.max_active = int(bool(warm_start)), int(max_active)
+        cfg.hbm_budget_bytes = int(hbm_budget_bytes)
+        self.s = C.c_void_p()
+        st = self.lib.uaamg_server_start(C.byref(self.s), C.byref(cfg))
+        if st != _capi.OK:
+            raise _capi.UaamgError(st, "server_start")
+        self._keep = {}
+
+    def submit(self, sim_id, solid, rhs, dx, dy, dz=1.0, p_out=None) -> int:
+        """Queues one solve; p_out (padded float64, optional) receives the pressure."""
+        solid = np.ascontiguousarray(solid, dtype=np.uint8)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        q = _capi.Request()
+        q.sim_id, q.dim = int(sim_id), solid.ndim
+        if solid.ndim == 3:
+            q.nz, q.ny, q.nx = (v - 2 for v in solid.shape)
+        else:
+            (q.ny, q.nx), q.nz = (v - 2 for v in solid.shape), 0
+        q.dx, q.dy, q.dz = float(dx), float(dy), float(dz)
+        q.solid, q.rhs = solid.ctypes.data, rhs.ctypes.data
+        if p_out is not None:
+            if p_out.dtype != np.float64 or not p_out.flags.c_contiguous or p_out.shape != solid.shape:
+                raise ValueError("p_out must be a C-contiguous float64 array of the padded shape")
+            q.p_out = p_out.ctypes.data
+        t = C.c_longlong()
+        st = self.lib.uaamg_server_submit(self.s, C.byref(q), C.byref(t))
+        if st != _capi.OK:
+            raise _capi.UaamgError(st, "server_submit")
+        self._keep[t.value] = p_out  # the output buffer must outlive the solve
+        return t.value
+
+    def poll(self, ticket):
+        """The result dict once the ticket finished (and releases it), else None."""
+        res, done = _capi.Result(), C.c_int()
+        st = self.lib.uaamg_server_poll(self.s, int(ticket), C.byref(res), C.byref(done))
+        if st != _capi.OK:
+            raise _capi.UaamgError(st, "server_poll")
+        if not done.value:
+            return None
+        self._keep.pop(int(ticket), None)
+        return res.as_dict()
+
+    def drain(self):
+        self.lib.uaamg_server_drain(self.s)
+
+    def info(self):
+        b, r, c = C.c_size_t(), C.c_int(), C.c_longlong()
+        self.lib.uaamg_server_info(self.s, C.byref(b), C.byref(r), C.byref(c))
+        return {"device_bytes": b.value, "resident": r.value, "completed": c.value}
+
+    def stop(self):
+        if self.s:
+            self.lib.uaamg_server_stop(self.s)
+            self.s = C.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
 
 # ---------------------------------------------------------------------------
 # Solver plug-ins
