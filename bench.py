@@ -29,6 +29,8 @@ import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# many concurrent streams in the batch and serving modes (before any CUDA context)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 sys.path.insert(0, ROOT)
 
 METRIC = "3D 256^3 PCG solve ms (1e-6 rel. residual)"
@@ -370,6 +372,264 @@ def run_ours(args):
     return 0
 
 
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O
+
+
+def run_batch(args):
+    """96 uneven 2D/3D problems solved as one uaamg_solve_batch call (host arrays in
+    and out; a step = the whole batch).  Beside: the same problems one uaamg_solve
+    at a time, and the batch in plain FP32."""
+    import numpy as np
+    import torch
+
+    from uaamg_b200 import workloads
+    from uaamg_b200.solver import Handle
+
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    probs = workloads.batch96()
+    hd = Handle(0)
+    if args.autotune:
+        hd.set_autotune(True)
+    opts = hd.options(args.precision, 1e-6, 500, "rel")
+    ps = [np.zeros_like(r) for _, r, *_ in probs]
+    items = [(s, r, p, dx, dy, dz) for (s, r, dx, dy, dz), p in zip(probs, ps)]
+
+    def step(o):
+        for p in ps:
+            p[...] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        stats = hd.solve_batch(items, o)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3, stats
+
+    for _ in range(args.warmup):
+        step(opts)
+    with ClockSampler(0) as clk:
+        times = []
+        for _ in range(args.steps):
+            t, stats = step(opts)
+            times.append(t)
+    clocks = clk.summary()
+    ms = statistics.mean(times)
+    O = _oracle()
+    rel = [O.true_residual(s, r, p, dx, dy, dz) for (s, r, dx, dy, dz), p in zip(probs, ps)]
+    worst = max(a / b for a, b in rel)
+    iters = [st.iterations for st in stats]
+    # beside: one problem at a time through uaamg_solve, and plain FP32 batched
+    seq = 0.0
+    for (s, r, dx, dy, dz), p in zip(probs, ps):
+        hd.set_problem(s, dx, dy, dz)
+        p[...] = 0.0
+        hd.solve(r, p, opts)  # hierarchy built, graph captured
+        p[...] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hd.solve(r, p, opts)
+        seq += (time.perf_counter() - t0) * 1e3
+    t32, st32 = step(hd.options("fp32", 1e-6, 500, "rel"))
+    cells = sum(int((s[1:-1, 1:-1] if s.ndim == 2 else s[1:-1, 1:-1, 1:-1]).size) for s, *_ in probs)
+    n_bytes = sum(s.size * 17 for s, *_ in probs)
+    line = {
+        "metric": "96-problem uneven batch solve ms (1e-6 rel. residual)", "value": round(ms, 3),
+        "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (FP64 reductions and solution)", "data": "synthetic",
+        "config": {"workload": "batch96: 64 2D (sizes {64..1024}^2) + 32 3D (sizes {32..128}^3) "
+                               "box-obstacle problems, smoothed-noise RHS (seed 20260404)",
+                   "precision": args.precision, "cells": cells, "autotune": bool(args.autotune),
+                   "solves_per_s": round(96 / (ms * 1e-3), 1),
+                   "iterations_min_median_max": [min(iters), int(statistics.median(iters)), max(iters)],
+                   "worst_true_rel_residual": worst,
+                   "timing": "host clock around the blocking batch call (per-problem streams)"},
+        "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": n_bytes,
+                "d2h_bytes_per_step": sum(s.size * 8 for s, *_ in probs)},
+        "clocks": clocks,
+        "beside": {"sequential_ms": round(seq, 3), "batched_speedup": round(seq / ms, 2),
+                   "fp32_batch_ms": round(t32, 3),
+                   "fp32_worst_true_rel_residual": max(
+                       a / b for a, b in (O.true_residual(s, r, p, dx, dy, dz)
+                                          for (s, r, dx, dy, dz), p in zip(probs, ps)))},
+    }
+    print(json.dumps(line), flush=True)
+    hd.close()
+    return 0
+
+
+def _serve_pass(srv, reqs, make, rate=None, max_outstanding=256, check=()):
+    """Submits reqs [(sim_id, step)] to the server: as fast as the producers build
+    them (closed loop, at most max_outstanding in the server), or at Poisson
+    arrivals of `rate` per second (open loop).  Returns (results, wall seconds,
+    {index: (p, solid, rhs, h)} for the indices in `check`)."""
+    import queue
+    import threading
+
+    import numpy as np
+
+    n = len(reqs)
+    arrivals = None
+    if rate:
+        rng = np.random.Generator(np.random.MT19937(20260506))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    work, lock = queue.Queue(), threading.Lock()
+    outstanding, results, kept = {}, [None] * n, {}
+    slots = threading.Semaphore(max_outstanding)
+    t_start = time.perf_counter()
+    done_submitting = threading.Event()
+
+    def producer():
+        while True:
+            item = work.get()
+            if item is None:
+                return
+            i, t_arr = item
+            sid, step = reqs[i]
+            solid, rhs, h = make(sid, step)
+            p = np.zeros_like(rhs) if i in check else None
+            t_sub = time.perf_counter()
+            tk = srv.submit(sid, solid, rhs, h, h, h if solid.ndim == 3 else 1.0, p_out=p)
+            with lock:
+                outstanding[tk] = (i, t_arr, t_sub)
+                if p is not None:
+                    kept[i] = (p, solid, rhs, h)
+
+    def poller():
+        while True:
+            with lock:
+                items = list(outstanding.items())
+            if not items and done_submitting.is_set():
+                return
+            for tk, (i, t_arr, t_sub) in items:
+                r = srv.poll(tk)
+                if r is None:
+                    continue
+                r["queue_host_ms"] = (t_sub - t_arr) * 1e3
+                r["total_ms"] = r["queue_host_ms"] + r["latency_ms"]
+                results[i] = r
+                with lock:
+                    del outstanding[tk]
+                slots.release()
+            time.sleep(0.0002)
+
+    prods = [threading.Thread(target=producer) for _ in range(6)]
+    pol = threading.Thread(target=poller)
+    for th in prods:
+        th.start()
+    pol.start()
+    for i in range(n):
+        if arrivals is not None:
+            wait = t_start + arrivals[i] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            t_arr = t_start + arrivals[i]
+        else:
+            slots.acquire()
+            t_arr = time.perf_counter()
+        if arrivals is not None:
+            slots.acquire()
+        work.put((i, t_arr))
+    for _ in prods:
+        work.put(None)
+    for th in prods:
+        th.join()
+    done_submitting.set()
+    pol.join()
+    wall = time.perf_counter() - t_start
+    return results, wall, kept
+
+
+def run_serve(args):
+    """10,000 served requests (500 simulation ids x 20 steps): closed-loop capacity,
+    then open-loop Poisson arrivals at 80 % of it; p50/p99 latency, solves/s."""
+    import concurrent.futures as cf
+
+    import numpy as np
+    import torch
+
+    from uaamg_b200 import workloads
+    from uaamg_b200.solver import Server
+
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    n_ids, steps = args.serve_ids, args.serve_steps
+    plan = workloads.serve_plan(n_ids, steps)
+    with cf.ThreadPoolExecutor(8) as ex:
+        fields = list(ex.map(lambda q: workloads.serve_fields(q[1], q[2], q[3]), plan))
+
+    def make(sid, t):
+        solid, r0, r1 = fields[sid]
+        return solid, r0 + (t / steps) * r1, 1.0 / plan[sid][2]
+
+    reqs = [(sid, t) for t in range(steps) for sid in range(n_ids)]
+    rng = np.random.Generator(np.random.MT19937(7))
+    check = set(int(i) for i in rng.choice(len(reqs), 24, replace=False))
+    O = _oracle()
+
+    def summary(res, wall):
+        lat = np.array([r["total_ms"] for r in res])
+        return {"solves_per_s": round(len(res) / wall, 1),
+                "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "mean_iterations": round(float(np.mean([r["iterations"] for r in res])), 2),
+                "warm_fraction": round(float(np.mean([r["warm"] for r in res])), 3),
+                "max_reported_rel_residual": max(r["rel_residual"] for r in res),
+                "all_ok": all(r["status"] == 0 for r in res)}
+
+    out = {}
+    for prec in ([args.precision, "fp32"] if not args.no_beside else [args.precision]):
+        srv = Server(0, prec, 1e-6, 500, max_active=args.serve_active)
+        # warm-up: every id's hierarchy and graph, not timed
+        _serve_pass(srv, [(sid, 0) for sid in range(n_ids)], make)
+        closed, wall_c, _ = _serve_pass(srv, reqs, make)
+        cap = len(reqs) / wall_c
+        entry = {"closed_loop": summary(closed, wall_c)}
+        if prec == args.precision:
+            srv.stop()
+            srv = Server(0, prec, 1e-6, 500, max_active=args.serve_active)
+            _serve_pass(srv, [(sid, 0) for sid in range(n_ids)], make)
+            with ClockSampler(0) as clk:
+                opened, wall_o, kept = _serve_pass(srv, reqs, make, rate=0.8 * cap, check=check)
+            entry["open_loop"] = summary(opened, wall_o)
+            entry["open_loop"]["arrival_rate_per_s"] = round(0.8 * cap, 1)
+            entry["clocks"] = clk.summary()
+            entry["info"] = srv.info()
+            worst = 0.0
+            for i, (p, solid, rhs, h) in kept.items():
+                a, b = O.true_residual(solid, rhs, p, h, h, h if solid.ndim == 3 else 1.0)
+                worst = max(worst, a / b)
+            entry["checked_true_rel_residual_max"] = worst
+            entry["checked_requests"] = len(kept)
+        srv.stop()
+        out[prec] = entry
+    main_ = out[args.precision]
+    line = {
+        "metric": "served pressure solves/s and p99 latency (1e-6 rel. residual)",
+        "value": main_["open_loop"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "steps": len(reqs), "warmup": n_ids, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (FP64 reductions and solution)", "data": "synthetic",
+        "config": {"workload": f"serve10k: {n_ids} simulation ids x {steps} steps, 70% 2D n^2 "
+                               "(n lognormal median 384, [64, 2048]), 30% 3D n^3 (median 96, "
+                               "[32, 256]), obstacle disk/sphere, evolving RHS (seed 20260505)",
+                   "precision": args.precision, "max_active": args.serve_active,
+                   "hbm_budget_gb": 150, "warm_start": True,
+                   "p50_ms": main_["open_loop"]["p50_ms"], "p99_ms": main_["open_loop"]["p99_ms"],
+                   "latency": "scheduled arrival -> result on the host"},
+        "e2e": {"value": main_["open_loop"]["solves_per_s"], "unit": "solves/s",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "forms": out,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -379,9 +639,19 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-beside", action="store_true")
+    ap.add_argument("--workload", default="spheres_256",
+                    choices=["spheres_256", "batch96", "serve10k"])
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--serve-ids", type=int, default=500)
+    ap.add_argument("--serve-steps", type=int, default=20)
+    ap.add_argument("--serve-active", type=int, default=16)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch96":
+        return run_batch(args)
+    if args.workload == "serve10k":
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -49,6 +49,7 @@ struct DevProblem {
     double* d_p = nullptr;
     cudaStream_t stream = nullptr;
     bool built = false;
+    std::vector<uint8_t> mask;  // host copy of the mask the hierarchy was built for
 
     size_t bytes() const { return (eng ? eng->device_bytes() : 0) + n * (1 + 16); }
 
@@ -64,6 +65,7 @@ struct DevProblem {
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
         built = false;
+        mask.clear();
         n = 0;
         prec = -1;
     }
@@ -97,13 +99,20 @@ struct DevProblem {
         return E_OK;
     }
 
-    // Mask upload + hierarchy (blocking on the problem's stream).
+    // Mask upload + hierarchy (blocking on the problem's stream); kept, with the
+    // engine's captured CUDA graph, while the mask does not change (as the
+    // reference's GPU adapter re-uploads its mask only on a resize,
+    // cuda_pcg_solver.cu:45-49).
     int build(const uint8_t* solid_host) {
+        if (built && mask.size() == n && std::memcmp(mask.data(), solid_host, n) == 0) return E_OK;
         if (cudaMemcpyAsync(d_solid, solid_host, n, cudaMemcpyHostToDevice, stream) != cudaSuccess)
             return E_CUDA;
         built = false;
         int e = eng->set_problem(dim, nx, ny, nz, dx, dy, dz, d_solid, dirichlet);
-        if (e == E_OK) built = true;
+        if (e == E_OK) {
+            built = true;
+            mask.assign(solid_host, solid_host + n);
+        }
         return e;
     }
 

@@ -391,3 +391,94 @@ WL_API long wl_obstacle_flow_3d(int nx, int ny, int nz, double dx, double dy, do
             }
     return nsolid;
 }
+
+// Serving workload, one simulation id: an n x n (2D) or n^3 (3D) box, h = 1/n, with
+// a disk / sphere of radius 0.05 n cells at (0.25 n, 0.5 n[, 0.5 n]) (cell centres
+// strictly inside are solid), and two right-hand sides rhs0, rhs1 = div(u)/dt of
+// two seeded velocity fields u = sum over 0 < |k| <= kmax of modes with N(0,1)/|k|^2
+// cosine and sine amplitudes per component (dt = 1e-3), evaluated in closed form
+// at cell centres: with phi = 2 pi k.x / L,
+//   div u = sum_k (2 pi / L) [ -(k.A_k) sin phi + (k.B_k) cos phi ].
+// A request at step t of the id uses rhs0 + (t / 20) rhs1 (an evolving field).
+// Both are zero at solids with zero fluid mean.  Separable evaluation: the
+// per-axis cosine/sine tables combine per row, so a cell costs 6 flops per mode.
+WL_API long wl_serve_fields(int dim, int n, int kmax, uint64_t seed, uint8_t* solid, double* rhs0,
+                            double* rhs1) {
+    const int nz = dim == 3 ? n : 0;
+    const size_t N = (size_t)(n + 2) * (n + 2) * (dim == 3 ? (size_t)(n + 2) : 1);
+    std::memset(solid, 0, N);
+    long nsolid = 0;
+    const double c0 = 0.25 * n, c1 = 0.5 * n, rad = 0.05 * n;
+    for (int k = dim == 3 ? 1 : 0; k <= nz; ++k)
+        for (int j = 1; j <= n; ++j)
+            for (int i = 1; i <= n; ++i) {
+                const double x = i - 0.5 - c0, y = j - 0.5 - c1, z = dim == 3 ? k - 0.5 - c1 : 0.0;
+                if (x * x + y * y + z * z < rad * rad) { solid[pid(n, n, i, j, k)] = 1; ++nsolid; }
+            }
+    std::mt19937_64 eng(seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    std::vector<int> kx, ky, kz;
+    const int kzr = dim == 3 ? kmax : 0;
+    for (int a = -kmax; a <= kmax; ++a)
+        for (int b = -kmax; b <= kmax; ++b)
+            for (int c = -kzr; c <= kzr; ++c) {
+                const int kk = a * a + b * b + c * c;
+                if (kk == 0 || kk > kmax * kmax) continue;
+                kx.push_back(a); ky.push_back(b); kz.push_back(c);
+            }
+    const size_t M = kx.size();
+    const double two_pi_l = 2.0 * M_PI / n, dt = 1e-3;
+    for (int field = 0; field < 2; ++field) {
+        std::vector<double> P(M), Q(M);  // div u = sum P sin(phi) + Q cos(phi)
+        for (size_t q = 0; q < M; ++q) {
+            const double kk = (double)(kx[q] * kx[q] + ky[q] * ky[q] + kz[q] * kz[q]);
+            const int kc[3] = {kx[q], ky[q], kz[q]};
+            double ka = 0, kb = 0;
+            for (int comp = 0; comp < dim; ++comp) {
+                const double A = nd(eng) / kk, B = nd(eng) / kk;
+                ka += kc[comp] * A;
+                kb += kc[comp] * B;
+            }
+            P[q] = -two_pi_l * ka / dt;
+            Q[q] = two_pi_l * kb / dt;
+        }
+        // per-axis tables of cos / sin (2 pi k x / L) at cell centres x = i - 0.5
+        auto table = [&](const std::vector<int>& kv, std::vector<double>& ct, std::vector<double>& st) {
+            ct.assign(M * (n + 2), 1.0);
+            st.assign(M * (n + 2), 0.0);
+            for (size_t q = 0; q < M; ++q)
+                for (int i = 1; i <= n; ++i) {
+                    const double ph = two_pi_l * kv[q] * (i - 0.5);
+                    ct[q * (n + 2) + i] = std::cos(ph);
+                    st[q * (n + 2) + i] = std::sin(ph);
+                }
+        };
+        std::vector<double> cxt, sxt, cyt, syt, czt, szt;
+        table(kx, cxt, sxt);
+        table(ky, cyt, syt);
+        if (dim == 3) table(kz, czt, szt);
+        std::vector<double> f(N, 0.0), cr(M), sr(M);
+        for (int k = dim == 3 ? 1 : 0; k <= nz; ++k)
+            for (int j = 1; j <= n; ++j) {
+                for (size_t q = 0; q < M; ++q) {  // phase of the row: phi_y + phi_z
+                    const double cy = cyt[q * (n + 2) + j], sy = syt[q * (n + 2) + j];
+                    const double cz = dim == 3 ? czt[q * (n + 2) + k] : 1.0;
+                    const double sz = dim == 3 ? szt[q * (n + 2) + k] : 0.0;
+                    cr[q] = cy * cz - sy * sz;
+                    sr[q] = sy * cz + cy * sz;
+                }
+                double* row = &f[pid(n, n, 0, j, k)];
+                for (int i = 1; i <= n; ++i) {
+                    double acc = 0.0;
+                    for (size_t q = 0; q < M; ++q) {
+                        const double cx = cxt[q * (n + 2) + i], sx = sxt[q * (n + 2) + i];
+                        acc += P[q] * (sx * cr[q] + cx * sr[q]) + Q[q] * (cx * cr[q] - sx * sr[q]);
+                    }
+                    row[i] = acc;
+                }
+            }
+        finish_rhs(f, solid, dim, n, n, nz);
+        std::memcpy(field == 0 ? rhs0 : rhs1, f.data(), N * sizeof(double));
+    }
+    return nsolid;
+}

@@ -9,6 +9,13 @@ Every generator returns padded numpy arrays in the reference's memory order
 * ``obstacle_2d``: 2048 x 1024, dx = 1e-3, dy = 1.5e-3, disk of radius 0.05*Ly at
   (0.25 Lx, 0.5 Ly); u = 1 + Fourier modes |k| <= 16 with N(0,1)/|k|^2
   amplitudes, v = modes; RHS = div(u)/dt, dt = 1e-3; seed 20260202.
+* ``batch96``: 64 2D problems with nx, ny uniform on {64, 128, ..., 1024} and 32 3D
+  problems with nx, ny, nz uniform on {32, 48, 64, 96, 128}; h = 1/max(dims);
+  random solid boxes up to a coverage U[0, 0.2]; smoothed-noise RHS; seed 20260404.
+* ``serve10k``: 500 simulation ids x 20 steps; 70 % 2D n x n with
+  n = clip(round(exp(N(ln 384, 0.5))), 64, 2048), 30 % 3D n^3 with
+  n = clip(round(exp(N(ln 96, 0.4))), 32, 256); obstacle disk / sphere; RHS of step
+  t = rhs0 + (t/20) rhs1 (wl_serve_fields); seed 20260505.
 """
 from __future__ import annotations
 
@@ -38,6 +45,8 @@ def _load():
         L.wl_obstacle_flow_2d.restype = C.c_long
         L.wl_obstacle_flow_3d.argtypes = [i, i, i, d, d, d, d, i, u64, d, p, p, p, p, p]
         L.wl_obstacle_flow_3d.restype = C.c_long
+        L.wl_serve_fields.argtypes = [i, i, i, u64, p, p, p]
+        L.wl_serve_fields.restype = C.c_long
         _lib = L
     return _lib
 
@@ -94,3 +103,46 @@ def obstacle_2d():
     dx, dy, dt = 1.0e-3, 1.5e-3, 1.0e-3
     s, u, v, r = obstacle_flow_2d(2048, 1024, dx, dy, dt)
     return s, u, v, r, dx, dy, dt
+
+
+def serve_fields(dim, n, seed, kmax=None):
+    """One serving simulation id: (solid, rhs0, rhs1), see wl_serve_fields."""
+    kmax = kmax if kmax is not None else (4 if dim == 2 else 2)
+    shape = (n + 2, n + 2, n + 2) if dim == 3 else (n + 2, n + 2)
+    solid = np.zeros(shape, np.uint8)
+    r0 = np.zeros(shape)
+    r1 = np.zeros(shape)
+    _load().wl_serve_fields(dim, n, kmax, seed, _p(solid), _p(r0), _p(r1))
+    return solid, r0, r1
+
+
+def batch96(seed=20260404):
+    """The 96 uneven batch problems: list of (solid, rhs, dx, dy, dz)."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    out = []
+    sizes2 = list(range(64, 1025, 64))
+    sizes3 = [32, 48, 64, 96, 128]
+    for q in range(96):
+        if q < 64:
+            nx, ny, nz, dim = int(rng.choice(sizes2)), int(rng.choice(sizes2)), 0, 2
+        else:
+            dim = 3
+            nx, ny, nz = (int(rng.choice(sizes3)) for _ in range(3))
+        cov = float(rng.uniform(0.0, 0.2))
+        s, r = boxes(dim, nx, ny, nz, cov, seed + 1 + q)
+        h = 1.0 / max(nx, ny, nz)
+        out.append((s, r, h, h, h if dim == 3 else 1.0))
+    return out
+
+
+def serve_plan(n_ids=500, steps=20, seed=20260505):
+    """The serving mix: list of (sim_id, dim, n, field_seed) for every id."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    plan = []
+    for sid in range(n_ids):
+        if rng.uniform() < 0.7:
+            dim, n = 2, int(np.clip(round(float(np.exp(rng.normal(np.log(384), 0.5)))), 64, 2048))
+        else:
+            dim, n = 3, int(np.clip(round(float(np.exp(rng.normal(np.log(96), 0.4)))), 32, 256))
+        plan.append((sid, dim, n, seed * 1000 + sid))
+    return plan
