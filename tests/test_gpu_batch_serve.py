@@ -121,3 +121,21 @@ def test_small_budget_evicts_idle_simulations():
     assert info["resident"] <= 2
     assert all(res["status"] == 0 for _, res, _, _ in out.values())
     assert any(res["warm"] == 0 for (sid, t), (_, res, _, _) in out.items() if t == 1)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_autotuned_chunks_give_identical_results(prec):
+    # the z-chunk length changes only the blocks' shape, never the arithmetic
+    s, r = workloads.spheres_3d(80, 64, 72, 12, 3.0, 9.0, seed=11)
+    h = 1.0 / 80
+    out = []
+    for tune in (False, True):
+        hd = Handle(0)
+        hd.set_autotune(tune)
+        hd.set_problem(s, h, h, h)
+        p = np.zeros_like(r)
+        st = hd.solve(r, p, hd.options(prec, 1e-6, 300, "rel"), strict=True)
+        out.append((p, st.iterations))
+        hd.close()
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])

@@ -92,6 +92,7 @@ uaamg_status engine_for(uaamg_handle* h, int p, uaamg::Engine** out) {
     }
     h->eng[p]->set_stream(h->stream);
     h->eng[p]->set_vcycle_sweeps(h->sweeps != 0);
+    h->eng[p]->set_autotune(h->autotune != 0);
     if (!h->ready[p]) {
         int e = h->eng[p]->set_problem(h->dim, h->nx, h->ny, h->nz, h->dx, h->dy, h->dz,
                                        h->d_solid, h->dirichlet);

@@ -14,6 +14,9 @@
 // make_geom_pitched); the caller's arrays use the reference layout and are
 // converted on the way in (rhs, warm-start p, preconditioner input) and out.
 #pragma once
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -433,7 +436,7 @@ private:
         // reductions: the finest-level marches (one partial per block) and the
         // row-walk kernels (vec_grid)
         {
-            const dim3 mg = march_grid<DIM>(g0, lv_[0].zc);
+            const dim3 mg = march_grid<DIM>(g0, 2);  // the most blocks any chunk length gives
             reduce_blocks_ = (long long)mg.x * mg.y * mg.z;
             if (reduce_blocks_ < max_reduce_blocks()) reduce_blocks_ = max_reduce_blocks();
         }
@@ -498,7 +501,62 @@ private:
         for (int l = 0; l < nl; ++l)
             UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_codes<DIM>, vec_grid(lv_[l].g), dim3(32, 8),
                          lv_[l].g, lv_[l].solid, lv_[l].code, l == 0 ? 1 : 0);
-        return sync_check();
+        if ((e = sync_check()) != E_OK) return e;
+        if (DIM == 3 && autotune_) return tune<DIM>();
+        return E_OK;
+    }
+
+    // Autotuner: for every level with marches, time its four V-cycle marches
+    // (down and up, on the level's own buffers) for each z-chunk length in
+    // {2, 4, 8, 16, 32} and keep the fastest; the choice is cached per level shape
+    // and precision for the process.  Chunk length changes only the blocks' shape,
+    // not the arithmetic, so the results do not depend on it.
+    template <int DIM>
+    int tune() {
+        static std::mutex mu;
+        static std::map<std::tuple<int, int, int, int, int, int>, int> cache;
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return E_CUDA;
+        const bool prof = prof_on_;
+        prof_on_ = false;
+        int e = E_OK;
+        for (int l = 0; l + 1 < (int)lv_.size() && e == E_OK; ++l) {
+            LevelBuf<T>& L = lv_[l];
+            const auto key = std::make_tuple((int)sizeof(T), mixed_ ? 1 : 0, L.g.nx, L.g.ny, L.g.nz,
+                                             l == 0 ? 1 : 0);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                auto it = cache.find(key);
+                if (it != cache.end()) { L.zc = it->second; continue; }
+            }
+            int best = L.zc;
+            float best_ms = 1e30f;
+            for (int zc = 2; zc <= 32 && e == E_OK; zc *= 2) {
+                if (zc > 2 && zc / 2 >= L.g.nz) break;
+                L.zc = zc;
+                for (int rep = 0; rep < 3; ++rep) {  // rep 0 warms up
+                    if (rep == 1) cudaEventRecord(a, st_);
+                    if (l == 0) { down_level<DIM, true>(l, nullptr); up_level<DIM, true>(l, nullptr, false); }
+                    else { down_level<DIM, false>(l, nullptr); up_level<DIM, false>(l, nullptr, false); }
+                }
+                cudaEventRecord(b, st_);
+                float ms = 0.f;
+                if (cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+                    e = sync_check();
+                    if (e == E_OK) e = E_CUDA;
+                    break;
+                }
+                if (ms < best_ms) { best_ms = ms; best = zc; }
+            }
+            L.zc = best;
+            std::lock_guard<std::mutex> lk(mu);
+            cache[key] = best;
+        }
+        prof_on_ = prof;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (e == E_OK) e = sync_check();
+        return e;
     }
 
     LevelView<T> view(int l, const T* r, T* z) const {
