@@ -38,6 +38,20 @@ WORKLOAD = ("spheres_256: 256^3 7-point Neumann Poisson, h=1/256, 32 seeded soli
             "r~U[8,24] cells, RHS = N(0,1) noise blurred sigma=4 cells, zero at solids, "
             "zero fluid mean (seed 20260303)")
 REF_ITER_FIXTURE = os.path.join(ROOT, "tests", "golden", "spheres_256_reference.json")
+METRIC_2D = "2D 2048x1024 projection PCG solve ms (1e-6 rel. residual)"
+WORKLOAD_2D = ("obstacle_2d: 2048x1024 MAC grid, dx=1e-3, dy=1.5e-3, Neumann walls, disk of "
+               "radius 0.05*Ly at (0.25 Lx, 0.5 Ly), RHS = div(u)/dt of u = 1 + Fourier modes "
+               "|k|<=16 with N(0,1)/|k|^2 amplitudes, dt=1e-3 (seed 20260202)")
+
+
+def _problem(name):
+    """(solid, rhs, dx, dy, dz, metric, workload) of a single-solve workload."""
+    from uaamg_b200 import workloads
+    if name == "obstacle_2d":
+        solid, _, _, rhs, dx, dy, _ = workloads.obstacle_2d()
+        return solid, rhs, dx, dy, 1.0, METRIC_2D, WORKLOAD_2D
+    solid, rhs, h = workloads.spheres_256()
+    return solid, rhs, h, h, h, METRIC, WORKLOAD
 
 
 def _peaks():
@@ -168,7 +182,7 @@ def run_reference(args):
     return 0
 
 
-def cpu_baseline_sample(solid, rhs, h, n_it):
+def cpu_baseline_sample(solid, rhs, h, n_it, dx=None, dy=None, dz=None):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -177,12 +191,12 @@ def cpu_baseline_sample(solid, rhs, h, n_it):
     tol_abs = 1e-6 * float((b[solid == 0] ** 2).sum()) ** 0.5
     t0 = time.perf_counter()
     if kind == "reference":
-        O.ref_pcg(solid, rhs, h, h, h, max_iter=1, tol=tol_abs)
+        O.ref_pcg(solid, rhs, dx or h, dy or h, dz or h, max_iter=1, tol=tol_abs)
     else:
-        O.pcg(solid, rhs, h, h, h, max_iter=1, tol=tol_abs, tol_mode=0)
+        O.pcg(solid, rhs, dx or h, dy or h, dz or h, max_iter=1, tol=tol_abs, tol_mode=0)
     t = (time.perf_counter() - t0) * 1e3
     return {"value": round(t * n_it / 2.0, 1), "unit": "ms", "cores": 1, "kind": kind,
-            "sample": (f"one PCG iteration of the same 256^3 solve (2 V-cycle applications), "
+            "sample": (f"one PCG iteration of the same solve (2 V-cycle applications), "
                        f"single thread, {t / 1e3:.1f} s; full solve = sample x {n_it}/2")}
 
 
@@ -203,9 +217,10 @@ def run_ours(args):
     from uaamg_b200 import _capi, workloads
     from uaamg_b200.solver import Handle
 
-    solid, rhs, h = workloads.spheres_256()
+    solid, rhs, dx, dy, dz, metric, workload = _problem(args.workload)
+    h = dx
     hd = Handle(device)
-    hd.set_problem(solid, h, h, h)
+    hd.set_problem(solid, dx, dy, dz)
     opts = hd.options(args.precision, 1e-6, 500, "rel", replace_every=10)
     d_rhs = torch.from_numpy(rhs).to(f"cuda:{device}")
     d_p = torch.zeros_like(d_rhs)
@@ -273,7 +288,7 @@ def run_ours(args):
     # true residual of the e2e result, recomputed in FP64 on the host (oracle)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    res, bn = O.true_residual(solid, rhs, p_np, h, h, h)
+    res, bn = O.true_residual(solid, rhs, p_np, dx, dy, dz)
 
     # in-situ per-kernel timing (one extra, unmeasured solve)
     d_p.zero_()
@@ -289,7 +304,7 @@ def run_ours(args):
     achieved = top["bytes_per_launch"] / (avg_ms * 1e-3) / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tfile):
+    if os.path.exists(tfile) and args.workload == "spheres_256":  # captured on this workload
         try:
             tk = json.load(open(tfile))
             key = f"{top['name']}@L{top['level']}"
@@ -334,11 +349,11 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        if os.path.exists(REF_ITER_FIXTURE):
+        if args.workload == "spheres_256" and os.path.exists(REF_ITER_FIXTURE):
             n_it = _ref_iterations()["iterations"]
         else:  # the FP64 GPU path runs the reference's iteration sequence
             n_it = beside.get("fp64", {}).get("iterations", stats["iterations"])
-        cpu = cpu_baseline_sample(solid, rhs, h, n_it)
+        cpu = cpu_baseline_sample(solid, rhs, h, n_it, dx, dy, dz)
 
     if ws > 1:
         import torch.distributed as dist
@@ -347,16 +362,17 @@ def run_ours(args):
     if rank != 0:
         return 0
     line = {
-        "metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": ws,
+        "metric": metric, "value": round(value, 4), "unit": "ms", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (FP64 reductions and solution)", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "precision": args.precision, "tol": 1e-6,
+        "config": {"workload": workload, "precision": args.precision, "tol": 1e-6,
                    "tol_rule": "FP64 true ||b-Ax||/||b||", "replace_every": 10,
                    "iterations": stats["iterations"],
                    "true_rel_residual": stats["rel_residual"],
                    "host_checked_rel_residual": res / bn,
-                   "l2": "inputs larger than L2 (solve working set ~1.2 GB vs 126 MB L2)",
+                   "l2": f"inputs larger than L2 (solve working set ~{hd.device_bytes() / 1e9:.2f} GB "
+                         "vs 126 MB L2)",
                    "parallelism": f"replicas x{ws}"},
         "roofline": roofline,
         "cpu_baseline": cpu,
@@ -640,7 +656,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-beside", action="store_true")
     ap.add_argument("--workload", default="spheres_256",
-                    choices=["spheres_256", "batch96", "serve10k"])
+                    choices=["spheres_256", "obstacle_2d", "batch96", "serve10k"])
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--serve-ids", type=int, default=500)
     ap.add_argument("--serve-steps", type=int, default=20)

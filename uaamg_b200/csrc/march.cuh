@@ -278,6 +278,39 @@ __device__ __forceinline__ bool step_barrier(bool ok, int* err) {
     return false;
 }
 
+// A x of one cell in FP32, as a sum of couplings times differences,
+// sum_n c_n (x - x_n) (+ the Dirichlet wall share of the diagonal times x): the
+// same value as d x - sum_n c_n x_n in exact arithmetic, but the differences of
+// nearby values are exact in floating point, so smooth fields keep their relative
+// accuracy instead of cancelling d x against the neighbour sum (an error of
+// eps / (k h)^2, several per cent on the smoothest modes of a 2048 x 1024 grid).
+// On the finest level a term exists where the code bit says the coupling does.
+template <int DIM, class T, bool FINE>
+__device__ __forceinline__ T fp32_ax(const MLevel<T>& L, uint32_t c, T d, const T (&cc)[6], T x,
+                                     T xr, T xl, T xt, T xb, T xk, T xf) {
+    if constexpr (FINE) {
+        const T tx = ((c & 1u) ? x - xr : T(0)) + ((c & 2u) ? x - xl : T(0));
+        const T ty = ((c & 4u) ? x - xt : T(0)) + ((c & 8u) ? x - xb : T(0));
+        T ax = tx * L.idx2 + ty * L.idy2;
+        T sum = ((c & 1u) ? L.idx2 : T(0)) + ((c & 2u) ? L.idx2 : T(0)) +
+                ((c & 4u) ? L.idy2 : T(0)) + ((c & 8u) ? L.idy2 : T(0));
+        if (DIM == 3) {
+            const T tz = ((c & 16u) ? x - xk : T(0)) + ((c & 32u) ? x - xf : T(0));
+            ax = ax + tz * L.idz2;
+            sum = sum + ((c & 16u) ? L.idz2 : T(0)) + ((c & 32u) ? L.idz2 : T(0));
+        }
+        return ax + (d - sum) * x;  // d - sum: the Dirichlet wall share (0 with Neumann walls)
+    } else {
+        T ax = cc[0] * (x - xr) + cc[1] * (x - xl) + cc[2] * (x - xt) + cc[3] * (x - xb);
+        T sum = cc[0] + cc[1] + cc[2] + cc[3];
+        if (DIM == 3) {
+            ax = ax + cc[4] * (x - xk) + cc[5] * (x - xf);
+            sum = sum + cc[4] + cc[5];
+        }
+        return ax + (d - sum) * x;  // d - sum: the Galerkin wall channel (0 with Neumann walls)
+    }
+}
+
 // Per-march ring depth and dynamic shared-memory size.
 template <int DIM, class T, bool FINE> struct FwdCfg {
     using P = MPlan<DIM, T, false, !FINE, false>;
@@ -522,11 +555,17 @@ __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant
                 const T d = mdiag<DIM, T, P, FINE>(L, lut, sg.c, c, q, o.i, o.j + e, k);
                 T cc[6];
                 mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
-                T ax = d * xb[q] - cc[0] * xb[q + 1] - cc[1] * xb[q - 1] - cc[2] * xb[q + W] -
-                       cc[3] * xb[q - W];
-                if (DIM == 3)
-                    ax = ax - cc[4] * boxv<T>(sg.n, P::QX * P::VB, q) -
-                         cc[5] * boxv<T>(sg.m, P::QX * P::VB, q);
+                const T xp = DIM == 3 ? boxv<T>(sg.n, P::QX * P::VB, q) : T(0);
+                const T xm = DIM == 3 ? boxv<T>(sg.m, P::QX * P::VB, q) : T(0);
+                T ax;
+                if constexpr (sizeof(T) == 8) {  // the reference's expression (bit-exact)
+                    ax = d * xb[q] - cc[0] * xb[q + 1] - cc[1] * xb[q - 1] - cc[2] * xb[q + W] -
+                         cc[3] * xb[q - W];
+                    if (DIM == 3) ax = ax - cc[4] * xp - cc[5] * xm;
+                } else {
+                    ax = fp32_ax<DIM, T, FINE>(L, c, d, cc, xb[q], xb[q + 1], xb[q - 1], xb[q + W],
+                                               xb[q - W], xp, xm);
+                }
                 rv[e] = boxv<T>(sg.c, P::QB * P::VB, q) - ax;
             }
         }
@@ -809,9 +848,13 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
                 if (DIM == 3) {
                     const T vF = (c & 32u) ? pv(sg.m, q) : (k > 1 ? p0 : wall);
                     const T vK = (c & 16u) ? pv(sg.n, q) : (k < g.nz ? p0 : wall);
-                    a_[e] = diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
+                    a_[e] = sizeof(T) == 8
+                                ? diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2
+                                : ((p0 - vL) + (p0 - vR)) * idx2 + ((p0 - vB) + (p0 - vT)) * idy2 +
+                                      ((p0 - vF) + (p0 - vK)) * idz2;
                 } else {
-                    a_[e] = diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2;
+                    a_[e] = sizeof(T) == 8 ? diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2
+                                           : ((p0 - vL) + (p0 - vR)) * idx2 + ((p0 - vB) + (p0 - vT)) * idy2;
                 }
                 acc[0] += (double)p0 * (double)a_[e];
             }
