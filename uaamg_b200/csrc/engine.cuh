@@ -17,6 +17,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -28,12 +29,13 @@
 namespace uaamg {
 namespace {
 
-template <class T>
+template <class T, class CS>
 struct LevelBuf {
     Geom g;
     double hx, hy, hz;
     uint8_t* solid = nullptr;
     T *cx = nullptr, *cy = nullptr, *cz = nullptr, *wd = nullptr, *dg = nullptr;
+    CS *hcx = nullptr, *hcy = nullptr, *hcz = nullptr;  // couplings as the marches read them
     T *x = nullptr, *b = nullptr;  // level >= 1 only (level 0 uses the CG's r and z)
     uint8_t* code = nullptr;       // cell codes (vec.cuh k_codes)
     int zc = 2;                    // planes per block of the z marches (march.cuh)
@@ -71,8 +73,12 @@ struct KTag {
 #define UAAMG_LAUNCH(tag, kern, grid, block, ...) \
     UAAMG_LAUNCH_SMEM(tag, kern, grid, block, 0, __VA_ARGS__)
 
-template <class T>
+// CS: storage type of the coarse-level couplings the marches read (T, or __half
+// in the mixed form: face counts with a per-axis scale).
+template <class T, class CS = T>
 class EngineT final : public Engine {
+    static constexpr bool kHalf = !std::is_same<CS, T>::value;
+
 public:
     explicit EngineT(bool mixed) : mixed_(mixed) {}
     ~EngineT() override {
@@ -161,7 +167,7 @@ public:
     // Host copies in the reference layout of level l (row pitch nx_l + 2).
     int copy_level(int l, uint8_t* solid, double* cx, double* cy, double* cz) override {
         if (l < 0 || l >= (int)lv_.size()) return E_ARG;
-        const LevelBuf<T>& L = lv_[l];
+        const LevelBuf<T, CS>& L = lv_[l];
         const Geom g = L.g;
         const Geom gr = make_geom(dim_, g.nx, g.ny, g.nz);
         if (cudaStreamSynchronize(st_) != cudaSuccess) return E_CUDA;
@@ -245,7 +251,7 @@ private:
     int dim_ = 0, dirichlet_ = 0;
     double dx_ = 1, dy_ = 1, dz_ = 1;
     Geom gref_;                      // the caller's (reference) layout of level 0
-    std::vector<LevelBuf<T>> lv_;
+    std::vector<LevelBuf<T, CS>> lv_;
     T *r_ = nullptr, *z_ = nullptr, *p_ = nullptr, *p2_ = nullptr, *ap_ = nullptr, *xlo_ = nullptr;
     double *b64_ = nullptr, *xd_ = nullptr, *partials_ = nullptr;
     int* err_ = nullptr;             // set by a kernel whose TMA wait gave up
@@ -379,11 +385,11 @@ private:
     template <int DIM, bool FINE>
     int march_attrs() {
         int e;
-        if ((e = smem_attr(k_fwd_smooth<DIM, T, FINE>, FwdCfg<DIM, T, FINE>::BYTES)) ||
-            (e = smem_attr(k_restrict_res<DIM, T, FINE>, ResCfg<DIM, T, FINE>::BYTES)) ||
-            (e = smem_attr(k_up_even<DIM, T, FINE>, UpeCfg<DIM, T, FINE>::BYTES)) ||
-            (e = smem_attr(k_up_odd<DIM, T, FINE, false>, UpoCfg<DIM, T, FINE>::BYTES)) ||
-            (e = smem_attr(k_up_odd<DIM, T, FINE, true>, UpoCfg<DIM, T, FINE>::BYTES)))
+        if ((e = smem_attr(k_fwd_smooth<DIM, T, FINE, CS>, FwdCfg<DIM, T, FINE, CS>::BYTES)) ||
+            (e = smem_attr(k_restrict_res<DIM, T, FINE, CS>, ResCfg<DIM, T, FINE, CS>::BYTES)) ||
+            (e = smem_attr(k_up_even<DIM, T, FINE, CS>, UpeCfg<DIM, T, FINE, CS>::BYTES)) ||
+            (e = smem_attr(k_up_odd<DIM, T, FINE, false, CS>, UpoCfg<DIM, T, FINE, CS>::BYTES)) ||
+            (e = smem_attr(k_up_odd<DIM, T, FINE, true, CS>, UpoCfg<DIM, T, FINE, CS>::BYTES)))
             return e;
         return E_OK;
     }
@@ -397,7 +403,7 @@ private:
         }
         double hx = dx_, hy = dy_, hz = dz_;
         while (nx >= 2 && ny >= 2 && (DIM == 2 || nz >= 2)) {
-            LevelBuf<T> L;
+            LevelBuf<T, CS> L;
             L.g = make_geom_pitched(DIM, nx, ny, nz);
             L.hx = hx; L.hy = hy; L.hz = hz;
             lv_.push_back(L);
@@ -412,7 +418,7 @@ private:
         const int nl = (int)lv_.size();
         int e;
         for (int l = 0; l < nl; ++l) {
-            LevelBuf<T>& L = lv_[l];
+            LevelBuf<T, CS>& L = lv_[l];
             L.zc = DIM == 3 ? pick_zc(L.g) : 2;
             const size_t n = (size_t)L.g.n;
             if ((e = alloc(L.solid, n))) return e;
@@ -425,6 +431,12 @@ private:
                 if ((e = alloc(L.x, n))) return e;
                 if ((e = alloc(L.b, n))) return e;
                 if ((e = alloc(L.dg, n))) return e;
+                if constexpr (kHalf) {
+                    if ((e = alloc(L.hcx, n)) || (e = alloc(L.hcy, n))) return e;
+                    if (DIM == 3 && (e = alloc(L.hcz, n))) return e;
+                } else {
+                    L.hcx = L.cx; L.hcy = L.cy; L.hcz = L.cz;
+                }
             }
         }
         const Geom g0 = lv_[0].g;
@@ -454,17 +466,18 @@ private:
         // plane-box tensor maps
         constexpr int BW = PBox<T>::W, BH = PBox<T>::H;
         for (int l = 0; l < nl; ++l) {
-            LevelBuf<T>& L = lv_[l];
+            LevelBuf<T, CS>& L = lv_[l];
             const T* b = l == 0 ? r_ : L.b;
             const T* x = l == 0 ? z_ : L.x;
             bool ok = encode_level_map<T>(&L.mb, b, L.g, DIM, BW, BH, 1) &&
                       encode_level_map<T>(&L.mx, x, L.g, DIM, BW, BH, 1) &&
                       encode_level_map<uint8_t>(&L.mcode, L.code, L.g, DIM, PBox<uint8_t>::W,
                                                 PBox<uint8_t>::H, 1);
+            constexpr int CW = PBox<CS>::W;
             if (ok && l > 0)
-                ok = encode_level_map<T>(&L.mcx, L.cx, L.g, DIM, BW, BH, 1) &&
-                     encode_level_map<T>(&L.mcy, L.cy, L.g, DIM, BW, BH, 1) &&
-                     (DIM == 2 || encode_level_map<T>(&L.mcz, L.cz, L.g, DIM, BW, BH, 1)) &&
+                ok = encode_level_map<CS>(&L.mcx, L.hcx, L.g, DIM, CW, BH, 1) &&
+                     encode_level_map<CS>(&L.mcy, L.hcy, L.g, DIM, CW, BH, 1) &&
+                     (DIM == 2 || encode_level_map<CS>(&L.mcz, L.hcz, L.g, DIM, CW, BH, 1)) &&
                      encode_level_map<T>(&L.mdg, L.dg, L.g, DIM, BW, BH, 1) &&
                      encode_level_map<T>(&L.mxq, L.x, L.g, DIM, QBox<T>::W, QBox<T>::H, 1);
             if (!ok) return E_CUDA;
@@ -482,7 +495,7 @@ private:
                          cell_grid<DIM>(lv_[l].g.nx, lv_[l].g.ny, lv_[l].g.nz), blk, lv_[l - 1].g,
                          lv_[l - 1].solid, lv_[l].g, lv_[l].solid);
         {
-            const LevelBuf<T>& L = lv_[0];
+            const LevelBuf<T, CS>& L = lv_[0];
             const T idx2 = (T)(1.0 / (L.hx * L.hx)), idy2 = (T)(1.0 / (L.hy * L.hy));
             const T idz2 = DIM == 3 ? (T)(1.0 / (L.hz * L.hz)) : T(0);
             UAAMG_LAUNCH((KTag{K_SETUP, 0, 0.0}), (k_fine_coeffs<DIM, T>),
@@ -490,11 +503,26 @@ private:
                          L.wd, idx2, idy2, idz2);
         }
         for (int l = 1; l < nl; ++l) {
-            const LevelBuf<T>& F = lv_[l - 1];
-            LevelBuf<T>& Cl = lv_[l];
+            const LevelBuf<T, CS>& F = lv_[l - 1];
+            LevelBuf<T, CS>& Cl = lv_[l];
             UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_galerkin<DIM, T>),
                          cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, F.g, F.cx, F.cy, F.cz, F.wd,
                          Cl.g, Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd);
+        }
+        for (int l = 1; l < nl; ++l) {
+            LevelBuf<T, CS>& Cl = lv_[l];
+            if constexpr (kHalf) {  // FP16 face counts (after every level's Galerkin sums)
+                const Geom& g0 = lv_[0].g;
+                const float cs[3] = {(float)(1.0 / (lv_[0].hx * lv_[0].hx)),
+                                     (float)(1.0 / (lv_[0].hy * lv_[0].hy)),
+                                     (float)(1.0 / (lv_[0].hz * lv_[0].hz))};
+                (void)g0;
+                T* src[3] = {Cl.cx, Cl.cy, Cl.cz};
+                CS* dst[3] = {Cl.hcx, Cl.hcy, Cl.hcz};
+                for (int a = 0; a < DIM; ++a)
+                    UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_coupling_half, max_reduce_blocks(), 256,
+                                 (long long)Cl.g.n, src[a], dst[a], cs[a]);
+            }
             UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_diag<DIM, T>), vec_grid(Cl.g), dim3(32, 8), Cl.g,
                          Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd, Cl.dg);
         }
@@ -521,7 +549,7 @@ private:
         prof_on_ = false;
         int e = E_OK;
         for (int l = 0; l + 1 < (int)lv_.size() && e == E_OK; ++l) {
-            LevelBuf<T>& L = lv_[l];
+            LevelBuf<T, CS>& L = lv_[l];
             const auto key = std::make_tuple((int)sizeof(T), mixed_ ? 1 : 0, L.g.nx, L.g.ny, L.g.nz,
                                              l == 0 ? 1 : 0);
             {
@@ -560,7 +588,7 @@ private:
     }
 
     LevelView<T> view(int l, const T* r, T* z) const {
-        const LevelBuf<T>& L = lv_[l];
+        const LevelBuf<T, CS>& L = lv_[l];
         LevelView<T> v;
         v.g = L.g;
         v.solid = L.solid;
@@ -589,7 +617,7 @@ private:
             const LevelView<T> v = view(l, r, z);
             sweep<DIM>(v, 1, done, l);
             sweep<DIM>(v, 0, done, l);
-            const LevelBuf<T>& Cl = lv_[l + 1];
+            const LevelBuf<T, CS>& Cl = lv_[l + 1];
             UAAMG_LAUNCH((KTag{K_RESTRICT, l, cells(v.g) * ((2.0 + DIM) * sizeof(T) + 1.0) + cells(Cl.g) * sizeof(T)}),
                          (k_restrict<DIM, T>), cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, v, Cl.g,
                          Cl.solid, Cl.b, done);
@@ -598,7 +626,7 @@ private:
         coarsest<DIM>(r, z, done);
         for (int l = nl - 2; l >= 0; --l) {
             const LevelView<T> v = view(l, r, z);
-            const LevelBuf<T>& Cl = lv_[l + 1];
+            const LevelBuf<T, CS>& Cl = lv_[l + 1];
             UAAMG_LAUNCH((KTag{K_PROLONG, l, cells(v.g) * (2.0 * sizeof(T) + 1.0) + cells(Cl.g) * (sizeof(T) + 1.0)}),
                          (k_prolong<DIM, T>), cell_grid<DIM>(Cl.g.nx, Cl.g.ny, Cl.g.nz), blk, Cl.g,
                          Cl.solid, Cl.x, v.g, v.solid, v.x, done);
@@ -611,7 +639,7 @@ private:
     template <int DIM>
     void coarsest(const T* r, T* z, const int* done) {
         const int nl = (int)lv_.size();
-        const LevelBuf<T>& C = lv_[nl - 1];
+        const LevelBuf<T, CS>& C = lv_[nl - 1];
         T* cxp = nl == 1 ? z : C.x;
         cudaMemsetAsync(cxp, 0, (size_t)C.g.n * sizeof(T), st_);
         LevelView<T> v = view(nl - 1, r, z);
@@ -628,13 +656,17 @@ private:
     }
 
     MLevel<T> mlevel(int l) const {
-        const LevelBuf<T>& L = lv_[l];
+        const LevelBuf<T, CS>& L = lv_[l];
         MLevel<T> v;
         v.g = L.g;
         v.cg = l + 1 < (int)lv_.size() ? lv_[l + 1].g : L.g;
         v.idx2 = (T)(1.0 / (L.hx * L.hx));
         v.idy2 = (T)(1.0 / (L.hy * L.hy));
         v.idz2 = L.g.nz ? (T)(1.0 / (L.hz * L.hz)) : T(0);
+        // FP16 couplings are face counts times the finest level's 1/h^2 per axis
+        v.csx = kHalf ? (T)(1.0 / (lv_[0].hx * lv_[0].hx)) : T(1);
+        v.csy = kHalf ? (T)(1.0 / (lv_[0].hy * lv_[0].hy)) : T(1);
+        v.csz = kHalf ? (T)(1.0 / (lv_[0].hz * lv_[0].hz)) : T(1);
         v.dirichlet = dirichlet_;
         v.zc = L.zc;
         return v;
@@ -645,16 +677,16 @@ private:
     // next-coarser level's x as parent boxes.
     template <int DIM>
     MarchMaps maps(int l, bool hasx, bool parent) const {
-        const LevelBuf<T>& L = lv_[l];
+        const LevelBuf<T, CS>& L = lv_[l];
         MarchMaps m;
         int q = 0;
         m.v[q++] = L.mb;
         if (hasx) m.v[q++] = L.mx;
-        if (l > 0) {
+        if (l > 0) {  // slot order of MPlan: the T boxes, then the couplings
+            m.v[q++] = L.mdg;
             m.v[q++] = L.mcx;
             m.v[q++] = L.mcy;
             if (DIM == 3) m.v[q++] = L.mcz;
-            m.v[q++] = L.mdg;
         }
         m.code = L.mcode;
         if (parent) m.xc = lv_[l + 1].mxq;
@@ -663,38 +695,38 @@ private:
 
     template <int DIM, bool FINE>
     void down_level(int l, const int* done) {
-        const LevelBuf<T>& L = lv_[l];
-        const LevelBuf<T>& Cl = lv_[l + 1];
+        const LevelBuf<T, CS>& L = lv_[l];
+        const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
-        const double coef = FINE ? 0.0 : (DIM + 1.0) * t;
+        const double coef = FINE ? 0.0 : DIM * (double)sizeof(CS) + t;  // couplings + diagonal
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
-        UAAMG_LAUNCH_SMEM((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_smooth<DIM, T, FINE>),
-                          grid, blk, (FwdCfg<DIM, T, FINE>::BYTES), maps<DIM>(l, false, false),
+        UAAMG_LAUNCH_SMEM((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_smooth<DIM, T, FINE, CS>),
+                          grid, blk, (FwdCfg<DIM, T, FINE, CS>::BYTES), maps<DIM>(l, false, false),
                           mlevel(l), x, done, err_);
         UAAMG_LAUNCH_SMEM((KTag{K_RES, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
-                          (k_restrict_res<DIM, T, FINE>), grid, blk, (ResCfg<DIM, T, FINE>::BYTES),
+                          (k_restrict_res<DIM, T, FINE, CS>), grid, blk, (ResCfg<DIM, T, FINE, CS>::BYTES),
                           maps<DIM>(l, true, false), mlevel(l), Cl.code, Cl.b, done, err_);
     }
 
     template <int DIM, bool FINE>
     void up_level(int l, const int* done, bool zdot) {
-        const LevelBuf<T>& L = lv_[l];
-        const LevelBuf<T>& Cl = lv_[l + 1];
+        const LevelBuf<T, CS>& L = lv_[l];
+        const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
-        const double coef = FINE ? 0.0 : (DIM + 1.0) * t;
+        const double coef = FINE ? 0.0 : DIM * (double)sizeof(CS) + t;  // couplings + diagonal
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
         UAAMG_LAUNCH_SMEM((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
-                          (k_up_even<DIM, T, FINE>), grid, blk, (UpeCfg<DIM, T, FINE>::BYTES),
+                          (k_up_even<DIM, T, FINE, CS>), grid, blk, (UpeCfg<DIM, T, FINE, CS>::BYTES),
                           maps<DIM>(l, false, true), mlevel(l), x, done, err_);
         if (zdot)
             UAAMG_LAUNCH_SMEM((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
-                              (k_up_odd<DIM, T, FINE, true>), grid, blk, (UpoCfg<DIM, T, FINE>::BYTES),
+                              (k_up_odd<DIM, T, FINE, true, CS>), grid, blk, (UpoCfg<DIM, T, FINE, CS>::BYTES),
                               maps<DIM>(l, true, false), mlevel(l), x, done, err_, partials_, cg_);
         else
             UAAMG_LAUNCH_SMEM((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
-                              (k_up_odd<DIM, T, FINE, false>), grid, blk, (UpoCfg<DIM, T, FINE>::BYTES),
+                              (k_up_odd<DIM, T, FINE, false, CS>), grid, blk, (UpoCfg<DIM, T, FINE, CS>::BYTES),
                               maps<DIM>(l, true, false), mlevel(l), x, done, err_, partials_, cg_);
     }
 

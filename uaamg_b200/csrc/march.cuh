@@ -34,6 +34,10 @@
 // instantiation compiled with -fmad=false the V-cycle reproduces the reference
 // bit for bit.
 #pragma once
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
 #include "kernels.cuh"
 #include "tma.cuh"
 
@@ -66,21 +70,27 @@ struct QBox {
     static constexpr uint32_t BYTES = (uint32_t)(W * H * sizeof(E));
 };
 
-// One ring stage: value boxes of T in slot order b, [x], [cx, cy, (cz), dg], the
-// code box, optionally the parent box.
-template <int DIM, class T, bool HASX, bool COEF, bool XC>
+// One ring stage: value boxes of T in slot order b, [x], [dg], then (coarse levels)
+// the coupling boxes cx, cy, [cz] of the coupling storage type CS, the code box,
+// optionally the parent box.  Slot q's map is MarchMaps::v[q].
+template <int DIM, class T, bool HASX, bool COEF, bool XC, class CS = T>
 struct MPlan {
-    static constexpr int NCOEF = COEF ? (DIM == 3 ? 4 : 3) : 0;
-    static constexpr int QB = 0, QX = 1, QC0 = HASX ? 2 : 1;
-    static constexpr int QCX = QC0, QCY = QC0 + 1, QCZ = QC0 + 2, QDG = QC0 + (DIM == 3 ? 3 : 2);
-    static constexpr int NV = 1 + (HASX ? 1 : 0) + NCOEF;
+    static constexpr int NT = 1 + (HASX ? 1 : 0) + (COEF ? 1 : 0);  // boxes of T
+    static constexpr int NCS = COEF ? (DIM == 3 ? 3 : 2) : 0;       // boxes of CS
+    static constexpr int NV = NT + NCS;
+    static constexpr int QB = 0, QX = 1, QDG = NT - 1;
     static constexpr bool XCB = XC;
     static constexpr size_t VB = align128(PBox<T>::BYTES);
-    static constexpr size_t OFF_CODE = NV * VB;
+    static constexpr size_t CB = align128(PBox<CS>::BYTES);
+    static constexpr size_t OFF_CX = NT * VB, OFF_CY = OFF_CX + CB, OFF_CZ = OFF_CY + CB;
+    static constexpr size_t OFF_CODE = NT * VB + NCS * CB;
     static constexpr size_t OFF_XC = OFF_CODE + align128(PBox<uint8_t>::BYTES);
     static constexpr size_t STAGE = OFF_XC + (XC ? align128(QBox<T>::BYTES) : 0);
-    static constexpr uint32_t TX_BYTES =
-        NV * PBox<T>::BYTES + PBox<uint8_t>::BYTES + (XC ? QBox<T>::BYTES : 0);
+    static constexpr uint32_t TX_BYTES = NT * PBox<T>::BYTES + NCS * PBox<CS>::BYTES +
+                                         PBox<uint8_t>::BYTES + (XC ? QBox<T>::BYTES : 0);
+    __host__ __device__ static constexpr size_t box_off(int q) {
+        return q < NT ? (size_t)q * VB : NT * VB + (size_t)(q - NT) * CB;
+    }
 };
 
 // Shared memory of a march: 128 B of barriers, the diagonal table, S stages, then
@@ -104,9 +114,20 @@ struct MLevel {
     Geom g;          // this level
     Geom cg;         // next-coarser level (restriction target / prolongation source)
     T idx2, idy2, idz2;
+    T csx, csy, csz; // coarse levels: coupling = stored value * cs (1 when stored in T)
     int dirichlet;   // finest level: add the Dirichlet wall diagonal
     int zc;          // planes per block (even)
 };
+
+// A stored coupling as T: FP16 couplings hold the coupling / cs (a face count).
+template <class T, class CS>
+__device__ __forceinline__ T coupling(CS v, T cs) {
+    if constexpr (std::is_same<CS, T>::value) {
+        return v;
+    } else {
+        return (T)__half2float(v) * cs;
+    }
+}
 
 // The dynamic shared memory of a march, declared 128-byte aligned (every TMA box
 // sits at a multiple of 128 bytes from it).  Used directly -- never through an
@@ -173,30 +194,31 @@ __device__ __forceinline__ T mdiag(const MLevel<T>& L, const T* lut, const unsig
         if (L.dirichlet) d = d + wall_diag_at<DIM, T>(L, i, j, k);
         return d;
     } else {
-        return boxv<T>(st, P::QDG * P::VB, q);
+        return boxv<T>(st, P::box_off(P::QDG), q);
     }
 }
 
-// Couplings of the cell at box position q in the reference's order
+// Couplings of the cell at box column a, row r in the reference's order
 // +x, -x, +y, -y, +z, -z (stc: this plane's stage, stm: the plane below).
-template <int DIM, class T, class P, bool FINE>
+template <int DIM, class T, class P, bool FINE, class CS>
 __device__ __forceinline__ void mcoup(const MLevel<T>& L, const unsigned char* stc,
-                                      const unsigned char* stm, int q, T (&c)[6]) {
-    constexpr int W = PBox<T>::W;
+                                      const unsigned char* stm, int a, int r, T (&c)[6]) {
     if constexpr (FINE) {
         c[0] = c[1] = L.idx2;
         c[2] = c[3] = L.idy2;
         c[4] = c[5] = L.idz2;
     } else {
-        const T* cx = reinterpret_cast<const T*>(stc + P::QCX * P::VB);
-        const T* cy = reinterpret_cast<const T*>(stc + P::QCY * P::VB);
-        c[0] = cx[q];
-        c[1] = cx[q - 1];
-        c[2] = cy[q];
-        c[3] = cy[q - W];
+        constexpr int W = PBox<CS>::W;
+        const int q = r * W + a;
+        const CS* cx = reinterpret_cast<const CS*>(stc + P::OFF_CX);
+        const CS* cy = reinterpret_cast<const CS*>(stc + P::OFF_CY);
+        c[0] = coupling<T, CS>(cx[q], L.csx);
+        c[1] = coupling<T, CS>(cx[q - 1], L.csx);
+        c[2] = coupling<T, CS>(cy[q], L.csy);
+        c[3] = coupling<T, CS>(cy[q - W], L.csy);
         if constexpr (DIM == 3) {
-            c[4] = reinterpret_cast<const T*>(stc + P::QCZ * P::VB)[q];
-            c[5] = reinterpret_cast<const T*>(stm + P::QCZ * P::VB)[q];
+            c[4] = coupling<T, CS>(reinterpret_cast<const CS*>(stc + P::OFF_CZ)[q], L.csz);
+            c[5] = coupling<T, CS>(reinterpret_cast<const CS*>(stm + P::OFF_CZ)[q], L.csz);
         } else {
             c[4] = c[5] = T(0);
         }
@@ -241,7 +263,7 @@ __device__ __forceinline__ void issue_plane(const MarchMaps& M, unsigned char* s
     fence_proxy_async();
     mbar_expect_tx(bar, P::TX_BYTES);
 #pragma unroll
-    for (int q = 0; q < P::NV; ++q) tma_load<DIM>(st + q * P::VB, &M.v[q], x0, y0, k, bar);
+    for (int q = 0; q < P::NV; ++q) tma_load<DIM>(st + P::box_off(q), &M.v[q], x0, y0, k, bar);
     tma_load<DIM>(st + P::OFF_CODE, &M.code, x0, y0, k, bar);
     if constexpr (P::XCB) tma_load<DIM>(st + P::OFF_XC, &M.xc, x0 / 2, y0 / 2, (k + 1) >> 1, bar);
 }
@@ -312,26 +334,26 @@ __device__ __forceinline__ T fp32_ax(const MLevel<T>& L, uint32_t c, T d, const 
 }
 
 // Per-march ring depth and dynamic shared-memory size.
-template <int DIM, class T, bool FINE> struct FwdCfg {
-    using P = MPlan<DIM, T, false, !FINE, false>;
+template <int DIM, class T, bool FINE, class CS = T> struct FwdCfg {
+    using P = MPlan<DIM, T, false, !FINE, false, CS>;
     static constexpr int S = FINE ? 8 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
-template <int DIM, class T, bool FINE> struct ResCfg {
-    using P = MPlan<DIM, T, true, !FINE, false>;
+template <int DIM, class T, bool FINE, class CS = T> struct ResCfg {
+    using P = MPlan<DIM, T, true, !FINE, false, CS>;
     static constexpr int S = FINE && sizeof(T) == 4 ? 6 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA;
 };
-template <int DIM, class T, bool FINE> struct UpeCfg {
-    using P = MPlan<DIM, T, false, !FINE, true>;
+template <int DIM, class T, bool FINE, class CS = T> struct UpeCfg {
+    using P = MPlan<DIM, T, false, !FINE, true, CS>;
     static constexpr int S = FINE ? 8 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
-template <int DIM, class T, bool FINE> struct UpoCfg {
-    using P = MPlan<DIM, T, true, !FINE, false>;
+template <int DIM, class T, bool FINE, class CS = T> struct UpoCfg {
+    using P = MPlan<DIM, T, true, !FINE, false, CS>;
     static constexpr int S = FINE && sizeof(T) == 4 ? 6 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA;
@@ -411,12 +433,12 @@ __device__ __forceinline__ void stages_next(const MRing<DIM, S, P>& R, Stages& s
 // Step k builds plane k+1's odd values (the pair's odd cell and the ring's odd
 // cells) into a plane buffer and smooths plane k's even cells from plane k's
 // buffer and the odd values of their own column one plane up and down (registers).
-template <int DIM, class T, bool FINE>
+template <int DIM, class T, bool FINE, class CS>
 __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__ MarchMaps M,
                                                          MLevel<T> L, T* __restrict__ x,
                                                          const int* __restrict__ done, int* err) {
     if (done && *done) return;
-    using C = FwdCfg<DIM, T, FINE>;
+    using C = FwdCfg<DIM, T, FINE, CS>;
     using P = typename C::P;
     using Lay = typename C::Lay;
     constexpr int S = C::S, N = PBox<T>::N, W = PBox<T>::W, WC = PBox<uint8_t>::W;
@@ -486,7 +508,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__
                 const T d = mdiag<DIM, T, P, FINE>(L, lut, sg.c, c, q, o.i, o.j + e, k);
                 if (!(d < T(1e-30))) {
                     T cc[6];
-                    mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
+                    mcoup<DIM, T, P, FINE, CS>(L, sg.c, sg.m, o.a, o.rb + e, cc);
                     xe = (boxv<T>(sg.c, P::QB * P::VB, q) +
                           nbsum<DIM, T>(cc, Yc, q, e ? ypb : ypa, e ? ymb : yma)) / d;
                 }
@@ -510,14 +532,14 @@ __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__
 // b_c = sum over the 2x2(x2) children in the reference's (di, dj, dk) order.  A
 // thread's pair is the dj = 0, 1 children of one coarse column, the di = 1 children
 // are the next lane's pair, dk = 0, 1 are consecutive planes.
-template <int DIM, class T, bool FINE>
+template <int DIM, class T, bool FINE, class CS>
 __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant__ MarchMaps M,
                                                            MLevel<T> L,
                                                            const uint8_t* __restrict__ ccode,
                                                            T* __restrict__ cb,
                                                            const int* __restrict__ done, int* err) {
     if (done && *done) return;
-    using C = ResCfg<DIM, T, FINE>;
+    using C = ResCfg<DIM, T, FINE, CS>;
     using P = typename C::P;
     using Lay = typename C::Lay;
     constexpr int S = C::S, W = PBox<T>::W, WC = PBox<uint8_t>::W;
@@ -554,7 +576,7 @@ __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant
             if (c & kActive) {
                 const T d = mdiag<DIM, T, P, FINE>(L, lut, sg.c, c, q, o.i, o.j + e, k);
                 T cc[6];
-                mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
+                mcoup<DIM, T, P, FINE, CS>(L, sg.c, sg.m, o.a, o.rb + e, cc);
                 const T xp = DIM == 3 ? boxv<T>(sg.n, P::QX * P::VB, q) : T(0);
                 const T xm = DIM == 3 ? boxv<T>(sg.m, P::QX * P::VB, q) : T(0);
                 T ax;
@@ -607,12 +629,12 @@ __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant
 // their pre-smoothed value plus the prolongation, (b + 0)/d + 2 x_c; even cells are
 // smoothed from those: x = (b + sum c_n x_n)/d (a skipped even cell keeps
 // 0 + 2 x_c).  Writes x on every interior cell.
-template <int DIM, class T, bool FINE>
+template <int DIM, class T, bool FINE, class CS>
 __global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ MarchMaps M,
                                                       MLevel<T> L, T* __restrict__ x,
                                                       const int* __restrict__ done, int* err) {
     if (done && *done) return;
-    using C = UpeCfg<DIM, T, FINE>;
+    using C = UpeCfg<DIM, T, FINE, CS>;
     using P = typename C::P;
     using Lay = typename C::Lay;
     constexpr int S = C::S, N = PBox<T>::N, W = PBox<T>::W, WC = PBox<uint8_t>::W;
@@ -691,7 +713,7 @@ __global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ Ma
                     xe = T(0) + prolong_at<T, P>(sg.c, o.a, o.rb + e);
                 } else {
                     T cc[6];
-                    mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
+                    mcoup<DIM, T, P, FINE, CS>(L, sg.c, sg.m, o.a, o.rb + e, cc);
                     xe = (boxv<T>(sg.c, P::QB * P::VB, q) +
                           nbsum<DIM, T>(cc, Yc, q, e ? ypb : ypa, e ? ymb : yma)) / d;
                 }
@@ -714,13 +736,13 @@ __global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ Ma
 // Second (odd) colour of the reverse sweep, in place: odd cells read only even
 // neighbours, which this kernel does not write.  ZDOT (finest level): also the
 // fluid sums of z, r*z and r (r = this level's b) and the CG's projection / beta.
-template <int DIM, class T, bool FINE, bool ZDOT>
+template <int DIM, class T, bool FINE, bool ZDOT, class CS>
 __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ MarchMaps M,
                                                      MLevel<T> L, T* x,
                                                      const int* __restrict__ done, int* err,
                                                      double* partials, CGState* cg) {
     if (done && *done) return;
-    using C = UpoCfg<DIM, T, FINE>;
+    using C = UpoCfg<DIM, T, FINE, CS>;
     using P = typename C::P;
     using Lay = typename C::Lay;
     constexpr int S = C::S, W = PBox<T>::W, WC = PBox<uint8_t>::W;
@@ -756,7 +778,7 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
                 const T d = mdiag<DIM, T, P, FINE>(L, lut, sg.c, c, q, o.i, o.j + od, k);
                 if (!(d < T(1e-30))) {
                     T cc[6];
-                    mcoup<DIM, T, P, FINE>(L, sg.c, sg.m, q, cc);
+                    mcoup<DIM, T, P, FINE, CS>(L, sg.c, sg.m, o.a, o.rb + od, cc);
                     const T vp = DIM == 3 ? boxv<T>(sg.n, P::QX * P::VB, q) : T(0);
                     const T vm = DIM == 3 ? boxv<T>(sg.m, P::QX * P::VB, q) : T(0);
                     const T xv = (boxv<T>(sg.c, P::QB * P::VB, q) + nbsum<DIM, T>(cc, xb, q, vp, vm)) / d;

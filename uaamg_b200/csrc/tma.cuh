@@ -14,6 +14,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
+#include <cuda_fp16.h>
 
 #include <cstdint>
 
@@ -43,6 +44,7 @@ inline CUtensorMapDataType tma_dtype();
 template <> inline CUtensorMapDataType tma_dtype<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
 template <> inline CUtensorMapDataType tma_dtype<double>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT64; }
 template <> inline CUtensorMapDataType tma_dtype<uint8_t>() { return CU_TENSOR_MAP_DATA_TYPE_UINT8; }
+template <> inline CUtensorMapDataType tma_dtype<__half>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT16; }
 
 // Encodes a rank-2 (2D level) or rank-3 tensor map over a padded level array of
 // element type E with box (bx, by[, bz]).  Returns false when the driver refuses

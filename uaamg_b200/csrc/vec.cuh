@@ -157,5 +157,18 @@ __global__ void k_diag(Geom g, const uint8_t* __restrict__ s, const T* __restric
     });
 }
 
+// Couplings of a coarse level stored in FP16 as face counts: h = half(rint(c/cs))
+// with cs the finest level's 1/h^2 along the axis, exact up to 2048 faces; the T
+// coupling is replaced by its decoded value h * cs, so the diagonal (k_diag), the
+// step-by-step V-cycle and the marches all use the same values.
+__global__ void k_coupling_half(long long n, float* c, __half* h, float cs) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        const __half v = __float2half_rn(rintf(c[t] / cs));
+        h[t] = v;
+        c[t] = __half2float(v) * cs;
+    }
+}
+
 }  // namespace
 }  // namespace uaamg
