@@ -121,10 +121,13 @@ UAAMG_API uaamg_status uaamg_set_dirichlet_walls(uaamg_handle* h, int on);
 
 /* V-cycle kernels of this handle: 0 (default) = z marches, four per level (forward
  * sweep; residual + restriction; prolongation + even colour; odd colour), each
- * streaming the level's planes through TMA-filled shared memory;
+ * streaming the level's planes through TMA-filled shared memory, down to the first
+ * level of at most 1024 cells; that level, the smaller ones and the coarsest
+ * solve run as ONE single-block kernel with the levels in shared memory;
  * 1 = one kernel per colour sweep, restriction and prolongation, step by step as
- * UAAMGPreconditioner3D::vCycle (uaamg_preconditioner_3d.cpp:183-196).  Both give
- * identical results; 1 exists to cross-check 0. */
+ * UAAMGPreconditioner3D::vCycle (uaamg_preconditioner_3d.cpp:183-196);
+ * 2 = z marches on every level and a separate coarsest-level kernel.
+ * All give identical results in FP64; 1 and 2 exist to cross-check 0. */
 UAAMG_API uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps);
 
 /* Solve lap(p) = rhs with HOST FP64 arrays (padded): the Solver::solve /

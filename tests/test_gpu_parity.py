@@ -36,12 +36,13 @@ def rel_l2_meanfree(a, b, solid):
 # --- golden fixtures ---------------------------------------------------------
 
 
-@pytest.fixture(params=["march", "sweeps"])
+@pytest.fixture(params=["march", "sweeps", "march_all"])
 def vkernels(request, handle):
-    """Both V-cycle implementations: z-march level kernels and per-colour sweeps."""
-    handle.set_vcycle_kernels(request.param == "sweeps")
+    """Every V-cycle implementation: z marches with the small-level cluster kernel,
+    per-colour sweeps, and z marches on every level."""
+    handle.set_vcycle_kernels({"march": 0, "sweeps": 1, "march_all": 2}[request.param])
     yield request.param
-    handle.set_vcycle_kernels(False)
+    handle.set_vcycle_kernels(0)
 
 
 @pytest.mark.parametrize("name", golden_names("vcycle_"))

@@ -31,7 +31,8 @@ UNITS = [
     ("runtime.cpp", ["-x", "cu"]),
     ("noalloc.cu", ["-fmad=false"]),
 ]
-HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "vec.cuh", "tma.cuh", "engine.cuh", "engine.h", "handle.h"]
+HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "tail.cuh", "vec.cuh", "tma.cuh", "engine.cuh",
+           "engine.h", "handle.h"]
 
 
 def _nvcc() -> str:

@@ -91,7 +91,8 @@ uaamg_status engine_for(uaamg_handle* h, int p, uaamg::Engine** out) {
         if (!h->eng[p]) return fail(h, UAAMG_OOM, "engine allocation failed");
     }
     h->eng[p]->set_stream(h->stream);
-    h->eng[p]->set_vcycle_sweeps(h->sweeps != 0);
+    h->eng[p]->set_vcycle_sweeps(h->sweeps == 1);
+    h->eng[p]->set_small_levels(h->sweeps == 0);
     h->eng[p]->set_autotune(h->autotune != 0);
     if (!h->ready[p]) {
         int e = h->eng[p]->set_problem(h->dim, h->nx, h->ny, h->nz, h->dx, h->dy, h->dz,
@@ -235,7 +236,8 @@ uaamg_status uaamg_set_stream(uaamg_handle* h, void* stream) {
 
 uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps) {
     if (!h) return UAAMG_INVALID_ARG;
-    h->sweeps = sweeps ? 1 : 0;
+    if (sweeps < 0 || sweeps > 2) return fail(h, UAAMG_INVALID_ARG, "V-cycle kernels: 0, 1 or 2");
+    h->sweeps = sweeps;
     return UAAMG_OK;
 }
 

@@ -23,6 +23,7 @@
 
 #include "engine.h"
 #include "kernels.cuh"
+#include "tail.cuh"
 #include "tma.cuh"
 #include "vec.cuh"
 
@@ -47,13 +48,14 @@ struct LevelBuf {
 // Kernel classes for the in-situ per-kernel timing (uaamg_profile_solve).
 enum KClass : int {
     K_SWEEP = 0, K_RESTRICT, K_PROLONG, K_COARSEST, K_PMATVEC, K_UPDATE, K_ZDOT, K_FWD, K_RES,
-    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_FOLD, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_SCALAR, K_NCLASS
+    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_FOLD, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_SCALAR, K_TAIL,
+    K_NCLASS
 };
 static const char* const kclass_names[K_NCLASS] = {
     "rbgs_sweep", "restrict_residual", "prolong_add", "coarsest_solve", "p_matvec_dot",
     "cg_update", "z_dot", "smooth_fwd", "residual_restrict", "prolong_smooth_even",
     "smooth_odd", "true_residual", "fold", "rhs_prepare", "output", "cast", "hierarchy_setup",
-    "scalar"};
+    "scalar", "small_levels"};
 
 struct KTag {
     int cls;
@@ -205,6 +207,7 @@ public:
     void set_vcycle_sweeps(bool on) override { sweeps_ = on; }
     void set_graphs(bool on) override { graphs_ = on; }
     void set_autotune(bool on) override { autotune_ = on; }
+    void set_small_levels(bool on) override { tail_on_ = on; }
 
     void set_profiling(bool on) override {
         prof_on_ = on;
@@ -274,6 +277,10 @@ private:
     bool sweeps_ = false;  // V-cycle as per-colour sweeps (cross-check) instead of the marches
     bool graphs_ = true;   // replay the PCG step as a CUDA graph
     bool autotune_ = false;  // time the marches' z-chunk lengths at set-up
+    bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
+    int tail_lt_ = 0;        // first level of the small-level kernel
+    int tail_nc_ = 0;        // 1: the hierarchy has a tail (0: it does not fit the kernel)
+    size_t tail_smem_ = 0;   // its dynamic shared memory (x and b of every tail level)
     cudaStream_t cap_ = nullptr;      // capture stream
     cudaGraphExec_t gexec_ = nullptr; // two PCG iterations
     long long gkey_ = -1;
@@ -530,8 +537,76 @@ private:
             UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_codes<DIM>, vec_grid(lv_[l].g), dim3(32, 8),
                          lv_[l].g, lv_[l].solid, lv_[l].code, l == 0 ? 1 : 0);
         if ((e = sync_check()) != E_OK) return e;
+        if ((e = tail_setup<DIM>()) != E_OK) return e;
         if (DIM == 3 && autotune_) return tune<DIM>();
         return E_OK;
+    }
+
+    bool use_tail() const { return tail_on_ && !sweeps_ && tail_nc_ > 0; }
+
+    // The small levels' one-block kernel (tail.cuh): from the first level (>= 1) of at
+    // most kTailCells cells down to the coarsest, while their x and b fit its shared
+    // memory and the coarsest has at most two cells a thread.
+    static size_t tail_cells_padded(const Geom& g) {
+        return (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz ? g.nz + 2 : 1);
+    }
+
+    template <int DIM>
+    int tail_setup() {
+        const int nl = (int)lv_.size();
+        tail_nc_ = 0;
+        tail_lt_ = nl;
+        if (nl < 2) return E_OK;
+        const Geom& gc = lv_[nl - 1].g;
+        size_t elems = 2 * tail_cells_padded(gc);
+        if (cells(gc) > 2.0 * tail_threads<T>() || elems * sizeof(T) > kTailSmemBytes) return E_OK;
+        int lt = nl - 1;
+        while (lt > 1 && cells(lv_[lt - 1].g) <= (double)kTailCells && nl - (lt - 1) <= kTailMaxLevels &&
+               (elems + 2 * tail_cells_padded(lv_[lt - 1].g)) * sizeof(T) <= kTailSmemBytes) {
+            --lt;
+            elems += 2 * tail_cells_padded(lv_[lt].g);
+        }
+        // the attribute belongs to the kernel, not to this engine: always the cap
+        if (cudaFuncSetAttribute(k_tail<DIM, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kTailSmemBytes) != cudaSuccess)
+            return E_CUDA;
+        tail_lt_ = lt;
+        tail_nc_ = 1;
+        tail_smem_ = elems * sizeof(T);
+        return E_OK;
+    }
+
+    // Levels tail_lt_ .. nl-1 of the V-cycle (b of tail_lt_ in, its x out).
+    template <int DIM>
+    void tail_launch(const int* done) {
+        const int nl = (int)lv_.size();
+        TailArgs<T> a{};
+        a.nlev = nl - tail_lt_;
+        int off = 0;
+        double bytes = 0.0;
+        for (int q = 0; q < a.nlev; ++q) {
+            const LevelBuf<T, CS>& L = lv_[tail_lt_ + q];
+            TailLevel<T>& t = a.lv[q];
+            t.g = L.g;
+            t.csx = L.g.nx + 2;
+            t.csxy = (L.g.nx + 2) * (L.g.ny + 2);
+            t.xs = off;
+            t.bs = off + (int)tail_cells_padded(L.g);
+            off += 2 * (int)tail_cells_padded(L.g);
+            t.code = L.code;
+            t.cx = L.cx;
+            t.cy = L.cy;
+            t.cz = DIM == 3 ? L.cz : nullptr;
+            t.dg = L.dg;
+            t.x = L.x;
+            t.b = L.b;
+            // codes, couplings and diagonal read once per pass, four passes
+            bytes += 4.0 * cells(L.g) * ((1.0 + DIM) * sizeof(T) + 1.0);
+        }
+        a.smem_elems = off;
+        bytes += 2.0 * cells(lv_[tail_lt_].g) * sizeof(T);  // the first level's b in, x out
+        UAAMG_LAUNCH_SMEM((KTag{K_TAIL, tail_lt_, bytes}), (k_tail<DIM, T>), 1, tail_threads<T>(),
+                          tail_smem_, a, done);
     }
 
     // Autotuner: for every level with marches, time its four V-cycle marches
@@ -549,6 +624,7 @@ private:
         prof_on_ = false;
         int e = E_OK;
         for (int l = 0; l + 1 < (int)lv_.size() && e == E_OK; ++l) {
+            if (use_tail() && l >= tail_lt_) break;  // the cluster kernel runs those levels
             LevelBuf<T, CS>& L = lv_[l];
             const auto key = std::make_tuple((int)sizeof(T), mixed_ ? 1 : 0, L.g.nx, L.g.ny, L.g.nz,
                                              l == 0 ? 1 : 0);
@@ -735,17 +811,19 @@ private:
     template <int DIM>
     void vcycle_march(const int* done, bool zdot) {
         const int nl = (int)lv_.size();
-        for (int l = 0; l + 1 < nl; ++l) {
+        const int lt = use_tail() ? tail_lt_ : nl - 1;  // first level below the marches
+        for (int l = 0; l < lt; ++l) {
             if (l == 0) down_level<DIM, true>(l, done);
             else down_level<DIM, false>(l, done);
         }
-        coarsest<DIM>(r_, z_, done);
+        if (use_tail()) tail_launch<DIM>(done);
+        else coarsest<DIM>(r_, z_, done);
         if (nl == 1 && zdot) {
             const Geom& g = lv_[0].g;
             UAAMG_LAUNCH((KTag{K_ZDOT, 0, cells(g) * (2.0 * sizeof(T) + 1.0)}), (k_zdot<DIM, T>),
                          vec_grid(g), dim3(32, 8), g, lv_[0].solid, r_, z_, partials_, cg_);
         }
-        for (int l = nl - 2; l >= 0; --l) {
+        for (int l = lt - 1; l >= 0; --l) {
             if (l == 0) up_level<DIM, true>(l, done, zdot);
             else up_level<DIM, false>(l, done, false);
         }
@@ -877,7 +955,7 @@ private:
         // and options.
         use_graph_ = graphs_ && !prof_on_;
         if (use_graph_) {
-            const long long key = ((long long)a.precond << 1) | (sweeps_ ? 1 : 0);
+            const long long key = ((long long)a.precond << 2) | (use_tail() ? 2 : 0) | (sweeps_ ? 1 : 0);
             if (!gexec_ || key != gkey_ || a.hist != ghist_) {
                 if (gexec_) { cudaGraphExecDestroy(gexec_); gexec_ = nullptr; }
                 if (!cap_ && cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking) != cudaSuccess)

@@ -82,6 +82,9 @@ public:
     virtual long launches() const = 0;
     // V-cycle as per-colour sweep kernels (the cross-check) instead of the fused kernels.
     virtual void set_vcycle_sweeps(bool on) = 0;
+    // Marches: run the small levels and the coarsest solve as one single-block
+    // kernel (default on; off: marches on every level).
+    virtual void set_small_levels(bool on) = 0;
     // Replay each pair of PCG iterations as one CUDA graph (default on).
     virtual void set_graphs(bool on) = 0;
     // 1: the next set_problem times each level's marches for a few z-chunk lengths

@@ -114,9 +114,10 @@ class Handle:
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.uaamg_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
 
-    def set_vcycle_kernels(self, sweeps: bool):
-        """False: z-march V-cycle kernels (default); True: per-colour sweep kernels."""
-        self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(bool(sweeps))), "vcycle")
+    def set_vcycle_kernels(self, mode):
+        """0 / False: z marches + the small-level cluster kernel (default);
+        1 / True: per-colour sweep kernels; 2: z marches on every level."""
+        self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(mode)), "vcycle")
 
     def set_dirichlet_walls(self, on: bool):
         self._check(self.lib.uaamg_set_dirichlet_walls(self.h, int(bool(on))), "dirichlet")
