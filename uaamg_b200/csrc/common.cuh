@@ -13,6 +13,11 @@
 
 namespace uaamg {
 
+// Cell code bits (one byte a cell, vec.cuh k_codes): interior fluid cell, colour
+// (i + j + k odd); on the finest level bits 0-5 mark the +x,-x,+y,-y,+z,-z
+// neighbours that are interior fluid cells.
+constexpr uint32_t kActive = 64u, kOdd = 128u;
+
 struct Geom {
     int nx, ny, nz;  // interior cells; nz == 0 for a 2D level
     int sx, sxy;     // strides in cells: sx = nx+2, sxy = (nx+2)(ny+2)
@@ -76,7 +81,7 @@ struct CGState {
     int replacements;  // replacements performed
     int dirichlet;     // 1: no null space (skip mean projections)
     int init;          // 1 while forming p0 = z0 (beta = 0)
-    int pad_;
+    int fold;          // mixed mode: the next x update first folds x_lo into x_hi
     unsigned int counter[8];  // last-block counters, one per reduction site
 };
 

@@ -14,6 +14,7 @@
 // make_geom_pitched); the caller's arrays use the reference layout and are
 // converted on the way in (rhs, warm-start p, preconditioner input) and out.
 #pragma once
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -48,14 +49,13 @@ struct LevelBuf {
 // Kernel classes for the in-situ per-kernel timing (uaamg_profile_solve).
 enum KClass : int {
     K_SWEEP = 0, K_RESTRICT, K_PROLONG, K_COARSEST, K_PMATVEC, K_UPDATE, K_ZDOT, K_FWD, K_RES,
-    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_FOLD, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_SCALAR, K_TAIL,
-    K_NCLASS
+    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_SCALAR, K_TAIL, K_NCLASS
 };
 static const char* const kclass_names[K_NCLASS] = {
     "rbgs_sweep", "restrict_residual", "prolong_add", "coarsest_solve", "p_matvec_dot",
     "cg_update", "z_dot", "smooth_fwd", "residual_restrict", "prolong_smooth_even",
-    "smooth_odd", "true_residual", "fold", "rhs_prepare", "output", "cast", "hierarchy_setup",
-    "scalar", "small_levels"};
+    "smooth_odd", "true_residual", "rhs_prepare", "output", "cast", "hierarchy_setup", "scalar",
+    "small_levels"};
 
 struct KTag {
     int cls;
@@ -294,6 +294,14 @@ private:
 
     int max_reduce_blocks() const { return 4 * num_sms_; }
 
+    // grid of the FP64 residual column walk (kernels.cuh k_resid_x64): 32 x 8 columns
+    // of kResidZc planes a block
+    static constexpr int kResidZc = 16;
+    static dim3 resid_grid(const Geom& g) {
+        return dim3((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 7) / 8),
+                    (unsigned)(g.nz ? (g.nz + kResidZc - 1) / kResidZc : 1));
+    }
+
     // grid of the row-walk kernels (kernels.cuh for_cells): capped at 4 blocks per SM
     dim3 vec_grid(const Geom& g) const {
         const long long items = (long long)g.ny * (g.nz ? g.nz : 1) * ((g.nx + 31) / 32);
@@ -457,6 +465,8 @@ private:
         {
             const dim3 mg = march_grid<DIM>(g0, 2);  // the most blocks any chunk length gives
             reduce_blocks_ = (long long)mg.x * mg.y * mg.z;
+            const dim3 rg = resid_grid(g0);
+            reduce_blocks_ = std::max(reduce_blocks_, (long long)rg.x * rg.y * rg.z);
             if (reduce_blocks_ < max_reduce_blocks()) reduce_blocks_ = max_reduce_blocks();
         }
         if ((e = alloc(partials_, (size_t)reduce_blocks_ * 4))) return e;
@@ -897,14 +907,15 @@ private:
                           (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st, partials_, cg_,
                           err_);
         const long long nvec = (long long)g.n / Vec16<T>::N;
+        // x_lo, r, p, Ap in; x_lo, r out (a fold after a replacement adds x_hi in and out)
         UAAMG_LAUNCH((KTag{K_UPDATE, 0, cells(g) * (6.0 * sizeof(T))}), k_update_flat<T>,
-                     max_reduce_blocks(), 256, nvec, xlo_, r_, pnew, ap_, partials_, cg_, cur_.hist);
+                     max_reduce_blocks(), 256, nvec, xlo_, r_, pnew, ap_, mixed_ ? xd_ : nullptr,
+                     partials_, cg_, cur_.hist);
         if (mixed_) {
-            UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T))}), k_fold_flat<T>,
-                         max_reduce_blocks(), 256, (long long)g.n, xd_, xlo_, cg_, 0);
-            UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (17.0 + sizeof(T))}),
-                         (k_true_residual<DIM, T>), vec_grid(g), dim3(32, 8), g, lv_[0].solid, b64_,
-                         xd_, r_, st, partials_, cg_, 5, 1, cur_.tol, cur_.tol_mode);
+            // residual replacement (when due): b, x_hi, x_lo, codes in; r out
+            UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (17.0 + 2.0 * sizeof(T))}),
+                         (k_resid_x64<DIM, T>), resid_grid(g), dim3(32, 8), g, lv_[0].code, b64_, xd_,
+                         xlo_, r_, st, kResidZc, partials_, cg_, 5, 1, cur_.tol, cur_.tol_mode);
             UAAMG_LAUNCH((KTag{K_SCALAR, 0, 0.0}), k_maxiter_check, 1, 1, cg_);
         }
         cg_precond<DIM>();
@@ -1015,22 +1026,17 @@ private:
         const Geom g = lv_[0].g;
         const dim3 vb(32, 8);
         const dim3 vg = vec_grid(g);
-        const int n = g.n;
         const Stencil st = stencil();
         const SolveArgs& a = cur_;
-        if (mixed_) {
-            UAAMG_LAUNCH((KTag{K_FOLD, 0, cells(g) * (16.0 + 2.0 * sizeof(T))}), k_fold_flat<T>,
-                         max_reduce_blocks(), 256, (long long)n, xd_, xlo_, cg_, 1);
-        } else if (sizeof(T) == sizeof(double)) {
-            cudaMemcpyAsync(xd_, xlo_, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st_);
-        } else {
-            UAAMG_LAUNCH((KTag{K_CAST, 0, 12.0 * n}), k_cast_to_f64<T>, (n + 255) / 256, 256, xlo_, xd_, n);
-        }
+        // the solution: x_hi + x_lo in mixed mode, else the working x alone
+        const double* xhi = mixed_ ? xd_ : nullptr;
+        const double xb = (mixed_ ? 8.0 : 0.0) + sizeof(T);
         // exit diagnostics: FP64 true residual of the accumulated solution
-        UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * 17.0}), (k_true_residual<DIM, T>), vg, vb, g,
-                     lv_[0].solid, b64_, xd_, (T*)nullptr, st, partials_, cg_, 5, 2, a.tol, a.tol_mode);
-        UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 24.0}), (k_export<DIM, double>), vg, vb, g, gref_, xd_,
-                     a.x, 1);
+        UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (9.0 + xb)}), (k_resid_x64<DIM, T>),
+                     resid_grid(g), dim3(32, 8), g, lv_[0].code, b64_, xhi, xlo_, (T*)nullptr, st,
+                     kResidZc, partials_, cg_, 5, 2, a.tol, a.tol_mode);
+        UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * (16.0 + xb)}), (k_export_x<DIM, T>), vg, vb, g, gref_,
+                     xhi, xlo_, a.x, 1);
         if (a.project_mean && a.ref_solid) {
             const dim3 rg = vec_grid(gref_);
             UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * 9.0}), k_sum_count<DIM>, rg, vb, gref_, a.ref_solid,

@@ -388,22 +388,51 @@ __global__ void k_sub_mean(Geom g, const uint8_t* __restrict__ s, double* v, con
     });
 }
 
+// The last block's bookkeeping of a true residual r.r (rr): mode 0 the initial
+// residual (r0, the absolute tolerance); mode 1 a residual replacement; 2 and 3
+// record it only.
+__device__ __forceinline__ void true_residual_done(CGState* cg, double rr, int mode, double tol,
+                                                   int tol_mode) {
+    cg->rr_true = rr;
+    if (mode == 0) {
+        cg->r0 = sqrt(rr);
+        cg->rr = rr;
+        cg->tol_abs = tol_mode ? tol * cg->bnorm : tol;
+        if (rr == 0.0) { cg->status = CG_CONVERGED; cg->done = 1; }  // b = 0: x = 0 exactly
+    } else if (mode == 1) {
+        // a true residual more than twice the recursive one means the FP32
+        // recurrence drifted: the next search direction restarts (beta = 0),
+        // since beta = r.z / r.z_old would mix the replaced residual with
+        // directions built for the drifted one
+        if (rr > 4.0 * cg->rr) cg->init = 1;
+        cg->rr = rr;
+        cg->replacements += 1;
+        if (cg->cand) {
+            cg->cand = 0;
+            if (sqrt(rr) < cg->tol_abs) { cg->status = CG_CONVERGED; cg->done = 1; }
+        }
+        if (!(rr == rr)) { cg->status = CG_NAN; cg->done = 1; }
+    }
+}
+
+// Mixed-mode residual replacement due now: every replace_every iterations, or when
+// the recursive residual met the tolerance (a candidate to confirm).
+__device__ __forceinline__ bool replacement_due(const CGState* cg) {
+    return !cg->done && (cg->cand || (cg->replace_every > 0 && cg->iter > 0 &&
+                                      cg->iter % cg->replace_every == 0));
+}
+
 // r = b - A x (FP64), copied into the working residual rw (type T), with
 // ||r||^2 reduced.  mode 0: initial residual (sets r0, and tol_abs = tol or
 // tol*||b|| for the relative rule, ||b|| being the RHS norm, not ||r0||);
-// mode 1: residual replacement (mixed); mode 2: exit diagnostics only;
-// mode 3: plain b <- b - A x for a warm start (rw may alias b: each cell reads
+// mode 1: residual replacement; mode 2: exit diagnostics only (the solve loop and
+// its exit use k_resid_x64 for both); mode 3: plain b <- b - A x for a warm start (rw may alias b: each cell reads
 // its own b before writing it).  When x == nullptr the residual is b itself.
 template <int DIM, class T>
 __global__ void k_true_residual(Geom g, const uint8_t* __restrict__ s, const double* b,
                                 const double* __restrict__ x, T* rw, Stencil st, double* partials,
                                 CGState* cg, int slot, int mode, double tol, int tol_mode) {
-    if (mode == 1) {
-        if (cg->done) return;
-        if (!(cg->cand || (cg->replace_every > 0 && cg->iter > 0 &&
-                           cg->iter % cg->replace_every == 0)))
-            return;
-    }
+    if (mode == 1 && !replacement_due(cg)) return;
     double acc[1] = {0.0};
     for_cells<DIM>(g, [&](int i, int j, int k, int id) {
         if (!s[id]) {
@@ -417,28 +446,69 @@ __global__ void k_true_residual(Geom g, const uint8_t* __restrict__ s, const dou
         }
     });
     double tot[1];
-    if (reduce_last<1>(acc, partials, &cg->counter[slot], tot)) {
-        const double rr = tot[0];
-        cg->rr_true = rr;
-        if (mode == 0) {
-            cg->r0 = sqrt(rr);
-            cg->rr = rr;
-            cg->tol_abs = tol_mode ? tol * cg->bnorm : tol;
-            if (rr == 0.0) { cg->status = CG_CONVERGED; cg->done = 1; }  // b = 0: x = 0 exactly
-        } else if (mode == 1) {
-            // a true residual more than twice the recursive one means the FP32
-            // recurrence drifted: the next search direction restarts (beta = 0),
-            // since beta = r.z / r.z_old would mix the replaced residual with
-            // directions built for the drifted one
-            if (rr > 4.0 * cg->rr) cg->init = 1;
-            cg->rr = rr;
-            cg->replacements += 1;
-            if (cg->cand) {
-                cg->cand = 0;
-                if (sqrt(rr) < cg->tol_abs) { cg->status = CG_CONVERGED; cg->done = 1; }
+    if (reduce_last<1>(acc, partials, &cg->counter[slot], tot))
+        true_residual_done(cg, tot[0], mode, tol, tol_mode);
+}
+
+// FP64 true residual r = b - A x of the finest level with x = x_hi + x_lo (either
+// part may be absent), the reference's operator (pcg_3d.cpp:38-55: a neighbour that
+// is not an interior fluid cell reads x_C, or -x_C across a Dirichlet wall),
+// neighbours from the cell codes.  A thread walks one (i, j) column through zc
+// planes, keeping x of the planes below, at and above in registers; every load of
+// a step is independent of the others.  Writes r as T to rw (0 on solid cells) when
+// given, reduces r.r; mode 1 (residual replacement, gated as replacement_due) also
+// asks the next x update to fold x_lo into x_hi; mode 2: exit diagnostics.
+template <int DIM, class T>
+__global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __restrict__ code,
+                                                   const double* __restrict__ b,
+                                                   const double* __restrict__ xhi,
+                                                   const T* __restrict__ xlo, T* __restrict__ rw,
+                                                   Stencil st, int zc, double* partials, CGState* cg,
+                                                   int slot, int mode, double tol, int tol_mode) {
+    if (mode == 1 && !replacement_due(cg)) return;
+    const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    double acc[1] = {0.0};
+    if (i <= g.nx && j <= g.ny) {
+        const int kb = DIM == 3 ? 1 + (int)blockIdx.z * zc : 0;
+        const int ke = DIM == 3 ? min(kb + zc, g.nz + 1) : 1;
+        auto X = [&](int q) -> double {
+            if (xhi && xlo) return xhi[q] + (double)xlo[q];
+            return xhi ? xhi[q] : (double)xlo[q];
+        };
+        const double idx2 = st.idx2, idy2 = st.idy2, idz2 = st.idz2, diag = st.diag;
+        const int sx = g.sx, sxy = g.sxy;
+        int id = cidx(g, i, j, kb);
+        double xm = DIM == 3 ? X(id - sxy) : 0.0, xc = X(id);
+        for (int k = kb; k < ke; ++k, id += sxy) {
+            const double xp = DIM == 3 ? X(id + sxy) : 0.0;
+            const uint32_t c = code[id];
+            const double bb = b[id];
+            const double xl = X(id - 1), xr = X(id + 1), xb = X(id - sx), xt = X(id + sx);
+            const double wall = st.dirichlet ? -xc : xc;
+            const double vL = (c & 2u) ? xl : (i > 1 ? xc : wall);
+            const double vR = (c & 1u) ? xr : (i < g.nx ? xc : wall);
+            const double vB = (c & 8u) ? xb : (j > 1 ? xc : wall);
+            const double vT = (c & 4u) ? xt : (j < g.ny ? xc : wall);
+            double ax;
+            if (DIM == 3) {
+                const double vF = (c & 32u) ? xm : (k > 1 ? xc : wall);
+                const double vK = (c & 16u) ? xp : (k < g.nz ? xc : wall);
+                ax = diag * xc - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
+            } else {
+                ax = diag * xc - (vL + vR) * idx2 - (vB + vT) * idy2;
             }
-            if (!(rr == rr)) { cg->status = CG_NAN; cg->done = 1; }
+            const double r = (c & kActive) ? bb - ax : 0.0;
+            acc[0] += r * r;
+            if (rw) rw[id] = (T)r;
+            xm = xc;
+            xc = xp;
         }
+    }
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[slot], tot)) {
+        if (mode == 1) cg->fold = 1;
+        true_residual_done(cg, tot[0], mode, tol, tol_mode);
     }
 }
 
@@ -493,18 +563,6 @@ __global__ void k_zdot(Geom g, const uint8_t* __restrict__ s, const T* __restric
     });
     double tot[3];
     if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
-}
-
-// FP64 <-> T conversions on the padded arrays.
-template <class T>
-__global__ void k_cast_from_f64(const double* __restrict__ a, T* b, int n) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) b[t] = (T)a[t];
-}
-template <class T>
-__global__ void k_cast_to_f64(const T* __restrict__ a, double* b, int n) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) b[t] = (double)a[t];
 }
 
 }  // namespace

@@ -44,7 +44,6 @@
 namespace uaamg {
 namespace {
 
-constexpr uint32_t kActive = 64u, kOdd = 128u;
 constexpr int kMX = 32, kMY = 16;                  // column tile
 constexpr int kThreads = 256;                      // one thread per x-pair of the tile
 constexpr int kHaloOdd = 2 * (kMX / 2 + 1) + kMY;  // odd cells of the 1-cell ring: 50

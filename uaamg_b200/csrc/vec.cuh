@@ -38,14 +38,39 @@ __device__ __forceinline__ void vaxpy_rr<double>(double2& x, double2& r, const d
     rr += r.y * r.y;
 }
 
+// Mixed mode: x_hi += x_lo, x_lo = 0 on one vector of x_lo (its N cells).
+template <class T>
+__device__ __forceinline__ void vfold(typename Vec16<T>::V& x, double* xhi, long long t);
+template <>
+__device__ __forceinline__ void vfold<float>(float4& x, double* xhi, long long t) {
+    double2* h = reinterpret_cast<double2*>(xhi) + 2 * t;
+    double2 a = h[0], b = h[1];
+    a.x += (double)x.x; a.y += (double)x.y; b.x += (double)x.z; b.y += (double)x.w;
+    h[0] = a;
+    h[1] = b;
+    x = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+template <>
+__device__ __forceinline__ void vfold<double>(double2& x, double* xhi, long long t) {
+    double2* h = reinterpret_cast<double2*>(xhi) + t;
+    double2 a = *h;
+    a.x += x.x; a.y += x.y;
+    *h = a;
+    x = make_double2(0.0, 0.0);
+}
+
+// In mixed mode (xhi given) a residual replacement in the previous iteration left
+// cg->fold set: x_lo is first folded into the FP64 x_hi (the value x_hi + x_lo the
+// replacement's residual was computed from) and restarts at 0.
 template <class T>
 __global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
                                                      const T* __restrict__ p,
-                                                     const T* __restrict__ ap, double* partials,
-                                                     CGState* cg, double* hist) {
+                                                     const T* __restrict__ ap, double* xhi,
+                                                     double* partials, CGState* cg, double* hist) {
     if (cg->done) return;
     using V = typename Vec16<T>::V;
     const T alpha = (T)cg->alpha;
+    const bool fold = xhi && cg->fold;
     V* xv = reinterpret_cast<V*>(x);
     V* rv = reinterpret_cast<V*>(r);
     const V* pv = reinterpret_cast<const V*>(p);
@@ -55,12 +80,14 @@ __global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nvec; t += stride) {
         V xx = xv[t], rr_ = rv[t];
         const V pp = __ldg(&pv[t]), aa = __ldg(&av[t]);
+        if (fold) vfold<T>(xx, xhi, t);
         vaxpy_rr<T>(xx, rr_, pp, aa, alpha, acc[0]);
         xv[t] = xx;
         rv[t] = rr_;
     }
     double tot[1];
     if (reduce_last<1>(acc, partials, &cg->counter[1], tot)) {
+        if (fold) cg->fold = 0;  // every other block has finished its loop
         const double rr = tot[0];
         cg->rr = rr;
         cg->iter += 1;
@@ -78,25 +105,6 @@ __global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
     }
 }
 
-// Mixed mode fold over the whole padded array (x_lo is 0 outside fluid cells).
-template <class T>
-__global__ void k_fold_flat(long long n, double* xhi, T* xlo, const CGState* cg, int force) {
-    if (!force) {
-        if (cg->done) return;
-        if (!(cg->cand || (cg->replace_every > 0 && cg->iter > 0 &&
-                           cg->iter % cg->replace_every == 0)))
-            return;
-    }
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
-        const T v = xlo[t];
-        if (v != T(0)) {
-            xhi[t] += (double)v;
-            xlo[t] = T(0);
-        }
-    }
-}
-
 // Layout conversions between the reference's layout (gr) and the pitched one (g).
 template <int DIM, class T>
 __global__ void k_import(Geom g, Geom gr, const double* __restrict__ src, T* dst) {
@@ -106,6 +114,17 @@ template <int DIM>
 __global__ void k_import_mask(Geom g, Geom gr, const uint8_t* __restrict__ src, uint8_t* dst) {
     for_cells<DIM>(g, [&](int i, int j, int k, int id) {
         dst[id] = src[cidx(gr, i, j, k)] ? 1 : 0;
+    });
+}
+// The solution x = x_hi + x_lo (either part may be absent) into the reference
+// layout: dst = x (overwrite) or dst += x (accumulate), interior cells.
+template <int DIM, class T>
+__global__ void k_export_x(Geom g, Geom gr, const double* __restrict__ xhi, const T* __restrict__ xlo,
+                           double* dst, int accumulate) {
+    for_cells<DIM>(g, [&](int i, int j, int k, int id) {
+        const double x = xhi && xlo ? xhi[id] + (double)xlo[id] : (xhi ? xhi[id] : (double)xlo[id]);
+        const int rid = cidx(gr, i, j, k);
+        dst[rid] = accumulate ? dst[rid] + x : x;
     });
 }
 // dst (reference layout) = src on interior cells (overwrite) or += src (accumulate).
