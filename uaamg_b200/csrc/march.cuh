@@ -234,10 +234,21 @@ __device__ __forceinline__ T nbsum(const T (&c)[6], const T* v, int q, T vp, T v
     return nb;
 }
 
+// A smoother's quotient num / d.  The mixed form (couplings stored in FP16)
+// divides with the fast reciprocal, within 2 ulp: its V-cycle is only a
+// preconditioner, and every cell's diagonal is perturbed the same way in each
+// sweep, so the cycle stays symmetric.  Plain FP32 keeps IEEE division and FP64
+// the reference's (bit-exact) division.
+template <class T, class CS>
+__device__ __forceinline__ T mdiv(T num, T d) {
+    if constexpr (!std::is_same<CS, T>::value) return __fdividef(num, d);
+    else return num / d;
+}
+
 // Pre-smoothed value of the cell at box position (a, r): an odd active cell
 // smoothed from x = 0 has x = (b + 0)/d (skipped, x = 0, when d < 1e-30); every
 // other cell 0.
-template <int DIM, class T, class P, bool FINE>
+template <int DIM, class T, class P, bool FINE, class CS>
 __device__ __forceinline__ T presmooth(const MLevel<T>& L, const T* lut, const unsigned char* st,
                                        int a, int r, int i, int j, int k) {
     const uint32_t c = st[P::OFF_CODE + r * PBox<uint8_t>::W + a];
@@ -245,7 +256,7 @@ __device__ __forceinline__ T presmooth(const MLevel<T>& L, const T* lut, const u
     const int q = r * PBox<T>::W + a;
     const T d = mdiag<DIM, T, P, FINE>(L, lut, st, c, q, i, j, k);
     if (d < T(1e-30)) return T(0);
-    return (boxv<T>(st, P::QB * P::VB, q) + T(0)) / d;
+    return mdiv<T, CS>(boxv<T>(st, P::QB * P::VB, q) + T(0), d);
 }
 
 // Prolongation 2 x_coarse of the fine cell at box position (a, r): the parent box
@@ -470,7 +481,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__
     // odd value of the pair at plane p (stage st), placed in its column (0: A, 1: B);
     // bo = 1 when B is the odd cell
     auto odd_pair = [&](const unsigned char* st, int p, int bo, T& ya, T& yb) -> T {
-        const T v = presmooth<DIM, T, P, FINE>(L, lut, st, o.a, o.rb + bo, o.i, o.j + bo, p);
+        const T v = presmooth<DIM, T, P, FINE, CS>(L, lut, st, o.a, o.rb + bo, o.i, o.j + bo, p);
         ya = bo ? T(0) : v;
         yb = bo ? v : T(0);
         return v;
@@ -489,7 +500,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__
             Yn[o.qa + (pn ? 0 : W)] = v;
             if (hal) {
                 const int s0 = (ib + jb + kn) & 1, a = s0 ? ha1 : ha0, r = s0 ? hr1 : hr0;
-                Yn[r * W + a] = presmooth<DIM, T, P, FINE>(L, lut, sg.n, a, r, ib + a, jb + r, kn);
+                Yn[r * W + a] = presmooth<DIM, T, P, FINE, CS>(L, lut, sg.n, a, r, ib + a, jb + r, kn);
             }
         }
         if (DIM == 2) {
@@ -508,8 +519,8 @@ __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__
                 if (!(d < T(1e-30))) {
                     T cc[6];
                     mcoup<DIM, T, P, FINE, CS>(L, sg.c, sg.m, o.a, o.rb + e, cc);
-                    xe = (boxv<T>(sg.c, P::QB * P::VB, q) +
-                          nbsum<DIM, T>(cc, Yc, q, e ? ypb : ypa, e ? ymb : yma)) / d;
+                    xe = mdiv<T, CS>(boxv<T>(sg.c, P::QB * P::VB, q) +
+                                         nbsum<DIM, T>(cc, Yc, q, e ? ypb : ypa, e ? ymb : yma), d);
                 }
             }
             const int base = o.gid + k * g.sxy;
@@ -657,7 +668,7 @@ __global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ Ma
         if ((c & (kActive | kOdd)) != (kActive | kOdd)) return T(0);
         const int qq = r * W + a;
         const T d = mdiag<DIM, T, P, FINE>(L, lut, st, c, qq, ci, cj, ck);
-        const T pre = d < T(1e-30) ? T(0) : (boxv<T>(st, P::QB * P::VB, qq) + T(0)) / d;
+        const T pre = d < T(1e-30) ? T(0) : mdiv<T, CS>(boxv<T>(st, P::QB * P::VB, qq) + T(0), d);
         return pre + prolong_at<T, P>(st, a, r);
     };
     int kb, ke;
@@ -713,8 +724,8 @@ __global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ Ma
                 } else {
                     T cc[6];
                     mcoup<DIM, T, P, FINE, CS>(L, sg.c, sg.m, o.a, o.rb + e, cc);
-                    xe = (boxv<T>(sg.c, P::QB * P::VB, q) +
-                          nbsum<DIM, T>(cc, Yc, q, e ? ypb : ypa, e ? ymb : yma)) / d;
+                    xe = mdiv<T, CS>(boxv<T>(sg.c, P::QB * P::VB, q) +
+                                         nbsum<DIM, T>(cc, Yc, q, e ? ypb : ypa, e ? ymb : yma), d);
                 }
             }
             const int base = o.gid + k * g.sxy;
@@ -780,7 +791,7 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
                     mcoup<DIM, T, P, FINE, CS>(L, sg.c, sg.m, o.a, o.rb + od, cc);
                     const T vp = DIM == 3 ? boxv<T>(sg.n, P::QX * P::VB, q) : T(0);
                     const T vm = DIM == 3 ? boxv<T>(sg.m, P::QX * P::VB, q) : T(0);
-                    const T xv = (boxv<T>(sg.c, P::QB * P::VB, q) + nbsum<DIM, T>(cc, xb, q, vp, vm)) / d;
+                    const T xv = mdiv<T, CS>(boxv<T>(sg.c, P::QB * P::VB, q) + nbsum<DIM, T>(cc, xb, q, vp, vm), d);
                     if (od) zb = xv; else za = xv;
                     if (od ? o.inb : o.ina) x[o.gid + k * g.sxy + (od ? g.sx : 0)] = xv;
                 }
