@@ -343,34 +343,36 @@ __device__ __forceinline__ T fp32_ax(const MLevel<T>& L, uint32_t c, T d, const 
     }
 }
 
-// Per-march ring depth and dynamic shared-memory size.
+// Per-march ring depth and dynamic shared-memory size.  A 2D march reads one plane;
+// in 3D the depths trade prefetch distance against blocks per SM (measured on the
+// 256^3 benchmark: 6 / 5 stages on the finest level beat 8 / 6 and 5 / 4).
 template <int DIM, class T, bool FINE, class CS = T> struct FwdCfg {
     using P = MPlan<DIM, T, false, !FINE, false, CS>;
-    static constexpr int S = FINE ? 8 : 4;
+    static constexpr int S = DIM == 2 ? 1 : FINE ? 6 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
 template <int DIM, class T, bool FINE, class CS = T> struct ResCfg {
     using P = MPlan<DIM, T, true, !FINE, false, CS>;
-    static constexpr int S = FINE && sizeof(T) == 4 ? 6 : 4;
+    static constexpr int S = DIM == 2 ? 1 : FINE && sizeof(T) == 4 ? 5 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA;
 };
 template <int DIM, class T, bool FINE, class CS = T> struct UpeCfg {
     using P = MPlan<DIM, T, false, !FINE, true, CS>;
-    static constexpr int S = FINE ? 8 : 4;
+    static constexpr int S = DIM == 2 ? 1 : FINE ? 6 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
 template <int DIM, class T, bool FINE, class CS = T> struct UpoCfg {
     using P = MPlan<DIM, T, true, !FINE, false, CS>;
-    static constexpr int S = FINE && sizeof(T) == 4 ? 6 : 4;
+    static constexpr int S = DIM == 2 ? 1 : FINE && sizeof(T) == 4 ? 5 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA;
 };
 template <int DIM, class T> struct PmvCfg {
     using P = MPlan<DIM, T, true, false, false>;
-    static constexpr int S = sizeof(T) == 4 ? 6 : 4;
+    static constexpr int S = DIM == 2 ? 1 : sizeof(T) == 4 ? 5 : 4;
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA;
 };
