@@ -49,12 +49,12 @@ struct LevelBuf {
 // Kernel classes for the in-situ per-kernel timing (uaamg_profile_solve).
 enum KClass : int {
     K_SWEEP = 0, K_RESTRICT, K_PROLONG, K_COARSEST, K_PMATVEC, K_UPDATE, K_ZDOT, K_FWD, K_RES,
-    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_SCALAR, K_TAIL, K_NCLASS
+    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_TAIL, K_NCLASS
 };
 static const char* const kclass_names[K_NCLASS] = {
     "rbgs_sweep", "restrict_residual", "prolong_add", "coarsest_solve", "p_matvec_dot",
     "cg_update", "z_dot", "smooth_fwd", "residual_restrict", "prolong_smooth_even",
-    "smooth_odd", "true_residual", "rhs_prepare", "output", "cast", "hierarchy_setup", "scalar",
+    "smooth_odd", "true_residual", "rhs_prepare", "output", "cast", "hierarchy_setup",
     "small_levels"};
 
 struct KTag {
@@ -294,12 +294,13 @@ private:
 
     int max_reduce_blocks() const { return 4 * num_sms_; }
 
-    // grid of the FP64 residual column walk (kernels.cuh k_resid_x64): 32 x 8 columns
-    // of kResidZc planes a block
+    // grid of the FP64 residual column walk (kernels.cuh k_resid_x64): tiles of
+    // 32 x 8 columns and kResidZc planes, at most 8 blocks of 256 threads per SM
     static constexpr int kResidZc = 16;
-    static dim3 resid_grid(const Geom& g) {
-        return dim3((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 7) / 8),
-                    (unsigned)(g.nz ? (g.nz + kResidZc - 1) / kResidZc : 1));
+    dim3 resid_grid(const Geom& g) const {
+        const long long tiles = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8) *
+                                (g.nz ? (g.nz + kResidZc - 1) / kResidZc : 1);
+        return dim3((unsigned)std::min<long long>(tiles, 8LL * num_sms_));
     }
 
     // grid of the row-walk kernels (kernels.cuh for_cells): capped at 4 blocks per SM
@@ -916,7 +917,6 @@ private:
             UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (17.0 + 2.0 * sizeof(T))}),
                          (k_resid_x64<DIM, T>), resid_grid(g), dim3(32, 8), g, lv_[0].code, b64_, xd_,
                          xlo_, r_, st, kResidZc, partials_, cg_, 5, 1, cur_.tol, cur_.tol_mode);
-            UAAMG_LAUNCH((KTag{K_SCALAR, 0, 0.0}), k_maxiter_check, 1, 1, cg_);
         }
         cg_precond<DIM>();
     }

@@ -453,9 +453,11 @@ __global__ void k_true_residual(Geom g, const uint8_t* __restrict__ s, const dou
 // FP64 true residual r = b - A x of the finest level with x = x_hi + x_lo (either
 // part may be absent), the reference's operator (pcg_3d.cpp:38-55: a neighbour that
 // is not an interior fluid cell reads x_C, or -x_C across a Dirichlet wall),
-// neighbours from the cell codes.  A thread walks one (i, j) column through zc
-// planes, keeping x of the planes below, at and above in registers; every load of
-// a step is independent of the others.  Writes r as T to rw (0 on solid cells) when
+// neighbours from the cell codes.  A block of 32 x 8 threads takes tiles of as many
+// (i, j) columns and zc planes in turn (the grid is a few blocks per SM, so a
+// launch with no replacement due ends quickly); a thread walks its column's planes,
+// keeping x of the planes below, at and above in registers; every load of a step
+// is independent of the others.  Writes r as T to rw (0 on solid cells) when
 // given, reduces r.r; mode 1 (residual replacement, gated as replacement_due) also
 // asks the next x update to fold x_lo into x_hi; mode 2: exit diagnostics.
 template <int DIM, class T>
@@ -466,11 +468,13 @@ __global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __rest
                                                    Stencil st, int zc, double* partials, CGState* cg,
                                                    int slot, int mode, double tol, int tol_mode) {
     if (mode == 1 && !replacement_due(cg)) return;
-    const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
     double acc[1] = {0.0};
-    if (i <= g.nx && j <= g.ny) {
-        const int kb = DIM == 3 ? 1 + (int)blockIdx.z * zc : 0;
+    const int tx = (g.nx + 31) / 32, ty = (g.ny + 7) / 8, tz = DIM == 3 ? (g.nz + zc - 1) / zc : 1;
+    for (int w = blockIdx.x; w < tx * ty * tz; w += gridDim.x) {
+        const int i = 1 + 32 * (w % tx) + (int)threadIdx.x;
+        const int j = 1 + 8 * ((w / tx) % ty) + (int)threadIdx.y;
+        if (i > g.nx || j > g.ny) continue;
+        const int kb = DIM == 3 ? 1 + (w / (tx * ty)) * zc : 0;
         const int ke = DIM == 3 ? min(kb + zc, g.nz + 1) : 1;
         auto X = [&](int q) -> double {
             if (xhi && xlo) return xhi[q] + (double)xlo[q];
@@ -509,6 +513,11 @@ __global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __rest
     if (reduce_last<1>(acc, partials, &cg->counter[slot], tot)) {
         if (mode == 1) cg->fold = 1;
         true_residual_done(cg, tot[0], mode, tol, tol_mode);
+        // a replacement at max_iter that did not confirm convergence ends the solve
+        if (mode == 1 && !cg->done && cg->iter >= cg->max_iter) {
+            cg->status = CG_MAXITER;
+            cg->done = 1;
+        }
     }
 }
 
@@ -522,12 +531,6 @@ __global__ void k_norm(Geom g, const uint8_t* __restrict__ s, const double* __re
     });
     double tot[1];
     if (reduce_last<1>(acc, partials, &cg->counter[slot], tot)) cg->bnorm = sqrt(tot[0]);
-}
-
-// Mixed mode: after a replacement that did not converge, stop at max_iter.
-__global__ void k_maxiter_check(CGState* cg) {
-    if (cg->done) return;
-    if (cg->iter >= cg->max_iter && !cg->cand) { cg->status = CG_MAXITER; cg->done = 1; }
 }
 
 // Null-space projection of z and the new r.z (pcg_3d.cpp:112-123), given the

@@ -61,7 +61,9 @@ __device__ __forceinline__ void vfold<double>(double2& x, double* xhi, long long
 
 // In mixed mode (xhi given) a residual replacement in the previous iteration left
 // cg->fold set: x_lo is first folded into the FP64 x_hi (the value x_hi + x_lo the
-// replacement's residual was computed from) and restarts at 0.
+// replacement's residual was computed from) and restarts at 0.  Mixed mode also
+// stops at max_iter here unless a convergence candidate awaits its confirmation
+// (the residual replacement that follows stops it otherwise).
 template <class T>
 __global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
                                                      const T* __restrict__ p,
@@ -101,6 +103,10 @@ __global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
             else { cg->status = CG_CONVERGED; cg->done = 1; }
         } else if (cg->iter >= cg->max_iter && cg->replace_every == 0) {
             cg->status = CG_MAXITER; cg->done = 1;
+        }
+        if (cg->replace_every > 0 && !cg->done && cg->iter >= cg->max_iter && !cg->cand) {
+            cg->status = CG_MAXITER;
+            cg->done = 1;
         }
     }
 }
