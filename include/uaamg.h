@@ -142,6 +142,25 @@ UAAMG_API uaamg_status uaamg_solve(uaamg_handle* h, const double* rhs, double* p
 UAAMG_API uaamg_status uaamg_solve_device(uaamg_handle* h, const double* d_rhs, double* d_p,
                                 const uaamg_options* opts, uaamg_stats* stats);
 
+/* Pressure projection with DEVICE arrays: the PressureProjection::project /
+ * PressureProjection3D::project drop-in (src/pressure/pressure.cpp:5-33,
+ * pressure_3d.cpp:5-40) run on the GPU around the solve.  rhs = div(u)/dt on fluid
+ * interior cells (fvc::divergence, include/core/grid.h:44-47), p = 0 (kept as the
+ * initial guess when opts->warm_start), the solve as uaamg_solve_device, then
+ * u -= dt * grad p on every face between two fluid cells (pressure.cpp:21-32,
+ * pressure_3d.cpp:21-39).  FP64 face arrays, i fastest: d_u (nx+1)(ny+2)[(nz+2)],
+ * d_v (nx+2)(ny+1)[(nz+2)], d_w (nx+2)(ny+2)(nz+1) (3D; NULL in 2D); d_p padded
+ * cells.  Divergence and corrected velocities are the reference's FP64 expressions,
+ * bit for bit.  Returns the solve's status; as in the reference, the velocities are
+ * corrected whatever the solve's outcome (not after an argument or CUDA error). */
+UAAMG_API uaamg_status uaamg_project_device(uaamg_handle* h, double dt, double* d_u, double* d_v,
+                                  double* d_w, double* d_p, const uaamg_options* opts,
+                                  uaamg_stats* stats);
+
+/* The same with HOST arrays (the velocities and p are copied in and out). */
+UAAMG_API uaamg_status uaamg_project(uaamg_handle* h, double dt, double* u, double* v, double* w,
+                           double* p, const uaamg_options* opts, uaamg_stats* stats);
+
 /* One V(1,1) cycle z = M^{-1} r with HOST FP64 arrays: the
  * Preconditioner[3D]::apply drop-in (include/solver/preconditioner/
  * preconditioner_3d.h:18-33, UAAMGPreconditioner3D::apply). */

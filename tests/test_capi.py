@@ -54,6 +54,8 @@ def test_null_and_bad_arguments_are_rejected():
     assert lib.uaamg_create(C.byref(h), 12345) == _capi.INVALID_ARG
     assert lib.uaamg_destroy(None) == _capi.INVALID_ARG
     assert lib.uaamg_solve(None, None, None, None, None) == _capi.INVALID_ARG
+    assert lib.uaamg_project(None, 1.0, None, None, None, None, None, None) == _capi.INVALID_ARG
+    assert lib.uaamg_project_device(None, 1.0, None, None, None, None, None, None) == _capi.INVALID_ARG
     assert lib.uaamg_last_error(None) == b"NULL handle"
 
 

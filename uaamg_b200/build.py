@@ -30,6 +30,7 @@ UNITS = [
     ("api.cpp", ["-x", "cu"]),
     ("runtime.cpp", ["-x", "cu"]),
     ("noalloc.cu", ["-fmad=false"]),
+    ("project.cu", ["-fmad=false"]),
 ]
 HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "tail.cuh", "vec.cuh", "tma.cuh", "engine.cuh",
            "engine.h", "handle.h"]

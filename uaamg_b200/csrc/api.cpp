@@ -75,6 +75,11 @@ void free_problem(uaamg_handle* h) {
     cudaFree(h->d_rhs); h->d_rhs = nullptr;
     cudaFree(h->d_p); h->d_p = nullptr;
     cudaFree(h->d_hist); h->d_hist = nullptr;
+    for (int a = 0; a < 3; ++a) {
+        cudaFree(h->d_face[a]);
+        h->d_face[a] = nullptr;
+        h->face_n[a] = 0;
+    }
     h->hist_cap = 0;
     h->n = 0;
     h->dim = 0;

@@ -17,11 +17,13 @@ struct uaamg_handle {
     double* d_rhs = nullptr;  // staging for the host-array entry points
     double* d_p = nullptr;
     double* d_hist = nullptr;
+    double* d_face[3] = {nullptr, nullptr, nullptr};  // face velocities of uaamg_project
+    size_t face_n[3] = {0, 0, 0};
     int hist_cap = 0;
     int last_iters = 0;
     uaamg::Engine* eng[3] = {nullptr, nullptr, nullptr};
     bool ready[3] = {false, false, false};
-    int sweeps = 0;  // V-cycle kernels: 0 marches + small-level cluster kernel, 1 sweeps, 2 marches
+    int sweeps = 0;  // V-cycle kernels: 0 marches + small-level kernel, 1 sweeps, 2 marches
     int autotune = 0;
     std::string err;
     struct BatchPool* batch = nullptr;  // runtime.cpp: per-problem slots of uaamg_solve_batch

@@ -183,6 +183,41 @@ class Handle:
         self._check(s, "solve_device", (_capi.OK,) if strict else self._SOLVE_OK)
         return st
 
+    def face_shapes(self):
+        """Shapes of the FP64 face-velocity arrays u, v[, w] of the current problem."""
+        shp = self.shape
+        if len(shp) == 2:
+            ny2, nx2 = shp
+            return [(ny2, nx2 - 1), (ny2 - 1, nx2)]
+        nz2, ny2, nx2 = shp
+        return [(nz2, ny2, nx2 - 1), (nz2, ny2 - 1, nx2), (nz2 - 1, ny2, nx2)]
+
+    def project(self, u, v, w, p, dt: float, opts: _capi.Options | None = None,
+                strict: bool = False):
+        """Pressure projection with host arrays (uaamg_project): rhs = div(u)/dt,
+        solve into p, u/v/w corrected in place.  Returns stats."""
+        faces = [u, v] + ([w] if len(self.shape) == 3 else [])
+        for a, shp in zip(faces + [p], self.face_shapes() + [self.shape]):
+            if a.shape != shp or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError(f"arrays must be C-contiguous float64 of shapes "
+                                 f"{self.face_shapes()} and {self.shape}")
+        st = _capi.Stats()
+        s = self.lib.uaamg_project(self.h, float(dt), _ptr(u), _ptr(v),
+                                   _ptr(w) if len(self.shape) == 3 else None, _ptr(p),
+                                   C.byref(opts or self.options()), C.byref(st))
+        self._check(s, "project", (_capi.OK,) if strict else self._SOLVE_OK)
+        return st
+
+    def project_device(self, d_u: int, d_v: int, d_w: int, d_p: int, dt: float,
+                       opts: _capi.Options | None = None, strict: bool = False):
+        """Pressure projection with device pointers (uaamg_project_device)."""
+        st = _capi.Stats()
+        s = self.lib.uaamg_project_device(self.h, float(dt), C.c_void_p(d_u), C.c_void_p(d_v),
+                                          C.c_void_p(d_w) if d_w else None, C.c_void_p(d_p),
+                                          C.byref(opts or self.options()), C.byref(st))
+        self._check(s, "project_device", (_capi.OK,) if strict else self._SOLVE_OK)
+        return st
+
     def profile_solve(self, d_rhs: int, d_p: int, opts: _capi.Options | None = None):
         """uaamg_profile_solve: (stats, [dict(name, level, launches, total_ms,
         bytes_per_launch)])."""
@@ -397,6 +432,19 @@ class GpuUAAMGPCG(Solver):
         self.last_stats = self.handle.solve(rhs, g.p, opts)
         return self.last_stats
 
+    def project(self, g, dt, max_iter, tol):
+        """The whole pressure projection on the GPU (uaamg_project): divergence,
+        solve and face correction; g.p and the face velocities are updated."""
+        self._sync_problem(g)
+        opts = Handle.options(self.precision, tol, max_iter, self.tol_mode, self.warm_start,
+                              self.replace_every, self.project_mean, self.preconditioner)
+        for name in ("p", "u", "v") + (("w",) if g.dim == 3 else ()):
+            a = getattr(g, name)
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                setattr(g, name, np.ascontiguousarray(a, dtype=np.float64))
+        self.last_stats = self.handle.project(g.u, g.v, g.w if g.dim == 3 else None, g.p, dt, opts)
+        return self.last_stats
+
     def name(self):
         base = "PCG(CUDA-B200-UAAMG" if self.preconditioner else "CG(CUDA-B200"
         return f"{base},{self.precision})"
@@ -488,7 +536,11 @@ class PressureProjection:
                 ok, dt * (p[2:-1, 1:-1, 1:-1] - p[1:-2, 1:-1, 1:-1]) / g.dz, 0.0)
 
     @classmethod
-    def project(cls, g, dt, solver, max_iter, tol):
+    def project(cls, g, dt, solver, max_iter, tol, on_device=True):
+        """A solver that can run the whole projection on the GPU does so (no
+        host-side divergence or correction); any other solver gets the host steps."""
+        if on_device and hasattr(solver, "project"):
+            return solver.project(g, dt, max_iter, tol)
         rhs = cls.rhs(g, dt)
         g.p[...] = 0.0
         stats = solver.solve(g, rhs, max_iter, tol)
