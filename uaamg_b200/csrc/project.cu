@@ -23,26 +23,24 @@ using uaamg::api::fail;
 
 namespace {
 
-constexpr int kProjThreads = 256;
+constexpr int kProjThreads = 128;
 
-inline int proj_grid(long long n) {
-    long long b = (n + kProjThreads - 1) / kProjThreads;
-    if (b > 4096) b = 4096;
-    return (int)(b < 1 ? 1 : b);
+// Grid over an array of rows: x covers a row of fx entries, y the rows j, z the
+// planes k (one block row a thread row; no index division).
+inline dim3 row_grid(int fx, int fy, int fz) {
+    return dim3((unsigned)((fx + kProjThreads - 1) / kProjThreads), (unsigned)fy, (unsigned)fz);
 }
 
 // rhs over the whole padded cell array (0 on ghost and solid cells).
 __global__ void k_divergence(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
                              const uint8_t* __restrict__ solid, const double* __restrict__ u,
                              const double* __restrict__ v, const double* __restrict__ w, double dt,
-                             double* __restrict__ rhs, long long n) {
-    const long long sx = nx + 2, sy = ny + 2;
-    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < n;
-         id += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(id % sx);
-        const long long r = id / sx;
-        const int j = (int)(r % sy);
-        const int k = dim == 3 ? (int)(r / sy) : 0;
+                             double* __restrict__ rhs) {
+    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x), j = (int)blockIdx.y;
+    const int k = dim == 3 ? (int)blockIdx.z : 0;
+    if (i > nx + 1) return;
+    {
+        const long long id = i + (long long)(nx + 2) * (j + (long long)(ny + 2) * k);
         double out = 0.0;
         const bool inner = i >= 1 && i <= nx && j >= 1 && j <= ny && (dim == 2 || (k >= 1 && k <= nz));
         if (inner && !solid[id]) {
@@ -65,29 +63,28 @@ __global__ void k_divergence(int dim, int nx, int ny, int nz, double dx, double 
     }
 }
 
-// One face array (axis 0: u, 1: v, 2: w) of nf faces: f -= dt * (p_hi - p_lo) / h on the
-// interior faces whose two cells are fluid.
+// One face array (axis 0: u, 1: v, 2: w): f -= dt * (p_hi - p_lo) / h on the interior
+// faces whose two cells are fluid.
 __global__ void k_correct_faces(int dim, int axis, int nx, int ny, int nz, double h,
                                 const uint8_t* __restrict__ solid, const double* __restrict__ p,
-                                double dt, double* __restrict__ f, long long nf) {
+                                double dt, double* __restrict__ f) {
     const int fx = axis == 0 ? nx + 1 : nx + 2;
     const int fy = axis == 1 ? ny + 1 : ny + 2;
     const long long csx = nx + 2, csxy = (long long)(nx + 2) * (ny + 2);
     const long long step = axis == 0 ? 1 : (axis == 1 ? csx : csxy);
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nf;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % fx);
-        const long long r = t / fx;
-        const int j = (int)(r % fy);
-        const int k = dim == 3 ? (int)(r / fy) : 0;
+    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x), j = (int)blockIdx.y;
+    const int k = dim == 3 ? (int)blockIdx.z : 0;
+    if (i >= fx) return;
+    {
+        const long long t = i + (long long)fx * (j + (long long)fy * k);
         bool ok;
         if (axis == 0) ok = i >= 1 && i <= nx - 1 && j >= 1 && j <= ny;
         else if (axis == 1) ok = i >= 1 && i <= nx && j >= 1 && j <= ny - 1;
         else ok = i >= 1 && i <= nx && j >= 1 && j <= ny && k >= 1 && k <= nz - 1;
         if (dim == 3 && axis != 2) ok = ok && k >= 1 && k <= nz;
-        if (!ok) continue;
+        if (!ok) return;
         const long long c0 = i + j * csx + k * csxy, c1 = c0 + step;
-        if (solid[c0] || solid[c1]) continue;
+        if (solid[c0] || solid[c1]) return;
         f[t] -= dt * (p[c1] - p[c0]) / h;
     }
 }
@@ -114,10 +111,11 @@ uaamg_status project_dev(uaamg_handle* h, double dt, double* d_u, double* d_v, d
     if (!d_u || !d_v || !d_p || (h->dim == 3 && !d_w)) return fail(h, UAAMG_INVALID_ARG, "NULL array");
     if (!(dt > 0.0)) return fail(h, UAAMG_INVALID_ARG, "dt must be positive");
     const int dim = h->dim, nx = h->nx, ny = h->ny, nz = h->nz;
+    if (ny + 2 > 65535 || (dim == 3 && nz + 2 > 65535))
+        return fail(h, UAAMG_INVALID_ARG, "projection: more than 65533 cells along y or z");
     const long long n = (long long)h->n;
-    k_divergence<<<proj_grid(n), kProjThreads, 0, h->stream>>>(dim, nx, ny, nz, h->dx, h->dy, h->dz,
-                                                               h->d_solid, d_u, d_v, d_w, dt,
-                                                               h->d_rhs, n);
+    k_divergence<<<row_grid(nx + 2, ny + 2, dim == 3 ? nz + 2 : 1), kProjThreads, 0, h->stream>>>(
+        dim, nx, ny, nz, h->dx, h->dy, h->dz, h->d_solid, d_u, d_v, d_w, dt, h->d_rhs);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(h, e, "divergence");
     const bool warm = opts && opts->warm_start;
@@ -128,9 +126,10 @@ uaamg_status project_dev(uaamg_handle* h, double dt, double* d_u, double* d_v, d
     double* f[3] = {d_u, d_v, d_w};
     const double hh[3] = {h->dx, h->dy, h->dz};
     for (int a = 0; a < dim; ++a) {
-        const long long nf = face_count(dim, nx, ny, nz, a);
-        k_correct_faces<<<proj_grid(nf), kProjThreads, 0, h->stream>>>(dim, a, nx, ny, nz, hh[a],
-                                                                       h->d_solid, d_p, dt, f[a], nf);
+        const int fx = a == 0 ? nx + 1 : nx + 2, fy = a == 1 ? ny + 1 : ny + 2;
+        const int fz = dim == 3 ? (a == 2 ? nz + 1 : nz + 2) : 1;
+        k_correct_faces<<<row_grid(fx, fy, fz), kProjThreads, 0, h->stream>>>(dim, a, nx, ny, nz, hh[a],
+                                                                              h->d_solid, d_p, dt, f[a]);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(h, e, "velocity correction");
     return s;

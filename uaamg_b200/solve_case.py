@@ -1,8 +1,11 @@
 """Command-line solve of the spheres workload: one GPU PCG solve of an n^3 Neumann
 Poisson problem with seeded solid spheres and a smoothed-noise right-hand side
-(the 256^3 benchmark problem at n = 256), through the C-ABI.
+(the 256^3 benchmark problem at n = 256), through the C-ABI.  With
+--workload obstacle_2d --project: one device-side pressure projection (divergence,
+solve, face correction) of the 2048 x 1024 obstacle flow.
 
     python -m uaamg_b200.solve_case --n 256 --precision mixed --max-iter 90
+    python -m uaamg_b200.solve_case --workload obstacle_2d --project
 
 Prints one line with the status, iterations, FP64 true relative residual and the
 wall time of the solve.  Used as the profiling target of the kernel summaries
@@ -27,7 +30,25 @@ def main(argv=None):
     ap.add_argument("--max-iter", type=int, default=500)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--workload", default="spheres", choices=["spheres", "obstacle_2d"])
+    ap.add_argument("--project", action="store_true")
     a = ap.parse_args(argv)
+    if a.workload == "obstacle_2d":
+        solid, u0, v0, rhs, dx, dy, dt = workloads.obstacle_2d()
+        hd = Handle(0)
+        hd.set_problem(solid, dx, dy)
+        opts = hd.options(a.precision, a.tol, a.max_iter, "rel")
+        for _ in range(a.repeat):
+            p = np.zeros_like(rhs)
+            u, v = u0.copy(), v0.copy()
+            t0 = time.perf_counter()
+            st = hd.project(u, v, None, p, dt, opts) if a.project else hd.solve(rhs, p, opts)
+            ms = (time.perf_counter() - t0) * 1e3
+        print(json.dumps({"workload": "obstacle_2d", "project": a.project, "precision": a.precision,
+                          "status": st.status, "iterations": st.iterations,
+                          "true_rel_residual": st.rel_residual, "ms": round(ms, 3)}))
+        hd.close()
+        return
     if a.n == 256:
         solid, rhs, h = workloads.spheres_256()
     else:
