@@ -161,6 +161,21 @@ UAAMG_API uaamg_status uaamg_project_device(uaamg_handle* h, double dt, double* 
 UAAMG_API uaamg_status uaamg_project(uaamg_handle* h, double dt, double* u, double* v, double* w,
                            double* p, const uaamg_options* opts, uaamg_stats* stats);
 
+/* Static pressure recovery with DEVICE arrays: the
+ * PressureProjection::recoverStaticPressure drop-in (src/pressure/pressure.cpp:35-66;
+ * the second pressure solve of each LFM cycle, src/lfm/lfm_simulator.cpp:199), 2D:
+ * rhs = -(du/dx^2 + 2 du/dy dv/dx + dv/dy^2) from cell-centre velocities (cross
+ * derivatives dropped next to solids), p = 0, then the solve as uaamg_solve_device on
+ * the current problem's hierarchy.  d_u (nx+1)(ny+2), d_v (nx+2)(ny+1), d_p padded;
+ * the right-hand side is the reference's FP64 expression, bit for bit. */
+UAAMG_API uaamg_status uaamg_static_pressure_device(uaamg_handle* h, const double* d_u,
+                                          const double* d_v, double* d_p,
+                                          const uaamg_options* opts, uaamg_stats* stats);
+
+/* The same with HOST arrays (u and v copied in, p out). */
+UAAMG_API uaamg_status uaamg_static_pressure(uaamg_handle* h, const double* u, const double* v,
+                                   double* p, const uaamg_options* opts, uaamg_stats* stats);
+
 /* One V(1,1) cycle z = M^{-1} r with HOST FP64 arrays: the
  * Preconditioner[3D]::apply drop-in (include/solver/preconditioner/
  * preconditioner_3d.h:18-33, UAAMGPreconditioner3D::apply). */

@@ -71,6 +71,7 @@ def lib():
                                               _p, _p]
         L.oracle_divergence_rhs.argtypes = [_i, _i, _i, _i, _d, _d, _d, _p, _p, _p, _p, _d,
                                             _p]
+        L.oracle_static_rhs_2d.argtypes = [_i, _i, _d, _d, _p, _p, _p, _p]
     return _lib
 
 
@@ -94,6 +95,7 @@ def ref():
         R.ref_pcg_3d.argtypes = [_i, _i, _i, _d, _d, _d, _p, _p, _p, _i, _d, _i]
         R.ref_project_2d.restype = _i
         R.ref_project_2d.argtypes = [_i, _i, _d, _d, _p, _p, _p, _d, _i, _d, _p]
+        R.ref_static_rhs_2d.argtypes = [_i, _i, _d, _d, _p, _p, _p, _p]
         R.ref_project_3d.restype = _i
         R.ref_project_3d.argtypes = [_i, _i, _i, _d, _d, _d, _p, _p, _p, _p, _d, _i, _d, _p]
     return _ref
@@ -262,6 +264,24 @@ def ref_pcg(solid, rhs, dx, dy, dz=1.0, max_iter=200, tol=1e-6, precond=True):
         n = ref().ref_pcg_2d(nx, ny, dx, dy, _ptr(solid), _ptr(rhs), _ptr(p), max_iter, tol,
                              int(precond))
     return p, n
+
+
+def static_rhs(solid, u, v, dx, dy):
+    """RHS of recoverStaticPressure (pressure.cpp:35-66), 2D, padded."""
+    solid = _c8(solid)
+    _, nx, ny, _ = _dims(solid.shape)
+    rhs = np.zeros(solid.shape)
+    lib().oracle_static_rhs_2d(nx, ny, dx, dy, _ptr(solid), _ptr(_cd(u)), _ptr(_cd(v)), _ptr(rhs))
+    return rhs
+
+
+def ref_static_rhs(solid, u, v, dx, dy):
+    """The same right-hand side as the reference's own recoverStaticPressure builds it."""
+    solid = _c8(solid)
+    _, nx, ny, _ = _dims(solid.shape)
+    rhs = np.zeros(solid.shape)
+    ref().ref_static_rhs_2d(nx, ny, dx, dy, _ptr(solid), _ptr(_cd(u)), _ptr(_cd(v)), _ptr(rhs))
+    return rhs
 
 
 def ref_project(solid, u, v, w, dx, dy, dz, dt, max_iter, tol):

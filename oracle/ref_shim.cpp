@@ -60,6 +60,18 @@ Grid3D make3(int nx, int ny, int nz, double dx, double dy, double dz, const uint
     return g;
 }
 
+// Records the right-hand side a caller hands to solve() and leaves p untouched.
+class CapturingSolver : public Solver {
+public:
+    explicit CapturingSolver(double* out) : out_(out) {}
+    void solve(Grid&, const std::vector<double>& rhs, int, double) override {
+        std::memcpy(out_, rhs.data(), sizeof(double) * rhs.size());
+    }
+    std::string name() const override { return "capture"; }
+private:
+    double* out_;
+};
+
 }  // namespace
 
 extern "C" {
@@ -135,6 +147,17 @@ int ref_project_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
     std::memcpy(v, g.v.data(), sizeof(double) * g.v_size());
     std::memcpy(p, g.p.data(), sizeof(double) * g.p_size());
     return applies;
+}
+
+// The right-hand side PressureProjection::recoverStaticPressure (pressure.cpp:35-66)
+// builds for u (nx+1)(ny+2), v (nx+2)(ny+1); rhs is padded (nx+2)(ny+2).
+void ref_static_rhs_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+                       const double* u, const double* v, double* rhs) {
+    Grid g = make2(nx, ny, dx, dy, solid);
+    std::memcpy(g.u.data(), u, sizeof(double) * g.u_size());
+    std::memcpy(g.v.data(), v, sizeof(double) * g.v_size());
+    CapturingSolver cap(rhs);
+    PressureProjection::recoverStaticPressure(g, cap, 1, 1e-6);
 }
 
 int ref_project_3d(int nx, int ny, int nz, double dx, double dy, double dz, const uint8_t* solid,

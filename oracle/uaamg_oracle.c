@@ -606,3 +606,39 @@ void oracle_correct_velocity(int dim, int nx, int ny, int nz, double dx, double 
                 w[i + j * sw + k * sww] -= dt * (p[cid(L, i, j, k + 1)] - p[cid(L, i, j, k)]) / dz;
             }
 }
+
+/* RHS of PressureProjection::recoverStaticPressure (pressure.cpp:35-66), 2D:
+ * rhs = -(du/dx^2 + 2 du/dy dv/dx + dv/dy^2) on fluid cells, with cell-centre
+ * velocities uc, vc at indices clamped to the interior and the cross derivatives
+ * dropped next to a solid (up/down for du/dy, left/right for dv/dx). */
+static double os_uc(const double* u, int nx, int ny, int i, int j) {
+    i = i < 1 ? 1 : (i > nx ? nx : i);
+    j = j < 1 ? 1 : (j > ny ? ny : j);
+    const long su = nx + 1;
+    return 0.5 * (u[i + j * su] + u[(i - 1) + j * su]);
+}
+static double os_vc(const double* v, int nx, int ny, int i, int j) {
+    i = i < 1 ? 1 : (i > nx ? nx : i);
+    j = j < 1 ? 1 : (j > ny ? ny : j);
+    const long sv = nx + 2;
+    return 0.5 * (v[i + j * sv] + v[i + (j - 1) * sv]);
+}
+
+void oracle_static_rhs_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+                          const double* u, const double* v, double* rhs) {
+    const long sp = nx + 2, su = nx + 1, sv = nx + 2;
+    memset(rhs, 0, sizeof(double) * (size_t)(nx + 2) * (ny + 2));
+    for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++) {
+            if (solid[i + j * sp]) continue;
+            double du_dx = (u[i + j * su] - u[(i - 1) + j * su]) / dx;
+            double dv_dy = (v[i + j * sv] - v[i + (j - 1) * sv]) / dy;
+            int sL = solid[(i - 1) + j * sp] != 0, sR = solid[(i + 1) + j * sp] != 0;
+            int sB = solid[i + (j - 1) * sp] != 0, sT = solid[i + (j + 1) * sp] != 0;
+            double du_dy = (sB || sT) ? 0.0
+                                      : (os_uc(u, nx, ny, i, j + 1) - os_uc(u, nx, ny, i, j - 1)) / (2 * dy);
+            double dv_dx = (sL || sR) ? 0.0
+                                      : (os_vc(v, nx, ny, i + 1, j) - os_vc(v, nx, ny, i - 1, j)) / (2 * dx);
+            rhs[i + j * sp] = -(du_dx * du_dx + 2.0 * du_dy * dv_dx + dv_dy * dv_dy);
+        }
+}

@@ -73,6 +73,10 @@ void oracle_divergence_rhs(int dim, int nx, int ny, int nz, double dx, double dy
                            const uint8_t* solid, const double* u, const double* v,
                            const double* w, double dt, double* rhs);
 
+/* RHS of PressureProjection::recoverStaticPressure (pressure.cpp:35-66), 2D. */
+void oracle_static_rhs_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+                          const double* u, const double* v, double* rhs);
+
 #ifdef __cplusplus
 }
 #endif

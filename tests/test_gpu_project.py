@@ -100,3 +100,33 @@ def test_pressure_projection_uses_the_device_path():
         results.append((g.p.copy(), g.u.copy(), g.v.copy()))
     (p1, u1, v1), (p2, u2, v2) = results
     assert np.array_equal(p1, p2) and np.array_equal(u1, u2) and np.array_equal(v1, v2)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_static_pressure_matches_reference_rhs_and_solve(prec):
+    """recoverStaticPressure (pressure.cpp:35-66): the device right-hand side is the
+    reference's, so the pressure equals the same solve of the oracle's RHS bit for bit;
+    the host- and device-array forms agree; 3D is rejected as in the reference."""
+    torch = pytest.importorskip("torch")
+    s, u, v, _, dx, dy, dz = _case(2, 23)
+    hd = Handle(0)
+    hd.set_problem(s, dx, dy, dz)
+    opts = hd.options(prec, 1e-8 if prec == "fp64" else 1e-6, 500, "rel")
+    rhs = O.static_rhs(s, u, v, dx, dy)
+    p_ref = np.zeros_like(rhs)
+    hd.solve(rhs, p_ref, opts)
+    p = np.full(s.shape, 3.0)  # overwritten: the recovery starts from p = 0
+    st = hd.static_pressure(u.copy(), v.copy(), p, opts)
+    assert st.status == 0 and np.array_equal(p, p_ref)
+    du, dv = torch.from_numpy(u.copy()).cuda(), torch.from_numpy(v.copy()).cuda()
+    dp = torch.zeros(s.shape, dtype=torch.float64, device="cuda")
+    hd.static_pressure_device(du.data_ptr(), dv.data_ptr(), dp.data_ptr(), opts)
+    torch.cuda.synchronize()
+    assert np.array_equal(dp.cpu().numpy(), p_ref)
+    hd.close()
+    s3, u3, v3, w3, h3, _, _ = _case(3, 5)
+    hd3 = Handle(0)
+    hd3.set_problem(s3, h3, h3, h3)
+    with pytest.raises(Exception):
+        hd3.static_pressure_device(1, 1, 1, hd3.options("fp64"))
+    hd3.close()

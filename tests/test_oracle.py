@@ -107,3 +107,18 @@ def test_oracle_relative_mode_reaches_tolerance():
     p2, it2, st2 = O.pcg(solid, rhs, 0.1, 0.1, 0.1, max_iter=200, tol=1e-6, tol_mode=1, x0=p,
                          warm=True)
     assert it2 <= 1
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference (oracle/_ref) not present")
+@pytest.mark.parametrize("seed", range(4))
+def test_static_pressure_rhs_matches_compiled_reference(seed):
+    """recoverStaticPressure's right-hand side (pressure.cpp:35-66): the restatement
+    equals what the reference's own function hands its solver, bit for bit, with
+    solids touching walls and each other (the clamped and dropped stencil branches)."""
+    rng = np.random.default_rng(seed)
+    nx, ny = [(17, 11), (32, 24), (9, 40), (64, 48)][seed]
+    dx, dy = rng.uniform(0.01, 1.0, size=2)
+    solid = (rng.random((ny + 2, nx + 2)) < [0.0, 0.1, 0.3, 0.05][seed]).astype(np.uint8)
+    u = rng.standard_normal((ny + 2, nx + 1))
+    v = rng.standard_normal((ny + 1, nx + 2))
+    assert np.array_equal(O.static_rhs(solid, u, v, dx, dy), O.ref_static_rhs(solid, u, v, dx, dy))

@@ -35,7 +35,8 @@ EXPORTS = [
     "uaamg_set_vcycle_kernels", "uaamg_residual_noalloc", "uaamg_solve_batch",
     "uaamg_set_autotune", "uaamg_server_default_config", "uaamg_server_start",
     "uaamg_server_submit", "uaamg_server_poll", "uaamg_server_drain", "uaamg_server_info",
-    "uaamg_server_stop", "uaamg_project", "uaamg_project_device",
+    "uaamg_server_stop", "uaamg_project", "uaamg_project_device", "uaamg_static_pressure",
+    "uaamg_static_pressure_device",
 ]
 
 
@@ -152,6 +153,8 @@ def load(path: str | None = None):
     L.uaamg_solve_device.argtypes = [p, p, p, C.POINTER(Options), C.POINTER(Stats)]
     L.uaamg_project.argtypes = [p, d, p, p, p, p, C.POINTER(Options), C.POINTER(Stats)]
     L.uaamg_project_device.argtypes = [p, d, p, p, p, p, C.POINTER(Options), C.POINTER(Stats)]
+    L.uaamg_static_pressure.argtypes = [p, p, p, p, C.POINTER(Options), C.POINTER(Stats)]
+    L.uaamg_static_pressure_device.argtypes = [p, p, p, p, C.POINTER(Options), C.POINTER(Stats)]
     L.uaamg_precond_apply.argtypes = [p, i, p, p]
     L.uaamg_residual_history.argtypes = [p, p, i]
     L.uaamg_num_levels.argtypes = [p, C.POINTER(i)]

@@ -89,6 +89,44 @@ __global__ void k_correct_faces(int dim, int axis, int nx, int ny, int nz, doubl
     }
 }
 
+// Cell-centre velocities of recoverStaticPressure, indices clamped to the interior.
+__device__ __forceinline__ double st_uc(const double* u, int nx, int ny, int i, int j) {
+    i = i < 1 ? 1 : (i > nx ? nx : i);
+    j = j < 1 ? 1 : (j > ny ? ny : j);
+    const long long su = nx + 1;
+    return 0.5 * (u[i + j * su] + u[(i - 1) + j * su]);
+}
+__device__ __forceinline__ double st_vc(const double* v, int nx, int ny, int i, int j) {
+    i = i < 1 ? 1 : (i > nx ? nx : i);
+    j = j < 1 ? 1 : (j > ny ? ny : j);
+    const long long sv = nx + 2;
+    return 0.5 * (v[i + j * sv] + v[i + (j - 1) * sv]);
+}
+
+// Right-hand side of PressureProjection::recoverStaticPressure (pressure.cpp:35-66),
+// 2D: rhs = -(du/dx^2 + 2 du/dy dv/dx + dv/dy^2) on fluid cells, the cross
+// derivatives dropped next to a solid; 0 on ghost and solid cells.
+__global__ void k_static_rhs(int nx, int ny, double dx, double dy, const uint8_t* __restrict__ solid,
+                             const double* __restrict__ u, const double* __restrict__ v,
+                             double* __restrict__ rhs) {
+    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x), j = (int)blockIdx.y;
+    if (i > nx + 1) return;
+    const long long sp = nx + 2, su = nx + 1, sv = nx + 2;
+    const long long id = i + j * sp;
+    double out = 0.0;
+    if (i >= 1 && i <= nx && j >= 1 && j <= ny && !solid[id]) {
+        const double du_dx = (u[i + j * su] - u[(i - 1) + j * su]) / dx;
+        const double dv_dy = (v[i + j * sv] - v[i + (j - 1) * sv]) / dy;
+        const bool sL = solid[id - 1], sR = solid[id + 1], sB = solid[id - sp], sT = solid[id + sp];
+        const double du_dy =
+            (sB || sT) ? 0.0 : (st_uc(u, nx, ny, i, j + 1) - st_uc(u, nx, ny, i, j - 1)) / (2 * dy);
+        const double dv_dx =
+            (sL || sR) ? 0.0 : (st_vc(v, nx, ny, i + 1, j) - st_vc(v, nx, ny, i - 1, j)) / (2 * dx);
+        out = -(du_dx * du_dx + 2.0 * du_dy * dv_dx + dv_dy * dv_dy);
+    }
+    rhs[id] = out;
+}
+
 long long face_count(int dim, int nx, int ny, int nz, int axis) {
     const long long zz = dim == 3 ? nz + 2 : 1;
     if (axis == 0) return (long long)(nx + 1) * (ny + 2) * zz;
@@ -133,6 +171,23 @@ uaamg_status project_dev(uaamg_handle* h, double dt, double* d_u, double* d_v, d
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(h, e, "velocity correction");
     return s;
+}
+
+// recoverStaticPressure: its right-hand side into the handle's staging RHS, p = 0,
+// the solve (the hierarchy of the current problem is reused).
+uaamg_status static_dev(uaamg_handle* h, const double* d_u, const double* d_v, double* d_p,
+                        const uaamg_options* opts, uaamg_stats* stats) {
+    if (!h->dim) return fail(h, UAAMG_NO_PROBLEM, "no problem set (call uaamg_set_problem_*)");
+    if (h->dim != 2) return fail(h, UAAMG_INVALID_ARG, "static pressure recovery is 2D (as in the reference)");
+    if (!d_u || !d_v || !d_p) return fail(h, UAAMG_INVALID_ARG, "NULL array");
+    if (h->ny + 2 > 65535) return fail(h, UAAMG_INVALID_ARG, "static pressure: more than 65533 rows");
+    k_static_rhs<<<row_grid(h->nx + 2, h->ny + 2, 1), kProjThreads, 0, h->stream>>>(
+        h->nx, h->ny, h->dx, h->dy, h->d_solid, d_u, d_v, h->d_rhs);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, "static rhs");
+    if ((e = cudaMemsetAsync(d_p, 0, h->n * sizeof(double), h->stream)) != cudaSuccess)
+        return cuda_fail(h, e, "zero p");
+    return uaamg_solve_device(h, h->d_rhs, d_p, opts, stats);
 }
 
 // Device copies of the face arrays for the host-array entry point, sized on demand.
@@ -198,6 +253,39 @@ uaamg_status uaamg_project(uaamg_handle* h, double dt, double* u, double* v, dou
     if (e != cudaSuccess) return cuda_fail(h, e, "download");
     if (stats)
         stats->solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return s;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+uaamg_status uaamg_static_pressure_device(uaamg_handle* h, const double* d_u, const double* d_v,
+                                          double* d_p, const uaamg_options* opts, uaamg_stats* stats) {
+    if (!h) return UAAMG_INVALID_ARG;
+    cudaSetDevice(h->device);
+    return static_dev(h, d_u, d_v, d_p, opts, stats);
+}
+
+uaamg_status uaamg_static_pressure(uaamg_handle* h, const double* u, const double* v, double* p,
+                                   const uaamg_options* opts, uaamg_stats* stats) {
+    if (!h) return UAAMG_INVALID_ARG;
+    if (!h->dim) return fail(h, UAAMG_NO_PROBLEM, "no problem set (call uaamg_set_problem_*)");
+    if (h->dim != 2) return fail(h, UAAMG_INVALID_ARG, "static pressure recovery is 2D (as in the reference)");
+    if (!u || !v || !p) return fail(h, UAAMG_INVALID_ARG, "NULL array");
+    cudaSetDevice(h->device);
+    uaamg_status s = ensure_faces(h);
+    if (s != UAAMG_OK) return s;
+    cudaError_t e = cudaMemcpyAsync(h->d_face[0], u, h->face_n[0] * sizeof(double), cudaMemcpyHostToDevice,
+                                    h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->d_face[1], v, h->face_n[1] * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "upload");
+    s = static_dev(h, h->d_face[0], h->d_face[1], h->d_p, opts, stats);
+    if (!solved(s)) return s;
+    e = cudaMemcpyAsync(p, h->d_p, h->n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "download");
     return s;
 }
 

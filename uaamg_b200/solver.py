@@ -218,6 +218,28 @@ class Handle:
         self._check(s, "project_device", (_capi.OK,) if strict else self._SOLVE_OK)
         return st
 
+    def static_pressure(self, u, v, p, opts: _capi.Options | None = None, strict: bool = False):
+        """recoverStaticPressure on the GPU with host arrays (uaamg_static_pressure, 2D):
+        p is overwritten with the static pressure.  Returns stats."""
+        for a, shp in zip((u, v, p), self.face_shapes() + [self.shape]):
+            if a.shape != shp or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("arrays must be C-contiguous float64 of the grid's shapes")
+        st = _capi.Stats()
+        s = self.lib.uaamg_static_pressure(self.h, _ptr(u), _ptr(v), _ptr(p),
+                                           C.byref(opts or self.options()), C.byref(st))
+        self._check(s, "static_pressure", (_capi.OK,) if strict else self._SOLVE_OK)
+        return st
+
+    def static_pressure_device(self, d_u: int, d_v: int, d_p: int,
+                               opts: _capi.Options | None = None, strict: bool = False):
+        """recoverStaticPressure with device pointers (uaamg_static_pressure_device)."""
+        st = _capi.Stats()
+        s = self.lib.uaamg_static_pressure_device(self.h, C.c_void_p(d_u), C.c_void_p(d_v),
+                                                  C.c_void_p(d_p), C.byref(opts or self.options()),
+                                                  C.byref(st))
+        self._check(s, "static_pressure_device", (_capi.OK,) if strict else self._SOLVE_OK)
+        return st
+
     def profile_solve(self, d_rhs: int, d_p: int, opts: _capi.Options | None = None):
         """uaamg_profile_solve: (stats, [dict(name, level, launches, total_ms,
         bytes_per_launch)])."""
@@ -445,6 +467,19 @@ class GpuUAAMGPCG(Solver):
         self.last_stats = self.handle.project(g.u, g.v, g.w if g.dim == 3 else None, g.p, dt, opts)
         return self.last_stats
 
+    def recover_static_pressure(self, g, max_iter, tol):
+        """recoverStaticPressure on the GPU (uaamg_static_pressure): g.p receives the
+        static pressure of the current velocity field (2D)."""
+        self._sync_problem(g)
+        opts = Handle.options(self.precision, tol, max_iter, self.tol_mode, False,
+                              self.replace_every, self.project_mean, self.preconditioner)
+        for name in ("p", "u", "v"):
+            a = getattr(g, name)
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                setattr(g, name, np.ascontiguousarray(a, dtype=np.float64))
+        self.last_stats = self.handle.static_pressure(g.u, g.v, g.p, opts)
+        return self.last_stats
+
     def name(self):
         base = "PCG(CUDA-B200-UAAMG" if self.preconditioner else "CG(CUDA-B200"
         return f"{base},{self.precision})"
@@ -534,6 +569,13 @@ class PressureProjection:
             ok = ~(s[1:-2, 1:-1, 1:-1] | s[2:-1, 1:-1, 1:-1])
             g.w[1:-1, 1:-1, 1:-1] -= np.where(
                 ok, dt * (p[2:-1, 1:-1, 1:-1] - p[1:-2, 1:-1, 1:-1]) / g.dz, 0.0)
+
+    @staticmethod
+    def recover_static_pressure(g, solver, max_iter, tol):
+        """PressureProjection::recoverStaticPressure (pressure.cpp:35-66): the static
+        pressure of the current velocities into g.p, its right-hand side built and
+        solved on the GPU."""
+        return solver.recover_static_pressure(g, max_iter, tol)
 
     @classmethod
     def project(cls, g, dt, solver, max_iter, tol, on_device=True):
