@@ -156,7 +156,7 @@ uaamg_status ensure_hist(uaamg_handle* h, int max_iter) {
 }
 
 uaamg_status solve_dev(uaamg_handle* h, const double* d_rhs, double* d_p, const uaamg_options* o,
-                       uaamg_stats* st) {
+                       uaamg_stats* st, cudaEvent_t p_ready = nullptr) {
     uaamg_options opts;
     uaamg_default_options(&opts);
     if (o) opts = *o;
@@ -180,6 +180,7 @@ uaamg_status solve_dev(uaamg_handle* h, const double* d_rhs, double* d_p, const 
     a.precond = opts.preconditioner;
     a.hist = h->d_hist;
     a.ref_solid = h->d_solid;
+    a.x_ready = p_ready;
     uaamg::SolveResult r;
     std::memset(&r, 0, sizeof(r));
     int e = eng->solve(a, &r);
@@ -228,6 +229,8 @@ uaamg_status uaamg_destroy(uaamg_handle* h) {
     free_problem(h);
     uaamg::api::free_batch(h);
     for (auto*& e : h->eng) { delete e; e = nullptr; }
+    if (h->p_ready) cudaEventDestroy(h->p_ready);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     delete h;
     return UAAMG_OK;
 }
@@ -277,9 +280,25 @@ uaamg_status uaamg_solve(uaamg_handle* h, const double* rhs, double* p, const ua
     auto t0 = std::chrono::steady_clock::now();
     const size_t bytes = h->n * sizeof(double);
     cudaError_t e = cudaMemcpyAsync(h->d_rhs, rhs, bytes, cudaMemcpyHostToDevice, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_p, p, bytes, cudaMemcpyHostToDevice, h->stream);
+    // p is read only when the solve adds its result to it (or at the start of a warm
+    // start): without a warm start it is uploaded on a side stream while the solve runs
+    cudaEvent_t p_ready = nullptr;
+    if (e == cudaSuccess && !(opts && opts->warm_start)) {
+        if (!h->copy_stream && cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+            h->copy_stream = nullptr;
+        if (h->copy_stream && !h->p_ready &&
+            cudaEventCreateWithFlags(&h->p_ready, cudaEventDisableTiming) != cudaSuccess)
+            h->p_ready = nullptr;
+        if (h->copy_stream && h->p_ready) {
+            e = cudaMemcpyAsync(h->d_p, p, bytes, cudaMemcpyHostToDevice, h->copy_stream);
+            if (e == cudaSuccess) e = cudaEventRecord(h->p_ready, h->copy_stream);
+            if (e == cudaSuccess) p_ready = h->p_ready;
+        }
+    }
+    if (e == cudaSuccess && !p_ready) e = cudaMemcpyAsync(h->d_p, p, bytes, cudaMemcpyHostToDevice, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "upload");
-    uaamg_status s = solve_dev(h, h->d_rhs, h->d_p, opts, stats);
+    uaamg_status s = solve_dev(h, h->d_rhs, h->d_p, opts, stats, p_ready);
+    if (p_ready) cudaEventSynchronize(p_ready);  // the upload has finished whatever the outcome
     if (s == UAAMG_OK || s == UAAMG_NOT_CONVERGED || s == UAAMG_BREAKDOWN || s == UAAMG_NAN) {
         e = cudaMemcpyAsync(p, h->d_p, bytes, cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);

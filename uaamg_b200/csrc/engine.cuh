@@ -950,6 +950,7 @@ private:
         UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 17.0}), k_sub_mean<DIM>, vg, vb, g, s, b64_, cg_);
         UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 9.0}), k_norm<DIM>, vg, vb, g, s, b64_, partials_, cg_, 4);
         if (a.warm) {  // b <- b - A x_in: the solve then finds the correction to x_in
+            if (a.x_ready) cudaStreamWaitEvent(st_, a.x_ready, 0);
             UAAMG_LAUNCH((KTag{K_RHS, 0, cells(g) * 16.0}), (k_import<DIM, double>), vg, vb, g, gref_, a.x, xd_);
             UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * 25.0}), (k_true_residual<DIM, double>), vg, vb,
                          g, s, b64_, xd_, b64_, st, partials_, cg_, 5, 3, a.tol, a.tol_mode);
@@ -1035,6 +1036,7 @@ private:
         UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (9.0 + xb)}), (k_resid_x64<DIM, T>),
                      resid_grid(g), dim3(32, 8), g, lv_[0].code, b64_, xhi, xlo_, (T*)nullptr, st,
                      kResidZc, partials_, cg_, 5, 2, a.tol, a.tol_mode);
+        if (a.x_ready) cudaStreamWaitEvent(st_, a.x_ready, 0);  // the caller's x, accumulated into
         UAAMG_LAUNCH((KTag{K_OUTPUT, 0, cells(g) * (16.0 + xb)}), (k_export_x<DIM, T>), vg, vb, g, gref_,
                      xhi, xlo_, a.x, 1);
         if (a.project_mean && a.ref_solid) {

@@ -24,6 +24,8 @@ struct SolveArgs {
     int precond;         // 1 UAAMG V-cycle, 0 identity (plain CG)
     double* hist;        // optional device array, max_iter+1: ||r_k|| per update
     const uint8_t* ref_solid;  // the caller's mask (reference layout), for project_mean
+    cudaEvent_t x_ready = nullptr;  // optional: x holds its input once this event completes
+                                    // (waited on just before x is first read)
 };
 
 struct SolveResult {

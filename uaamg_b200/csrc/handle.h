@@ -18,6 +18,8 @@ struct uaamg_handle {
     double* d_p = nullptr;
     double* d_hist = nullptr;
     double* d_face[3] = {nullptr, nullptr, nullptr};  // face velocities of uaamg_project
+    cudaStream_t copy_stream = nullptr;  // uaamg_solve: p's upload beside the solve
+    cudaEvent_t p_ready = nullptr;
     size_t face_n[3] = {0, 0, 0};
     int hist_cap = 0;
     int last_iters = 0;
