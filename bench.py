@@ -220,6 +220,7 @@ def run_ours(args):
     solid, rhs, dx, dy, dz, metric, workload = _problem(args.workload)
     h = dx
     hd = Handle(device)
+    hd.set_autotune(bool(args.autotune))  # set-up only: chunk lengths timed before the solve
     hd.set_problem(solid, dx, dy, dz)
     opts = hd.options(args.precision, 1e-6, 500, "rel", replace_every=10)
     d_rhs = torch.from_numpy(rhs).to(f"cuda:{device}")
@@ -420,6 +421,7 @@ def run_ours(args):
                    "iterations": stats["iterations"],
                    "true_rel_residual": stats["rel_residual"],
                    "host_checked_rel_residual": res / bn,
+                   "autotune": bool(args.autotune),
                    "l2": f"inputs larger than L2 (solve working set ~{hd.device_bytes() / 1e9:.2f} GB "
                          "vs 126 MB L2)",
                    "parallelism": f"replicas x{ws}"},
@@ -708,7 +710,9 @@ def main():
     ap.add_argument("--no-beside", action="store_true")
     ap.add_argument("--workload", default="spheres_256",
                     choices=["spheres_256", "obstacle_2d", "batch96", "serve10k"])
-    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--autotune", dest="autotune", action="store_true", default=True,
+                    help="time the marches' z-chunk lengths at set-up (default on; outside the timing)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--serve-ids", type=int, default=500)
     ap.add_argument("--serve-steps", type=int, default=20)
     ap.add_argument("--serve-active", type=int, default=16)
