@@ -387,3 +387,21 @@ def test_obstacle2d_against_cpu_reference(handle):
     p = np.zeros_like(rhs)
     s = handle.solve(rhs, p, handle.options("fp32", 1e-6, 300, "rel"))
     assert s.status in (0, 1) and np.isfinite(p).all()
+
+
+@pytest.mark.parametrize("max_iter", [1, 7, 10, 11, 20])
+def test_mixed_stops_at_max_iter_around_replacements(handle, max_iter):
+    """The mixed form stops after exactly max_iter updates (NOT_CONVERGED) whether
+    max_iter falls before, on or after a residual-replacement iteration, and reports
+    the FP64 true residual of the iterate it returns."""
+    from uaamg_b200 import workloads
+    solid, rhs = workloads.spheres_3d(48, 40, 36, nspheres=5, rmin=3, rmax=7, seed=4)
+    h = 1 / 48
+    handle.set_problem(solid, h, h, h)
+    p = np.zeros_like(rhs)
+    st = handle.solve(rhs, p, handle.options("mixed", 1e-14, max_iter, "rel"))
+    assert st.status == 1 and st.iterations == max_iter
+    # no replacement on the last iteration: the exit residual is recomputed anyway
+    assert st.replacements == (max_iter - 1) // 10
+    res, bn = O.true_residual(solid, rhs, p, h, h, h)
+    assert abs(st.rel_residual - res / bn) <= 1e-6 * res / bn
