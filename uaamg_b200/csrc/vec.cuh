@@ -78,31 +78,36 @@ __global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
     const V* pv = reinterpret_cast<const V*>(p);
     const V* av = reinterpret_cast<const V*>(ap);
     double acc[1] = {0.0};
-    // two vectors a thread per trip, their loads issued together
     const long long stride = (long long)gridDim.x * blockDim.x;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    for (; t + stride < nvec; t += 2 * stride) {
-        const long long t2 = t + stride;
-        V xx = xv[t], rr_ = rv[t], x2 = xv[t2], r2 = rv[t2];
-        const V pp = __ldg(&pv[t]), aa = __ldg(&av[t]), p2 = __ldg(&pv[t2]), a2 = __ldg(&av[t2]);
-        if (fold) {
+    if (fold) {  // after a replacement (one iteration in replace_every): one vector a trip
+        for (; t < nvec; t += stride) {
+            V xx = xv[t], rr_ = rv[t];
+            const V pp = __ldg(&pv[t]), aa = __ldg(&av[t]);
             vfold<T>(xx, xhi, t);
-            vfold<T>(x2, xhi, t2);
+            vaxpy_rr<T>(xx, rr_, pp, aa, alpha, acc[0]);
+            xv[t] = xx;
+            rv[t] = rr_;
         }
-        vaxpy_rr<T>(xx, rr_, pp, aa, alpha, acc[0]);
-        vaxpy_rr<T>(x2, r2, p2, a2, alpha, acc[0]);
-        xv[t] = xx;
-        rv[t] = rr_;
-        xv[t2] = x2;
-        rv[t2] = r2;
-    }
-    if (t < nvec) {
-        V xx = xv[t], rr_ = rv[t];
-        const V pp = __ldg(&pv[t]), aa = __ldg(&av[t]);
-        if (fold) vfold<T>(xx, xhi, t);
-        vaxpy_rr<T>(xx, rr_, pp, aa, alpha, acc[0]);
-        xv[t] = xx;
-        rv[t] = rr_;
+    } else {  // two vectors a thread per trip, their loads issued together
+        for (; t + stride < nvec; t += 2 * stride) {
+            const long long t2 = t + stride;
+            V xx = xv[t], rr_ = rv[t], x2 = xv[t2], r2 = rv[t2];
+            const V pp = __ldg(&pv[t]), aa = __ldg(&av[t]), p2 = __ldg(&pv[t2]), a2 = __ldg(&av[t2]);
+            vaxpy_rr<T>(xx, rr_, pp, aa, alpha, acc[0]);
+            vaxpy_rr<T>(x2, r2, p2, a2, alpha, acc[0]);
+            xv[t] = xx;
+            rv[t] = rr_;
+            xv[t2] = x2;
+            rv[t2] = r2;
+        }
+        if (t < nvec) {
+            V xx = xv[t], rr_ = rv[t];
+            const V pp = __ldg(&pv[t]), aa = __ldg(&av[t]);
+            vaxpy_rr<T>(xx, rr_, pp, aa, alpha, acc[0]);
+            xv[t] = xx;
+            rv[t] = rr_;
+        }
     }
     double tot[1];
     if (reduce_last<1>(acc, partials, &cg->counter[1], tot)) {
