@@ -38,7 +38,7 @@ def rel_l2_meanfree(a, b, solid):
 
 @pytest.fixture(params=["march", "sweeps", "march_all"])
 def vkernels(request, handle):
-    """Every V-cycle implementation: z marches with the small-level cluster kernel,
+    """Every V-cycle implementation: z marches with the single-block small-level kernel,
     per-colour sweeps, and z marches on every level."""
     handle.set_vcycle_kernels({"march": 0, "sweeps": 1, "march_all": 2}[request.param])
     yield request.param

@@ -635,7 +635,7 @@ private:
         prof_on_ = false;
         int e = E_OK;
         for (int l = 0; l + 1 < (int)lv_.size() && e == E_OK; ++l) {
-            if (use_tail() && l >= tail_lt_) break;  // the cluster kernel runs those levels
+            if (use_tail() && l >= tail_lt_) break;  // the small-level kernel runs those levels
             LevelBuf<T, CS>& L = lv_[l];
             const auto key = std::make_tuple((int)sizeof(T), mixed_ ? 1 : 0, L.g.nx, L.g.ny, L.g.nz,
                                              l == 0 ? 1 : 0);

@@ -115,7 +115,7 @@ class Handle:
         self._check(self.lib.uaamg_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
 
     def set_vcycle_kernels(self, mode):
-        """0 / False: z marches + the small-level cluster kernel (default);
+        """0 / False: z marches + the single-block small-level kernel (default);
         1 / True: per-colour sweep kernels; 2: z marches on every level."""
         self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(mode)), "vcycle")
 
