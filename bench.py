@@ -447,22 +447,36 @@ def _oracle():
     return O
 
 
+def _init_group(ws, local):
+    """One process per GPU: the NCCL group used only for the end-of-run scalars."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+
 def run_batch(args):
     """96 uneven 2D/3D problems solved as one uaamg_solve_batch call (host arrays in
-    and out; a step = the whole batch).  Beside: the same problems one uaamg_solve
-    at a time, and the batch in plain FP32."""
+    and out; a step = the whole batch).  With N GPUs each rank solves its round-robin
+    share of the 96 (uaamg_b200.shard) and the step time is the slowest rank's.
+    Beside (one GPU): the same problems one uaamg_solve at a time, and the batch in
+    plain FP32."""
     import numpy as np
     import torch
 
-    from uaamg_b200 import workloads
+    from uaamg_b200 import shard, workloads
     from uaamg_b200.solver import Handle
 
-    ws, rank, _ = _dist()
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(0)
-    probs = workloads.batch96()
-    hd = Handle(0)
+    ws, rank, local = _dist()
+    device = local if ws > 1 else 0
+    if ws > 1:
+        _init_group(ws, local)
+    torch.cuda.set_device(device)
+    probs_all = workloads.batch96()
+    probs = shard.shard(probs_all, rank, ws)
+    hd = Handle(device)
     if args.autotune:
         hd.set_autotune(True)
     opts = hd.options(args.precision, 1e-6, 500, "rel")
@@ -480,17 +494,38 @@ def run_batch(args):
 
     for _ in range(args.warmup):
         step(opts)
-    with ClockSampler(0) as clk:
+    with ClockSampler(device) as clk:
         times = []
         for _ in range(args.steps):
             t, stats = step(opts)
             times.append(t)
     clocks = clk.summary()
-    ms = statistics.mean(times)
+    ms = shard.reduce_max(statistics.mean(times))
     O = _oracle()
     rel = [O.true_residual(s, r, p, dx, dy, dz) for (s, r, dx, dy, dz), p in zip(probs, ps)]
-    worst = max(a / b for a, b in rel)
-    iters = [st.iterations for st in stats]
+    worst = shard.reduce_max(max(a / b for a, b in rel))
+    iters = shard.gather([st.iterations for st in stats])
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        hd.close()
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
+        line = {
+            "metric": "96-problem uneven batch solve ms (1e-6 rel. residual)", "value": round(ms, 3),
+            "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 reductions and solution)", "data": "synthetic",
+            "config": {"workload": "batch96 sharded round-robin over the GPUs (one process each)",
+                       "precision": args.precision, "solves_per_s": round(96 / (ms * 1e-3), 1),
+                       "iterations_min_median_max": [min(iters), int(np.median(iters)), max(iters)],
+                       "worst_true_rel_residual": worst,
+                       "timing": "slowest rank's host clock around its blocking batch call"},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+        return 0
     # beside: one problem at a time through uaamg_solve, and plain FP32 batched
     seq = 0.0
     for (s, r, dx, dy, dz), p in zip(probs, ps):
@@ -615,36 +650,40 @@ def _serve_pass(srv, reqs, make, rate=None, max_outstanding=256, check=()):
 
 def run_serve(args):
     """10,000 served requests (500 simulation ids x 20 steps): closed-loop capacity,
-    then open-loop Poisson arrivals at 80 % of it; p50/p99 latency, solves/s."""
+    then open-loop Poisson arrivals at 80 % of it; p50/p99 latency, solves/s.  With N
+    GPUs each rank serves the simulation ids it owns (uaamg_b200.shard.owns) on its own
+    GPU; rates are summed over the ranks and latencies pooled."""
     import concurrent.futures as cf
 
     import numpy as np
     import torch
 
-    from uaamg_b200 import workloads
+    from uaamg_b200 import shard, workloads
     from uaamg_b200.solver import Server
 
-    ws, rank, _ = _dist()
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(0)
+    ws, rank, local = _dist()
+    device = local if ws > 1 else 0
+    if ws > 1:
+        _init_group(ws, local)
+    torch.cuda.set_device(device)
     n_ids, steps = args.serve_ids, args.serve_steps
     plan = workloads.serve_plan(n_ids, steps)
+    mine = [sid for sid in range(n_ids) if shard.owns(sid, rank, ws)]
     with cf.ThreadPoolExecutor(8) as ex:
-        fields = list(ex.map(lambda q: workloads.serve_fields(q[1], q[2], q[3]), plan))
+        fields = dict(zip(mine, ex.map(lambda sid: workloads.serve_fields(*plan[sid][1:4]), mine)))
 
     def make(sid, t):
         solid, r0, r1 = fields[sid]
         return solid, r0 + (t / steps) * r1, 1.0 / plan[sid][2]
 
-    reqs = [(sid, t) for t in range(steps) for sid in range(n_ids)]
-    rng = np.random.Generator(np.random.MT19937(7))
-    check = set(int(i) for i in rng.choice(len(reqs), 24, replace=False))
+    reqs = [(sid, t) for t in range(steps) for sid in mine]
+    rng = np.random.Generator(np.random.MT19937(7 + rank))
+    check = set(int(i) for i in rng.choice(len(reqs), max(1, 24 // ws), replace=False))
     O = _oracle()
 
-    def summary(res, wall):
+    def summary(res, rate):
         lat = np.array([r["total_ms"] for r in res])
-        return {"solves_per_s": round(len(res) / wall, 1),
+        return {"solves_per_s": round(rate, 1),
                 "p50_ms": round(float(np.percentile(lat, 50)), 3),
                 "p99_ms": round(float(np.percentile(lat, 99)), 3),
                 "mean_iterations": round(float(np.mean([r["iterations"] for r in res])), 2),
@@ -654,40 +693,47 @@ def run_serve(args):
 
     out = {}
     for prec in ([args.precision, "fp32"] if not args.no_beside else [args.precision]):
-        srv = Server(0, prec, 1e-6, 500, max_active=args.serve_active)
+        srv = Server(device, prec, 1e-6, 500, max_active=args.serve_active)
         # warm-up: every id's hierarchy and graph, not timed
-        _serve_pass(srv, [(sid, 0) for sid in range(n_ids)], make)
+        _serve_pass(srv, [(sid, 0) for sid in mine], make)
         closed, wall_c, _ = _serve_pass(srv, reqs, make)
-        cap = len(reqs) / wall_c
-        entry = {"closed_loop": summary(closed, wall_c)}
+        cap = len(reqs) / wall_c  # this rank's capacity
+        entry = {"closed_loop": summary(shard.gather(closed), shard.reduce_sum(cap))}
         if prec == args.precision:
             srv.stop()
-            srv = Server(0, prec, 1e-6, 500, max_active=args.serve_active)
-            _serve_pass(srv, [(sid, 0) for sid in range(n_ids)], make)
-            with ClockSampler(0) as clk:
+            srv = Server(device, prec, 1e-6, 500, max_active=args.serve_active)
+            _serve_pass(srv, [(sid, 0) for sid in mine], make)
+            with ClockSampler(device) as clk:
                 opened, wall_o, kept = _serve_pass(srv, reqs, make, rate=0.8 * cap, check=check)
-            entry["open_loop"] = summary(opened, wall_o)
-            entry["open_loop"]["arrival_rate_per_s"] = round(0.8 * cap, 1)
+            entry["open_loop"] = summary(shard.gather(opened), shard.reduce_sum(len(reqs) / wall_o))
+            entry["open_loop"]["arrival_rate_per_s"] = round(shard.reduce_sum(0.8 * cap), 1)
             entry["clocks"] = clk.summary()
             entry["info"] = srv.info()
             worst = 0.0
             for i, (p, solid, rhs, h) in kept.items():
                 a, b = O.true_residual(solid, rhs, p, h, h, h if solid.ndim == 3 else 1.0)
                 worst = max(worst, a / b)
-            entry["checked_true_rel_residual_max"] = worst
-            entry["checked_requests"] = len(kept)
+            entry["checked_true_rel_residual_max"] = shard.reduce_max(worst)
+            entry["checked_requests"] = int(shard.reduce_sum(len(kept)))
         srv.stop()
         out[prec] = entry
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
     main_ = out[args.precision]
     line = {
         "metric": "served pressure solves/s and p99 latency (1e-6 rel. residual)",
-        "value": main_["open_loop"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "value": main_["open_loop"]["solves_per_s"], "unit": "solves/s", "n_gpus": ws,
         "steps": len(reqs), "warmup": n_ids, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP64 reductions and solution)", "data": "synthetic",
         "config": {"workload": f"serve10k: {n_ids} simulation ids x {steps} steps, 70% 2D n^2 "
                                "(n lognormal median 384, [64, 2048]), 30% 3D n^3 (median 96, "
                                "[32, 256]), obstacle disk/sphere, evolving RHS (seed 20260505)",
-                   "precision": args.precision, "max_active": args.serve_active,
+                   "precision": args.precision, "max_active_per_gpu": args.serve_active,
+                   "sharding": "simulation ids round-robin over the GPUs (one process each)",
                    "hbm_budget_gb": 150, "warm_start": True,
                    "p50_ms": main_["open_loop"]["p50_ms"], "p99_ms": main_["open_loop"]["p99_ms"],
                    "latency": "scheduled arrival -> result on the host"},
