@@ -43,15 +43,24 @@ WORKLOAD_2D = ("obstacle_2d: 2048x1024 MAC grid, dx=1e-3, dy=1.5e-3, Neumann wal
                "radius 0.05*Ly at (0.25 Lx, 0.5 Ly), RHS = div(u)/dt of u = 1 + Fourier modes "
                "|k|<=16 with N(0,1)/|k|^2 amplitudes, dt=1e-3 (seed 20260202)")
 
+METRIC_VAR = "2D 2048x1024 variable-coefficient PCG solve ms (1e-6 rel. residual)"
+WORKLOAD_VAR = ("layered_2d: the obstacle_2d grid, mask and RHS with the variable-coefficient "
+                "Laplacian (lap_diag/lap_off_x/lap_off_y) of a layered medium, x conductivity "
+                "1+0.5 sin(2 pi y/Ly), y conductivity 1+0.5 cos(2 pi x/Lx)")
+
 
 def _problem(name):
-    """(solid, rhs, dx, dy, dz, metric, workload) of a single-solve workload."""
+    """(solid, rhs, dx, dy, dz, metric, workload, lap) of a single-solve workload;
+    lap = (lap_diag, lap_off_x, lap_off_y) or None for the uniform operator."""
     from uaamg_b200 import workloads
     if name == "obstacle_2d":
         solid, _, _, rhs, dx, dy, _ = workloads.obstacle_2d()
-        return solid, rhs, dx, dy, 1.0, METRIC_2D, WORKLOAD_2D
+        return solid, rhs, dx, dy, 1.0, METRIC_2D, WORKLOAD_2D, None
+    if name == "layered_2d":
+        solid, rhs, dx, dy, lap = workloads.layered_2d()
+        return solid, rhs, dx, dy, 1.0, METRIC_VAR, WORKLOAD_VAR, lap
     solid, rhs, h = workloads.spheres_256()
-    return solid, rhs, h, h, h, METRIC, WORKLOAD
+    return solid, rhs, h, h, h, METRIC, WORKLOAD, None
 
 
 def _peaks():
@@ -182,7 +191,7 @@ def run_reference(args):
     return 0
 
 
-def cpu_baseline_sample(solid, rhs, h, n_it, dx=None, dy=None, dz=None):
+def cpu_baseline_sample(solid, rhs, h, n_it, dx=None, dy=None, dz=None, lap=None):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
@@ -190,7 +199,11 @@ def cpu_baseline_sample(solid, rhs, h, n_it, dx=None, dy=None, dz=None):
     b = O.pcg_rhs(solid, rhs)
     tol_abs = 1e-6 * float((b[solid == 0] ** 2).sum()) ** 0.5
     t0 = time.perf_counter()
-    if kind == "reference":
+    if lap is not None and kind == "reference":
+        O.ref_pcg_var(solid, lap, rhs, dx, dy, max_iter=1, tol=tol_abs)
+    elif lap is not None:
+        O.pcg_var(solid, lap, rhs, dx, dy, max_iter=1, tol=tol_abs, tol_mode=0)
+    elif kind == "reference":
         O.ref_pcg(solid, rhs, dx or h, dy or h, dz or h, max_iter=1, tol=tol_abs)
     else:
         O.pcg(solid, rhs, dx or h, dy or h, dz or h, max_iter=1, tol=tol_abs, tol_mode=0)
@@ -217,11 +230,13 @@ def run_ours(args):
     from uaamg_b200 import _capi, workloads
     from uaamg_b200.solver import Handle
 
-    solid, rhs, dx, dy, dz, metric, workload = _problem(args.workload)
+    solid, rhs, dx, dy, dz, metric, workload, lap = _problem(args.workload)
     h = dx
     hd = Handle(device)
     hd.set_autotune(bool(args.autotune))  # set-up only: chunk lengths timed before the solve
     hd.set_problem(solid, dx, dy, dz)
+    if lap is not None:
+        hd.set_variable_laplacian(*lap)
     opts = hd.options(args.precision, 1e-6, 500, "rel", replace_every=10)
     d_rhs = torch.from_numpy(rhs).to(f"cuda:{device}")
     d_p = torch.zeros_like(d_rhs)
@@ -289,7 +304,10 @@ def run_ours(args):
     # true residual of the e2e result, recomputed in FP64 on the host (oracle)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    res, bn = O.true_residual(solid, rhs, p_np, dx, dy, dz)
+    if lap is not None:
+        res, bn = O.true_residual_var(solid, lap, rhs, p_np)
+    else:
+        res, bn = O.true_residual(solid, rhs, p_np, dx, dy, dz)
 
     # in-situ per-kernel timing (one extra, unmeasured solve)
     d_p.zero_()
@@ -403,7 +421,7 @@ def run_ours(args):
             n_it = _ref_iterations()["iterations"]
         else:  # the FP64 GPU path runs the reference's iteration sequence
             n_it = beside.get("fp64", {}).get("iterations", stats["iterations"])
-        cpu = cpu_baseline_sample(solid, rhs, h, n_it, dx, dy, dz)
+        cpu = cpu_baseline_sample(solid, rhs, h, n_it, dx, dy, dz, lap)
 
     if ws > 1:
         import torch.distributed as dist
@@ -755,7 +773,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-beside", action="store_true")
     ap.add_argument("--workload", default="spheres_256",
-                    choices=["spheres_256", "obstacle_2d", "batch96", "serve10k"])
+                    choices=["spheres_256", "obstacle_2d", "layered_2d", "batch96", "serve10k"])
     ap.add_argument("--autotune", dest="autotune", action="store_true", default=True,
                     help="time the marches' z-chunk lengths at set-up (default on; outside the timing)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")

@@ -114,6 +114,21 @@ UAAMG_API uaamg_status uaamg_set_problem_3d(uaamg_handle* h, int nx, int ny, int
 UAAMG_API uaamg_status uaamg_set_problem_device(uaamg_handle* h, int dim, int nx, int ny, int nz,
                                       double dx, double dy, double dz,
                                       const uint8_t* d_solid);
+/* Variable-coefficient Laplacian for the outer CG, 2D (Grid::init_variable_lap and
+ * Grid::lap_diag / lap_off_x / lap_off_y, include/core/grid.h:23-31,
+ * src/core/grid.cpp:12-17, as PCG::solve applies them, src/solver/pcg.cpp:35-46):
+ * padded (nx+2)(ny+2) FP64 HOST arrays, copied to the device.  Every later solve of
+ * the current problem (uaamg_solve*, uaamg_project*, uaamg_static_pressure*) uses
+ *   A v = lap_diag v_C + lap_off_x (v_L + v_R) + lap_off_y (v_B + v_T)
+ * on fluid cells (a solid or out-of-domain neighbour reads v_C; solid rows 0) for its
+ * search directions and FP64 residuals; the UAAMG V-cycle keeps its uniform
+ * couplings, as the reference's does.  All three NULL: back to the uniform
+ * operator.  UAAMG_INVALID_ARG for a 3D problem (Grid3D has no such arrays) or when
+ * only some are NULL; UAAMG_NO_PROBLEM before uaamg_set_problem_*, which clears the
+ * coefficients. */
+UAAMG_API uaamg_status uaamg_set_variable_laplacian(uaamg_handle* h, const double* lap_diag,
+                                          const double* lap_off_x,
+                                          const double* lap_off_y);
 /* Cell-centred Dirichlet p = 0 on every domain wall instead of Neumann (the
  * standalone Ax=b check of test/solver/test_amgpcg.cpp:29-70, on the MAC grid).
  * Takes effect at the next uaamg_set_problem_*. */

@@ -72,6 +72,14 @@ def lib():
         L.oracle_divergence_rhs.argtypes = [_i, _i, _i, _i, _d, _d, _d, _p, _p, _p, _p, _d,
                                             _p]
         L.oracle_static_rhs_2d.argtypes = [_i, _i, _d, _d, _p, _p, _p, _p]
+        L.oracle_pcg_var_2d.restype = _i
+        L.oracle_pcg_var_2d.argtypes = [_i, _i, _d, _d, _p, _p, _p, _p, _p, _p, _i, _d, _i, _i,
+                                        _i, _p, C.POINTER(_i)]
+        L.oracle_matvec_var_2d.argtypes = [_i, _i, _p, _p, _p, _p, _p, _p]
+        L.oracle_true_residual_var_2d.restype = _d
+        L.oracle_true_residual_var_2d.argtypes = [_i, _i, _p, _p, _p, _p, _p, _p, C.POINTER(_d)]
+        L.oracle_smooth_cylinder_2d.argtypes = [_i, _i, _d, _d, _d, _d, _d, _d, _i, _p, _p, _p,
+                                                _p]
     return _lib
 
 
@@ -96,6 +104,9 @@ def ref():
         R.ref_project_2d.restype = _i
         R.ref_project_2d.argtypes = [_i, _i, _d, _d, _p, _p, _p, _d, _i, _d, _p]
         R.ref_static_rhs_2d.argtypes = [_i, _i, _d, _d, _p, _p, _p, _p]
+        R.ref_pcg_var_2d.restype = _i
+        R.ref_pcg_var_2d.argtypes = [_i, _i, _d, _d, _p, _p, _p, _p, _p, _p, _i, _d, _i]
+        R.ref_smooth_cylinder_2d.argtypes = [_i, _i, _d, _d, _d, _d, _d, _d, _p, _p, _p, _p]
         R.ref_project_3d.restype = _i
         R.ref_project_3d.argtypes = [_i, _i, _i, _d, _d, _d, _p, _p, _p, _p, _d, _i, _d, _p]
     return _ref
@@ -235,7 +246,79 @@ def correct_velocity(solid, p, dt, u, v, w, dx, dy, dz=1.0):
     return u, v, w
 
 
+def pcg_var(solid, lap, rhs, dx, dy, max_iter=200, tol=1e-6, precond=True, tol_mode=1,
+            x0=None, warm=False):
+    """Restated 2D PCG with the variable-coefficient operator (pcg.cpp:35-46);
+    lap = (lap_diag, lap_off_x, lap_off_y), padded.  Returns (x, updates, status)."""
+    solid = _c8(solid)
+    _, nx, ny, _ = _dims(solid.shape)
+    ld, lx, ly = (_cd(a) for a in lap)
+    rhs = _cd(rhs)
+    x = np.zeros_like(rhs) if x0 is None else _cd(x0).copy()
+    st = _i()
+    n = lib().oracle_pcg_var_2d(nx, ny, dx, dy, _ptr(solid), _ptr(ld), _ptr(lx), _ptr(ly),
+                                _ptr(rhs), _ptr(x), max_iter, tol, int(precond), tol_mode,
+                                int(warm), None, C.byref(st))
+    return x, n, st.value
+
+
+def matvec_var(solid, lap, x):
+    solid = _c8(solid)
+    _, nx, ny, _ = _dims(solid.shape)
+    ld, lx, ly = (_cd(a) for a in lap)
+    x = _cd(x)
+    ax = np.zeros_like(x)
+    lib().oracle_matvec_var_2d(nx, ny, _ptr(solid), _ptr(ld), _ptr(lx), _ptr(ly), _ptr(x),
+                               _ptr(ax))
+    return ax
+
+
+def true_residual_var(solid, lap, rhs, x):
+    """(||b - A x||, ||b||) with the variable-coefficient operator, FP64."""
+    solid = _c8(solid)
+    _, nx, ny, _ = _dims(solid.shape)
+    ld, lx, ly = (_cd(a) for a in lap)
+    bn = _d()
+    r = lib().oracle_true_residual_var_2d(nx, ny, _ptr(solid), _ptr(ld), _ptr(lx), _ptr(ly),
+                                          _ptr(_cd(rhs)), _ptr(_cd(x)), C.byref(bn))
+    return r, bn.value
+
+
+def smooth_cylinder(solid, dx, dy, cx, cy, r, tw=0.0, inside=False):
+    """Restated SmoothCylinder::applyToLaplacian: (solid', (diag, off_x, off_y))."""
+    solid = _c8(solid).copy()
+    _, nx, ny, _ = _dims(solid.shape)
+    lap = tuple(np.zeros(solid.shape) for _ in range(3))
+    lib().oracle_smooth_cylinder_2d(nx, ny, dx, dy, cx, cy, r, tw, int(inside), _ptr(solid),
+                                    *(_ptr(a) for a in lap))
+    return solid, lap
+
+
 # --- the reference itself (compiled from its own sources) -------------------
+
+
+def ref_pcg_var(solid, lap, rhs, dx, dy, max_iter=200, tol=1e-6, precond=True):
+    """The reference's PCG::solve on a grid with init_variable_lap() and the given
+    coefficients.  Returns (p, preconditioner applications)."""
+    solid = _c8(solid)
+    _, nx, ny, _ = _dims(solid.shape)
+    ld, lx, ly = (_cd(a) for a in lap)
+    rhs = _cd(rhs)
+    p = np.zeros_like(rhs)
+    n = ref().ref_pcg_var_2d(nx, ny, dx, dy, _ptr(solid), _ptr(ld), _ptr(lx), _ptr(ly),
+                             _ptr(rhs), _ptr(p), max_iter, tol, int(precond))
+    return p, n
+
+
+def ref_smooth_cylinder(solid, dx, dy, cx, cy, r, tw=0.0):
+    """SmoothCylinder(cx, cy, r, dx, dy, tw).applyToLaplacian as the reference
+    runs it: (solid', (diag, off_x, off_y))."""
+    solid = _c8(solid).copy()
+    _, nx, ny, _ = _dims(solid.shape)
+    lap = tuple(np.zeros(solid.shape) for _ in range(3))
+    ref().ref_smooth_cylinder_2d(nx, ny, dx, dy, cx, cy, r, tw, _ptr(solid),
+                                 *(_ptr(a) for a in lap))
+    return solid, lap
 
 
 def ref_vcycle(solid, r, dx, dy, dz=1.0):

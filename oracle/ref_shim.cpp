@@ -10,6 +10,8 @@
 //   IdentityPreconditioner[3D]     include/solver/preconditioner/identity_preconditioner*.h
 //   PressureProjection[3D]         src/pressure/pressure.cpp:5-33, src/pressure/pressure_3d.cpp:5-40
 //   Grid / Grid3D                  include/core/grid.h:16-48, include/core/grid_3d.h:14-38
+//   Grid::init_variable_lap        src/core/grid.cpp:12-17 (PCG::solve's lap_* branch)
+//   SmoothCylinder                 src/geometry/cylinder_model.cpp:40-71
 #include "core/grid.h"
 #include "core/grid_3d.h"
 #include "solver/pcg.h"
@@ -20,6 +22,7 @@
 #include "solver/preconditioner/identity_preconditioner_3d.h"
 #include "pressure/pressure.h"
 #include "pressure/pressure_3d.h"
+#include "geometry/cylinder_model.h"
 
 #include <cstdint>
 #include <cstring>
@@ -114,6 +117,46 @@ int ref_pcg_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
     solver.solve(g, rv, max_iter, tol);
     std::memcpy(p, g.p.data(), sizeof(double) * n);
     return applies;
+}
+
+// PCG(UAAMG) or PCG(Identity) on a grid whose variable-coefficient Laplacian is set
+// (Grid::init_variable_lap, then the caller's padded lap_diag / lap_off_x / lap_off_y),
+// so that PCG::solve takes its pcg.cpp:35-46 branch.
+int ref_pcg_var_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+                   const double* lap_diag, const double* lap_off_x, const double* lap_off_y,
+                   const double* rhs, double* p, int max_iter, double tol, int precond) {
+    Grid g = make2(nx, ny, dx, dy, solid);
+    const int n = g.p_size();
+    g.init_variable_lap();
+    std::memcpy(g.lap_diag.data(), lap_diag, sizeof(double) * n);
+    std::memcpy(g.lap_off_x.data(), lap_off_x, sizeof(double) * n);
+    std::memcpy(g.lap_off_y.data(), lap_off_y, sizeof(double) * n);
+    std::memcpy(g.p.data(), p, sizeof(double) * n);
+    int applies = 0;
+    std::unique_ptr<Preconditioner> inner;
+    if (precond) inner = std::make_unique<UAAMGPreconditioner>();
+    else         inner = std::make_unique<IdentityPreconditioner>();
+    PCG solver(std::make_unique<Counting<Preconditioner, Grid>>(std::move(inner), &applies));
+    std::vector<double> rv(rhs, rhs + n);
+    solver.solve(g, rv, max_iter, tol);
+    std::memcpy(p, g.p.data(), sizeof(double) * n);
+    return applies;
+}
+
+// SmoothCylinder(cx, cy, R, dx, dy, tw)::applyToLaplacian on a grid with the given
+// mask: solid (in/out, OR-ed by the model) and the three padded coefficient arrays
+// (out; zero where the model leaves them).
+void ref_smooth_cylinder_2d(int nx, int ny, double dx, double dy, double cx, double cy, double R,
+                            double tw, uint8_t* solid, double* diag, double* ox, double* oy) {
+    Grid g = make2(nx, ny, dx, dy, solid);
+    const int n = g.p_size();
+    g.init_variable_lap();
+    SmoothCylinder cyl(cx, cy, R, dx, dy, tw);
+    cyl.applyToLaplacian(g, g.lap_diag, g.lap_off_x, g.lap_off_y);
+    for (int c = 0; c < n; ++c) solid[c] = g.solid[c] ? 1 : 0;
+    std::memcpy(diag, g.lap_diag.data(), sizeof(double) * n);
+    std::memcpy(ox, g.lap_off_x.data(), sizeof(double) * n);
+    std::memcpy(oy, g.lap_off_y.data(), sizeof(double) * n);
 }
 
 int ref_pcg_3d(int nx, int ny, int nz, double dx, double dy, double dz, const uint8_t* solid,

@@ -328,6 +328,8 @@ void oh_vcycle(oh_hier* h, const double* r, double* z) {
 typedef struct {
     olevel g;               /* geometry + mask only (p/b/coeff arrays unused) */
     int dirichlet;
+    /* 2D variable-coefficient operator (Grid::lap_*, grid.h:23-31), or NULL */
+    const double *ld, *lox, *loy;
 } ogrid;
 
 static void grid_init(ogrid* G, int dim, int nx, int ny, int nz, double dx, double dy, double dz,
@@ -342,7 +344,8 @@ static void grid_init(ogrid* G, int dim, int nx, int ny, int nz, double dx, doub
     G->dirichlet = dirichlet;
 }
 
-/* pcg_3d.cpp:38-55 / pcg.cpp:47-59 (uniform-coefficient branch) */
+/* pcg_3d.cpp:38-55 / pcg.cpp:47-59 (uniform-coefficient branch); pcg.cpp:35-46
+ * (variable-coefficient branch, 2D: d v_C + ox (v_L + v_R) + oy (v_B + v_T)) */
 static void pcg_matvec(const ogrid* G, const double* v, double* av) {
     const olevel* L = &G->g;
     const double idx2 = 1.0 / (L->dx * L->dx), idy2 = 1.0 / (L->dy * L->dy);
@@ -364,6 +367,8 @@ static void pcg_matvec(const ogrid* G, const double* v, double* av) {
                     double vF = k > 1 ? (!L->solid[cid(L, i, j, k - 1)] ? v[cid(L, i, j, k - 1)] : vc) : wall;
                     double vK = k < nz ? (!L->solid[cid(L, i, j, k + 1)] ? v[cid(L, i, j, k + 1)] : vc) : wall;
                     av[id] = diag * vc - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
+                } else if (G->ld) {
+                    av[id] = G->ld[id] * vc + G->lox[id] * (vL + vR) + G->loy[id] * (vB + vT);
                 } else {
                     av[id] = diag * vc - (vL + vR) * idx2 - (vB + vT) * idy2;
                 }
@@ -457,12 +462,14 @@ double oracle_true_residual(int dim, int nx, int ny, int nz, double dx, double d
     return sqrt(rr);
 }
 
-int oracle_pcg(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
-               const uint8_t* solid, const double* rhs_in, double* x, int max_iter,
-               double tol, int precond, int tol_mode, int warm, int dirichlet,
-               double* hist, int* status) {
+static int pcg_impl(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
+                    const uint8_t* solid, const double* ld, const double* lox,
+                    const double* loy, const double* rhs_in, double* x, int max_iter,
+                    double tol, int precond, int tol_mode, int warm, int dirichlet,
+                    double* hist, int* status) {
     ogrid G;
     grid_init(&G, dim, nx, ny, nz, dx, dy, dz, solid, dirichlet);
+    G.ld = ld; G.lox = lox; G.loy = loy;
     const size_t n = (size_t)G.g.n;
     double* r = (double*)calloc(n, sizeof(double));
     double* z = (double*)calloc(n, sizeof(double));
@@ -528,6 +535,100 @@ int oracle_pcg(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
     oh_destroy(h);
     free(r); free(z); free(p); free(ap);
     return updates;
+}
+
+int oracle_pcg(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
+               const uint8_t* solid, const double* rhs_in, double* x, int max_iter,
+               double tol, int precond, int tol_mode, int warm, int dirichlet,
+               double* hist, int* status) {
+    return pcg_impl(dim, nx, ny, nz, dx, dy, dz, solid, NULL, NULL, NULL, rhs_in, x, max_iter,
+                    tol, precond, tol_mode, warm, dirichlet, hist, status);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Variable-coefficient Laplacian (Grid::lap_*, pcg.cpp:35-46), 2D            */
+
+int oracle_pcg_var_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+                      const double* lap_diag, const double* lap_off_x, const double* lap_off_y,
+                      const double* rhs_in, double* x, int max_iter, double tol, int precond,
+                      int tol_mode, int warm, double* hist, int* status) {
+    return pcg_impl(2, nx, ny, 0, dx, dy, 1.0, solid, lap_diag, lap_off_x, lap_off_y, rhs_in, x,
+                    max_iter, tol, precond, tol_mode, warm, 0, hist, status);
+}
+
+void oracle_matvec_var_2d(int nx, int ny, const uint8_t* solid, const double* lap_diag,
+                          const double* lap_off_x, const double* lap_off_y, const double* x,
+                          double* ax) {
+    ogrid G;
+    grid_init(&G, 2, nx, ny, 0, 1.0, 1.0, 1.0, solid, 0);
+    G.ld = lap_diag; G.lox = lap_off_x; G.loy = lap_off_y;
+    memset(ax, 0, sizeof(double) * (size_t)G.g.n);
+    pcg_matvec(&G, x, ax);
+}
+
+double oracle_true_residual_var_2d(int nx, int ny, const uint8_t* solid, const double* lap_diag,
+                                   const double* lap_off_x, const double* lap_off_y,
+                                   const double* rhs, const double* x, double* bnorm) {
+    ogrid G;
+    grid_init(&G, 2, nx, ny, 0, 1.0, 1.0, 1.0, solid, 0);
+    G.ld = lap_diag; G.lox = lap_off_x; G.loy = lap_off_y;
+    size_t n = (size_t)G.g.n;
+    double* b = (double*)calloc(n, sizeof(double));
+    double* ax = (double*)calloc(n, sizeof(double));
+    pcg_prepare_rhs(&G, rhs, b);
+    pcg_matvec(&G, x, ax);
+    for (size_t c = 0; c < n; c++) ax[c] = b[c] - ax[c];
+    double rr = pcg_dot(&G, ax, ax);
+    if (bnorm) *bnorm = sqrt(pcg_dot(&G, b, b));
+    free(b); free(ax);
+    return sqrt(rr);
+}
+
+/* SmoothCylinder::applyToLaplacian (cylinder_model.cpp:5-10, 40-48, 50-71): solid
+ * fraction phi = smoothstep((r - R) / tw) of the cell centre; phi > 0.9 marks the
+ * cell solid (diag 1e15, no couplings); otherwise face permeabilities
+ * c = 1 - (phi + phi_nb)/2 + 0.1 give diag = (cL + cR)/dx^2 + (cB + cT)/dy^2 and
+ * off_x = -(cL + cR)/(2 dx^2), off_y = -(cB + cT)/(2 dy^2).  inside != 0 flips the
+ * fraction to smoothstep((R - r) / tw), solid inside the disk.  Interior cells
+ * only; solid is OR-ed, the ghost coefficients are left as they are. */
+static double oc_smoothstep(double t) {
+    if (t <= -1.0) return 0.0;
+    if (t >= 1.0) return 1.0;
+    double s = (t + 1.0) * 0.5;
+    return s * s * (3.0 - 2.0 * s);
+}
+
+static double oc_frac(double cx, double cy, double R, double tw, int inside, double x, double y) {
+    double r = sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy));
+    return oc_smoothstep(inside ? (R - r) / tw : (r - R) / tw);
+}
+
+void oracle_smooth_cylinder_2d(int nx, int ny, double dx, double dy, double cx, double cy,
+                               double R, double tw, int inside, uint8_t* solid, double* diag,
+                               double* ox, double* oy) {
+    const double eps = 0.1, large = 1e15;
+    if (!(tw > 0)) tw = dx;
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            long idx = i + (long)j * (nx + 2);
+            double xc = (i - 0.5) * dx, yc = (j - 0.5) * dy;
+            double phi = oc_frac(cx, cy, R, tw, inside, xc, yc);
+            if (phi > 0.9) {
+                solid[idx] = 1;
+                diag[idx] = large; ox[idx] = 0; oy[idx] = 0;
+            } else {
+                double pL = oc_frac(cx, cy, R, tw, inside, xc - dx, yc);
+                double pR = oc_frac(cx, cy, R, tw, inside, xc + dx, yc);
+                double pB = oc_frac(cx, cy, R, tw, inside, xc, yc - dy);
+                double pT = oc_frac(cx, cy, R, tw, inside, xc, yc + dy);
+                double cL = 1.0 - 0.5 * (phi + pL) + eps, cR = 1.0 - 0.5 * (phi + pR) + eps;
+                double cB = 1.0 - 0.5 * (phi + pB) + eps, cT = 1.0 - 0.5 * (phi + pT) + eps;
+                double ix = 1.0 / (dx * dx), iy = 1.0 / (dy * dy);
+                diag[idx] = (cL + cR) * ix + (cB + cT) * iy;
+                ox[idx] = -0.5 * (cL + cR) * ix;
+                oy[idx] = -0.5 * (cB + cT) * iy;
+            }
+        }
 }
 
 /* ------------------------------------------------------------------------- */

@@ -73,6 +73,25 @@ void oracle_divergence_rhs(int dim, int nx, int ny, int nz, double dx, double dy
                            const uint8_t* solid, const double* u, const double* v,
                            const double* w, double dt, double* rhs);
 
+/* Variable-coefficient Laplacian of PCG::solve (pcg.cpp:35-46; Grid::lap_diag,
+ * lap_off_x, lap_off_y, grid.h:23-31), 2D, padded arrays: the PCG of oracle_pcg
+ * with that operator (Neumann walls), A x, and ||b - A x|| (with ||b|| in *bnorm). */
+int oracle_pcg_var_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
+                      const double* lap_diag, const double* lap_off_x, const double* lap_off_y,
+                      const double* rhs, double* x, int max_iter, double tol, int precond,
+                      int tol_mode, int warm, double* hist, int* status);
+void oracle_matvec_var_2d(int nx, int ny, const uint8_t* solid, const double* lap_diag,
+                          const double* lap_off_x, const double* lap_off_y, const double* x,
+                          double* ax);
+double oracle_true_residual_var_2d(int nx, int ny, const uint8_t* solid, const double* lap_diag,
+                                   const double* lap_off_x, const double* lap_off_y,
+                                   const double* rhs, const double* x, double* bnorm);
+/* SmoothCylinder::applyToLaplacian (cylinder_model.cpp:50-71) on padded arrays;
+ * inside != 0: solid fraction 1 inside the disk instead of outside. */
+void oracle_smooth_cylinder_2d(int nx, int ny, double dx, double dy, double cx, double cy,
+                               double R, double tw, int inside, uint8_t* solid, double* diag,
+                               double* ox, double* oy);
+
 /* RHS of PressureProjection::recoverStaticPressure (pressure.cpp:35-66), 2D. */
 void oracle_static_rhs_2d(int nx, int ny, double dx, double dy, const uint8_t* solid,
                           const double* u, const double* v, double* rhs);

@@ -11,7 +11,12 @@ parity tests:
   vcycle_2d_cylinder  src/solver/cuda/test_cuda_uaamg.cu:134-185 (64x16, Lx = 4, R = 0.1)
   vcycle_3d_uniform   src/solver/cuda/test_cuda_uaamg_3d.cu:15-58 (16x8x4)
   pcg_3d_gauss        src/solver/cuda/test_cuda_uaamg_3d.cu:60-96 (30 it, tol 1e-10)
-plus random-solid / odd-size / anisotropic cases and a 2D and 3D projection.
+plus random-solid / odd-size / anisotropic cases and a 2D and 3D projection, and the
+variable-coefficient branch of PCG::solve (pcg.cpp:35-46, Grid::init_variable_lap):
+
+  varlap_2d_smooth_cylinder  the coefficients of the reference's own
+                             SmoothCylinder::applyToLaplacian (cylinder_model.cpp:50-71)
+  varlap_2d_layered          a layered medium (layered_lap below)
 
 Run from the repository root after ``make -C oracle ref``:
     python tests/golden/make_golden.py
@@ -67,6 +72,23 @@ def _random_solid(shape, frac, rng):
     s = (rng.random(shape) < frac).astype(np.uint8)
     s[~_interior(shape)] = 0
     return s
+
+
+def layered_lap(solid, dx, dy, amp):
+    """lap_diag / lap_off_x / lap_off_y of a layered medium: x conductivity
+    1 + amp sin(2 pi (j - 1/2) / ny) by row, y conductivity 1 + amp cos(2 pi (i - 1/2) / nx)
+    by column (a symmetric operator with zero row sums); solid cells d = 1e15."""
+    ny, nx = solid.shape[0] - 2, solid.shape[1] - 2
+    j, i = np.meshgrid(np.arange(ny + 2), np.arange(nx + 2), indexing="ij")
+    kx = 1.0 + amp * np.sin(2.0 * np.pi * (j - 0.5) / ny)
+    ky = 1.0 + amp * np.cos(2.0 * np.pi * (i - 0.5) / nx)
+    fl = _interior(solid.shape) & (solid == 0)
+    ix, iy = 1.0 / (dx * dx), 1.0 / (dy * dy)
+    ox = np.where(fl, -kx * ix, 0.0)
+    oy = np.where(fl, -ky * iy, 0.0)
+    d = np.where(fl, 2.0 * kx * ix + 2.0 * ky * iy, 0.0)
+    d[_interior(solid.shape) & (solid != 0)] = 1e15
+    return d, ox, oy
 
 
 def cases():
@@ -127,6 +149,23 @@ def cases():
     w = 0.1 * rng.standard_normal((nz + 1, ny + 2, nx + 2))
     out.append(dict(name="project_3d", kind="project", solid=s, u=u, v=v, w=w, dx=h, dy=h, dz=h,
                     dt=dt, max_iter=200, tol=1e-5))
+    # --- variable-coefficient Laplacian (2D) ---------------------------------
+    # The reference's SmoothCylinder takes the solid fraction as 1 OUTSIDE the disk
+    # (cylinder_model.cpp:45-48), so the fluid is the disk itself, and its per-cell
+    # off-diagonals make the operator non-symmetric: CG on it stalls, so a fixed
+    # number of iterations is compared (tol = 0).
+    nx, ny, dx, dy = 40, 32, 1.0 / 40, 1.0 / 32
+    s, (d, ox, oy) = O.ref_smooth_cylinder(np.zeros((ny + 2, nx + 2), np.uint8), dx, dy,
+                                           0.5, 0.5, 0.35)
+    r = np.where(_interior(s.shape) & (s == 0), rng.standard_normal(s.shape), 0.0)
+    out.append(dict(name="varlap_2d_smooth_cylinder", kind="pcg_var", solid=s, r=r, lap_diag=d,
+                    lap_off_x=ox, lap_off_y=oy, dx=dx, dy=dy, dz=1.0, max_iter=12, tol=0.0))
+    nx, ny, dx, dy = 53, 37, 1e-3, 1.5e-3
+    s = _cylinder(nx, ny, dx, dy, 0.25 * nx * dx, 0.5 * ny * dy, 0.1 * ny * dy)
+    d, ox, oy = layered_lap(s, dx, dy, 0.5)
+    r = np.where(_interior(s.shape) & (s == 0), _gauss(s.shape), 0.0)
+    out.append(dict(name="varlap_2d_layered", kind="pcg_var", solid=s, r=r, lap_diag=d,
+                    lap_off_x=ox, lap_off_y=oy, dx=dx, dy=dy, dz=1.0, max_iter=200, tol=1e-9))
     return out
 
 
@@ -135,6 +174,12 @@ def main():
         name = c.pop("name")
         if c["kind"] == "vcycle":
             c["z"] = O.ref_vcycle(c["solid"], c["r"], c["dx"], c["dy"], c["dz"])
+        elif c["kind"] == "pcg_var":
+            lap = (c["lap_diag"], c["lap_off_x"], c["lap_off_y"])
+            p, n = O.ref_pcg_var(c["solid"], lap, c["r"], c["dx"], c["dy"], c["max_iter"],
+                                 c["tol"])
+            c["p"] = p
+            c["applies"] = n
         elif c["kind"] == "pcg":
             p, n = O.ref_pcg(c["solid"], c["r"], c["dx"], c["dy"], c["dz"], c["max_iter"], c["tol"])
             c["p"] = p

@@ -57,6 +57,7 @@ def test_null_and_bad_arguments_are_rejected():
     assert lib.uaamg_project(None, 1.0, None, None, None, None, None, None) == _capi.INVALID_ARG
     assert lib.uaamg_project_device(None, 1.0, None, None, None, None, None, None) == _capi.INVALID_ARG
     assert lib.uaamg_static_pressure(None, None, None, None, None, None) == _capi.INVALID_ARG
+    assert lib.uaamg_set_variable_laplacian(None, None, None, None) == _capi.INVALID_ARG
     assert lib.uaamg_last_error(None) == b"NULL handle"
 
 

@@ -22,6 +22,11 @@ def test_restatement_matches_golden_bit_exact(name):
         p, n, _ = O.pcg(g["solid"], g["r"], g["dx"], g["dy"], g["dz"], g["max_iter"], g["tol"],
                         tol_mode=0)
         assert np.array_equal(p, g["p"]), f"max diff {np.abs(p - g['p']).max()}"
+    elif g["kind"] == "pcg_var":
+        lap = (g["lap_diag"], g["lap_off_x"], g["lap_off_y"])
+        p, n, _ = O.pcg_var(g["solid"], lap, g["r"], g["dx"], g["dy"], g["max_iter"], g["tol"],
+                            tol_mode=0)
+        assert np.array_equal(p, g["p"]), f"max diff {np.abs(p - g['p']).max()}"
     else:
         w = g["w"] if g["w"].size else None
         rhs = O.divergence_rhs(g["solid"], g["u"], g["v"], w, g["dx"], g["dy"], g["dz"], g["dt"])
@@ -155,3 +160,77 @@ def test_host_projection_mirror_matches_compiled_reference(seed):
     PressureProjection.project(g, dt, _OracleSolver(), 40, 1e-9)
     assert np.array_equal(g.p, pr)
     assert np.array_equal(g.u, ur) and np.array_equal(g.v, vr)
+
+
+# --- variable-coefficient Laplacian (Grid::lap_*, pcg.cpp:35-46) -------------
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference (oracle/_ref) not present")
+@pytest.mark.parametrize("case", [(40, 32, 0.5, 0.5, 0.35, 0.0), (57, 31, 0.3, 0.6, 0.2, 0.05),
+                                  (16, 16, 0.5, 0.5, 0.6, 0.0)])
+def test_smooth_cylinder_restatement_matches_compiled_reference(case):
+    nx, ny, cx, cy, r, tw = case
+    dx, dy = 1.0 / nx, 1.0 / ny
+    rng = np.random.default_rng(nx)
+    solid = np.zeros((ny + 2, nx + 2), np.uint8)
+    solid[1:-1, 1:-1] = rng.random((ny, nx)) < 0.05
+    s1, l1 = O.smooth_cylinder(solid, dx, dy, cx, cy, r, tw)
+    s2, l2 = O.ref_smooth_cylinder(solid, dx, dy, cx, cy, r, tw)
+    assert np.array_equal(s1, s2)
+    for a, b in zip(l1, l2):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference (oracle/_ref) not present")
+@pytest.mark.parametrize("seed", range(4))
+def test_variable_pcg_restatement_matches_compiled_reference(seed):
+    """Restated PCG with lap_* against PCG::solve on a grid with init_variable_lap:
+    the reference's own SmoothCylinder coefficients (fixed iterations: that operator
+    is non-symmetric) and random layered media (to convergence), bit for bit."""
+    from uaamg_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    nx, ny = int(rng.integers(20, 70)), int(rng.integers(20, 70))
+    dx, dy = 1.0 / nx, float(rng.uniform(0.5, 2.0)) / ny
+    solid = np.zeros((ny + 2, nx + 2), np.uint8)
+    if seed % 2:
+        solid, lap = O.ref_smooth_cylinder(solid, dx, dy, 0.5, 0.5 * ny * dy, 0.4)
+        max_iter, tol = 15, 0.0
+    else:
+        solid[1:-1, 1:-1] = rng.random((ny, nx)) < 0.03
+        lap = W.layered_lap_2d(solid, dx, dy, float(rng.uniform(0.1, 0.8)))
+        max_iter, tol = 300, 1e-9
+    rhs = np.where(solid == 0, rng.standard_normal(solid.shape), 0.0)
+    rhs[[0, -1], :] = 0.0
+    rhs[:, [0, -1]] = 0.0
+    p, n, _ = O.pcg_var(solid, lap, rhs, dx, dy, max_iter, tol, tol_mode=0)
+    pr, nr = O.ref_pcg_var(solid, lap, rhs, dx, dy, max_iter, tol)
+    assert np.array_equal(p, pr), f"max diff {np.abs(p - pr).max()}"
+    assert nr in (n, n + 1)
+
+
+def test_layered_coefficients_generator():
+    """The bench's layered-medium generator equals the fixture script's formula and
+    gives a symmetric operator with zero row sums (so a zero-mean RHS is solvable)."""
+    import importlib.util
+    from uaamg_b200 import workloads as W
+    spec = importlib.util.spec_from_file_location(
+        "make_golden", os.path.join(ROOT, "tests", "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    nx, ny, dx, dy = 45, 29, 1e-3, 1.5e-3
+    rng = np.random.default_rng(3)
+    solid = np.zeros((ny + 2, nx + 2), np.uint8)
+    solid[1:-1, 1:-1] = rng.random((ny, nx)) < 0.1
+    lap = W.layered_lap_2d(solid, dx, dy, 0.5)
+    for a, b in zip(lap, mg.layered_lap(solid, dx, dy, 0.5)):
+        np.testing.assert_allclose(a, b, rtol=1e-14, atol=0)
+    x = rng.standard_normal(solid.shape)
+    y = rng.standard_normal(solid.shape)
+    fl = (solid == 0)
+    fl[[0, -1], :] = False
+    fl[:, [0, -1]] = False
+    x, y = np.where(fl, x, 0.0), np.where(fl, y, 0.0)
+    ax, ay = O.matvec_var(solid, lap, x), O.matvec_var(solid, lap, y)
+    assert abs(np.sum(y * ax) - np.sum(x * ay)) <= 1e-12 * np.sum(np.abs(y * ax))
+    one = np.where(fl, 1.0, 0.0)
+    assert np.abs(O.matvec_var(solid, lap, one)).max() <= 1e-9 * np.abs(lap[0][fl]).max()

@@ -29,7 +29,8 @@ TOL_ABS, TOL_REL = 0, 1
 EXPORTS = [
     "uaamg_default_options", "uaamg_create", "uaamg_destroy", "uaamg_set_stream",
     "uaamg_set_problem_2d", "uaamg_set_problem_3d", "uaamg_set_problem_device",
-    "uaamg_set_dirichlet_walls", "uaamg_solve", "uaamg_solve_device", "uaamg_precond_apply",
+    "uaamg_set_dirichlet_walls", "uaamg_set_variable_laplacian", "uaamg_solve",
+    "uaamg_solve_device", "uaamg_precond_apply",
     "uaamg_residual_history", "uaamg_num_levels", "uaamg_level_dims", "uaamg_copy_level",
     "uaamg_device_bytes", "uaamg_last_error", "uaamg_status_string", "uaamg_profile_solve",
     "uaamg_set_vcycle_kernels", "uaamg_residual_noalloc", "uaamg_solve_batch",
@@ -147,6 +148,7 @@ def load(path: str | None = None):
     L.uaamg_set_problem_3d.argtypes = [p, i, i, i, d, d, d, p]
     L.uaamg_set_problem_device.argtypes = [p, i, i, i, i, d, d, d, p]
     L.uaamg_set_dirichlet_walls.argtypes = [p, i]
+    L.uaamg_set_variable_laplacian.argtypes = [p, p, p, p]
     L.uaamg_set_vcycle_kernels.argtypes = [p, i]
     L.uaamg_residual_noalloc.argtypes = [i, i, i, i, d, d, d, p, p, p, p, p]
     L.uaamg_solve.argtypes = [p, p, p, C.POINTER(Options), C.POINTER(Stats)]

@@ -79,7 +79,10 @@ void free_problem(uaamg_handle* h) {
         cudaFree(h->d_face[a]);
         h->d_face[a] = nullptr;
         h->face_n[a] = 0;
+        cudaFree(h->d_lap[a]);
+        h->d_lap[a] = nullptr;
     }
+    h->lap_on = false;
     h->hist_cap = 0;
     h->n = 0;
     h->dim = 0;
@@ -99,6 +102,10 @@ uaamg_status engine_for(uaamg_handle* h, int p, uaamg::Engine** out) {
     h->eng[p]->set_vcycle_sweeps(h->sweeps == 1);
     h->eng[p]->set_small_levels(h->sweeps == 0);
     h->eng[p]->set_autotune(h->autotune != 0);
+    if (h->lap_on)
+        h->eng[p]->set_operator(h->d_lap[0], h->d_lap[1], h->d_lap[2], h->nx + 2, h->lap_version);
+    else
+        h->eng[p]->set_operator(nullptr, nullptr, nullptr, 0, h->lap_version);
     if (!h->ready[p]) {
         int e = h->eng[p]->set_problem(h->dim, h->nx, h->ny, h->nz, h->dx, h->dy, h->dz,
                                        h->d_solid, h->dirichlet);
@@ -246,6 +253,42 @@ uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps) {
     if (!h) return UAAMG_INVALID_ARG;
     if (sweeps < 0 || sweeps > 2) return fail(h, UAAMG_INVALID_ARG, "V-cycle kernels: 0, 1 or 2");
     h->sweeps = sweeps;
+    return UAAMG_OK;
+}
+
+uaamg_status uaamg_set_variable_laplacian(uaamg_handle* h, const double* lap_diag,
+                                          const double* lap_off_x, const double* lap_off_y) {
+    if (!h) return UAAMG_INVALID_ARG;
+    const int given = (lap_diag != nullptr) + (lap_off_x != nullptr) + (lap_off_y != nullptr);
+    if (given != 0 && given != 3)
+        return fail(h, UAAMG_INVALID_ARG, "variable Laplacian: give all three arrays or none");
+    if (!h->dim) return fail(h, UAAMG_NO_PROBLEM, "no problem set (call uaamg_set_problem_*)");
+    if (h->dim != 2)
+        return fail(h, UAAMG_INVALID_ARG, "variable Laplacian: 2D problems only");
+    if (!given) {
+        h->lap_on = false;
+        return UAAMG_OK;
+    }
+    cudaSetDevice(h->device);
+    const double* src[3] = {lap_diag, lap_off_x, lap_off_y};
+    const size_t bytes = h->n * sizeof(double);
+    for (int a = 0; a < 3; ++a) {
+        if (!h->d_lap[a] && cudaMalloc(&h->d_lap[a], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(h, UAAMG_OOM, "variable Laplacian: device allocation failed");
+        }
+    }
+    // the solves in flight may still read the previous coefficients
+    cudaError_t e = h->stream ? cudaStreamSynchronize(h->stream) : cudaDeviceSynchronize();
+    for (int a = 0; a < 3 && e == cudaSuccess; ++a)
+        e = cudaMemcpyAsync(h->d_lap[a], src[a], bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        h->lap_on = false;
+        return cuda_fail(h, e, "variable Laplacian upload");
+    }
+    h->lap_on = true;
+    ++h->lap_version;
     return UAAMG_OK;
 }
 

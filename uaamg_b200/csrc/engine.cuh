@@ -208,6 +208,19 @@ public:
     void set_graphs(bool on) override { graphs_ = on; }
     void set_autotune(bool on) override { autotune_ = on; }
     void set_small_levels(bool on) override { tail_on_ = on; }
+    void set_operator(const double* d, const double* ox, const double* oy, int sx,
+                      long version) override {
+        vver_ = version;
+        if (d == vd_ && ox == vox_ && oy == voy_ && sx == vsx_) return;
+        // a captured step holds the operator's pointers: capture again
+        if (gexec_) {
+            cudaStreamSynchronize(st_);
+            cudaGraphExecDestroy(gexec_);
+            gexec_ = nullptr;
+        }
+        gkey_ = -1;
+        vd_ = d; vox_ = ox; voy_ = oy; vsx_ = sx;
+    }
 
     void set_profiling(bool on) override {
         prof_on_ = on;
@@ -256,6 +269,11 @@ private:
     Geom gref_;                      // the caller's (reference) layout of level 0
     std::vector<LevelBuf<T, CS>> lv_;
     T *r_ = nullptr, *z_ = nullptr, *p_ = nullptr, *p2_ = nullptr, *ap_ = nullptr, *xlo_ = nullptr;
+    // variable-coefficient operator (set_operator); not owned
+    const double *vd_ = nullptr, *vox_ = nullptr, *voy_ = nullptr;
+    int vsx_ = 0;
+    long vver_ = 0, vconv_ = -1;     // contents version set / converted into vf_
+    float* vf_[3] = {nullptr, nullptr, nullptr};  // FP32 forms: s, ox, oy (level layout)
     double *b64_ = nullptr, *xd_ = nullptr, *partials_ = nullptr;
     int* err_ = nullptr;             // set by a kernel whose TMA wait gave up
     CUtensorMap map_p_, map_p2_;     // plane boxes of the two search-direction buffers
@@ -293,6 +311,15 @@ private:
     std::vector<KTag> prof_tag_;
 
     int max_reduce_blocks() const { return 4 * num_sms_; }
+
+    // grid of the variable-coefficient search-direction kernel: rows of 32 cells,
+    // eight per block, up to 8 blocks per SM (within the partials' capacity)
+    dim3 var_grid(const Geom& g) const {
+        const long long items = (long long)g.ny * ((g.nx + 31) / 32);
+        long long nb = std::min<long long>((items + 7) / 8, 8LL * num_sms_);
+        nb = std::min<long long>(nb, reduce_blocks_);
+        return dim3((unsigned)(nb < 1 ? 1 : nb));
+    }
 
     // grid of the FP64 residual column walk (kernels.cuh k_resid_x64): tiles of
     // 32 x 8 columns and kResidZc planes, at most 8 blocks of 256 threads per SM
@@ -352,6 +379,8 @@ private:
         bytes_ = 0;
         r_ = z_ = p_ = p2_ = ap_ = xlo_ = nullptr;
         b64_ = xd_ = partials_ = nullptr;
+        vf_[0] = vf_[1] = vf_[2] = nullptr;
+        vconv_ = -1;
         err_ = nullptr;
         cg_ = nullptr;
         if (cg_host_) { cudaFreeHost(cg_host_); cg_host_ = nullptr; }
@@ -877,6 +906,14 @@ private:
         st.idz2 = dim_ == 3 ? 1.0 / (dz_ * dz_) : 0.0;
         st.diag = dim_ == 3 ? 2.0 * (st.idx2 + st.idy2 + st.idz2) : 2.0 * (st.idx2 + st.idy2);
         st.dirichlet = dirichlet_;
+        const bool var = dim_ == 2 && vd_ && vox_ && voy_;
+        st.vsx = var ? vsx_ : 0;
+        st.vd = var ? vd_ : nullptr;
+        st.vox = var ? vox_ : nullptr;
+        st.voy = var ? voy_ : nullptr;
+        st.fs = var ? vf_[0] : nullptr;
+        st.fx = var ? vf_[1] : nullptr;
+        st.fy = var ? vf_[2] : nullptr;
         return st;
     }
 
@@ -900,13 +937,20 @@ private:
         const Geom& g = lv_[0].g;
         const Stencil st = stencil();
         T* pnew = from_p ? p2_ : p_;
-        MarchMaps pm = maps<DIM>(0, true, false);  // z and the current search direction
-        pm.v[0] = lv_[0].mx;
-        pm.v[1] = from_p ? map_p_ : map_p2_;
-        UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
-                          (k_pmatvec<DIM, T>), march_grid<DIM>(g, lv_[0].zc), dim3(kThreads),
-                          (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st, partials_, cg_,
-                          err_);
+        if (DIM == 2 && st.vd) {
+            // z, p_old, codes, the three coefficients in; p, Ap out
+            UAAMG_LAUNCH((KTag{K_PMATVEC, 0, cells(g) * (7.0 * sizeof(T) + 1.0)}), k_pmatvec_var<T>,
+                         var_grid(g), dim3(32, 8), g, lv_[0].code, z_, from_p ? p_ : p2_, pnew, ap_,
+                         st, partials_, cg_);
+        } else {
+            MarchMaps pm = maps<DIM>(0, true, false);  // z and the current search direction
+            pm.v[0] = lv_[0].mx;
+            pm.v[1] = from_p ? map_p_ : map_p2_;
+            UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
+                              (k_pmatvec<DIM, T>), march_grid<DIM>(g, lv_[0].zc), dim3(kThreads),
+                              (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st, partials_, cg_,
+                              err_);
+        }
         const long long nvec = (long long)g.n / Vec16<T>::N;
         // x_lo, r, p, Ap in; x_lo, r out (a fold after a replacement adds x_hi in and out)
         UAAMG_LAUNCH((KTag{K_UPDATE, 0, cells(g) * (6.0 * sizeof(T))}), k_update_flat<T>,
@@ -929,6 +973,22 @@ private:
         const dim3 vb(32, 8);
         const dim3 vg = vec_grid(g);
         const int n = g.n;
+        if (DIM == 2 && sizeof(T) == 4 && vd_ && vox_ && voy_ && vconv_ != vver_) {
+            // FP32 copies of the variable-coefficient operator (once per contents)
+            if (!vf_[0]) {
+                for (int q = 0; q < 3; ++q)
+                    if (int e = alloc(vf_[q], (size_t)n)) return e;
+                if (gexec_) {  // a captured step holds the copies' (null) pointers
+                    cudaStreamSynchronize(st_);
+                    cudaGraphExecDestroy(gexec_);
+                    gexec_ = nullptr;
+                }
+                gkey_ = -1;
+            }
+            UAAMG_LAUNCH((KTag{K_SETUP, 0, cells(g) * 36.0}), k_var_coeffs, vg, vb, g, stencil(),
+                         vf_[0], vf_[1], vf_[2]);
+            vconv_ = vver_;
+        }
         const Stencil st = stencil();
 
         CGState init = {};

@@ -87,6 +87,13 @@ public:
     // Marches: run the small levels and the coarsest solve as one single-block
     // kernel (default on; off: marches on every level).
     virtual void set_small_levels(bool on) = 0;
+    // 2D variable-coefficient outer-CG operator (the lap_diag / lap_off_x / lap_off_y
+    // branch of PCG::solve, pcg.cpp:35-46): device arrays in the caller's padded
+    // layout with row stride sx, read in place by every solve until changed;
+    // nullptr: the uniform operator.  The V-cycle keeps its own couplings.  version
+    // changes whenever the arrays' contents do (the FP32 forms keep converted copies).
+    virtual void set_operator(const double* d, const double* ox, const double* oy, int sx,
+                              long version) = 0;
     // Replay each pair of PCG iterations as one CUDA graph (default on).
     virtual void set_graphs(bool on) = 0;
     // 1: the next set_problem times each level's marches for a few z-chunk lengths

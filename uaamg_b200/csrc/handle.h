@@ -18,6 +18,9 @@ struct uaamg_handle {
     double* d_p = nullptr;
     double* d_hist = nullptr;
     double* d_face[3] = {nullptr, nullptr, nullptr};  // face velocities of uaamg_project
+    double* d_lap[3] = {nullptr, nullptr, nullptr};   // lap_diag, lap_off_x, lap_off_y
+    bool lap_on = false;                              // uaamg_set_variable_laplacian
+    long lap_version = 0;                             // bumped on every upload
     cudaStream_t copy_stream = nullptr;  // uaamg_solve: p's upload beside the solve
     cudaEvent_t p_ready = nullptr;
     size_t face_n[3] = {0, 0, 0};

@@ -307,7 +307,29 @@ __global__ void k_coarsest(LevelView<T> L, const int* __restrict__ done) {
 struct Stencil {
     double idx2, idy2, idz2, diag;
     int dirichlet;
+    // 2D variable-coefficient operator (Grid::lap_diag / lap_off_x / lap_off_y,
+    // include/core/grid.h:23-31), the caller's padded arrays in the reference
+    // layout (index i + j * vsx); vd == nullptr: the uniform operator
+    int vsx;
+    const double* __restrict__ vd;
+    const double* __restrict__ vox;
+    const double* __restrict__ voy;
+    // FP32 forms: per-cell copies in the level's own layout (index id) of
+    // s = d + 2 ox + 2 oy, ox and oy, for the difference form of the operator
+    const float* __restrict__ fs;
+    const float* __restrict__ fx;
+    const float* __restrict__ fy;
 };
+
+
+// The variable-coefficient branch of PCG::solve's operator (pcg.cpp:35-46):
+// A v = d v_C + ox (v_L + v_R) + oy (v_B + v_T) with the same neighbour rule as the
+// uniform operator, summed in the reference's order.
+template <class T>
+__device__ __forceinline__ T var_op(const Stencil& st, int i, int j, T vc, T vL, T vR, T vB, T vT) {
+    const long long q = i + (long long)j * st.vsx;
+    return (T)st.vd[q] * vc + (T)st.vox[q] * (vL + vR) + (T)st.voy[q] * (vB + vT);
+}
 
 // Reference PCG operator (pcg_3d.cpp:38-55, pcg.cpp:47-59): a solid or out-of-domain
 // neighbour reads p_C (Neumann; -p_C for a Dirichlet wall); solid rows are 0.
@@ -348,6 +370,18 @@ __device__ __forceinline__ void for_cells(const Geom& g, F&& f) {
         const int k = DIM == 3 ? 1 + row / g.ny : 0;
         f(i, j, k, cidx(g, i, j, k));
     }
+}
+
+// s = d + 2 ox + 2 oy (FP64), ox, oy of every interior cell as FP32 in the level's
+// layout, from the caller's padded arrays (reference layout, row stride st.vsx).
+__global__ void k_var_coeffs(Geom g, Stencil st, float* fs, float* fx, float* fy) {
+    for_cells<2>(g, [&](int i, int j, int, int id) {
+        const long long q = i + (long long)j * st.vsx;
+        const double d = st.vd[q], ox = st.vox[q], oy = st.voy[q];
+        fs[id] = (float)(d + 2.0 * ox + 2.0 * oy);
+        fx[id] = (float)ox;
+        fy[id] = (float)oy;
+    });
 }
 
 // Sum and count over fluid interior cells of a FP64 field: cg->sum0, cg->nfluid.
@@ -437,8 +471,17 @@ __global__ void k_true_residual(Geom g, const uint8_t* __restrict__ s, const dou
     for_cells<DIM>(g, [&](int i, int j, int k, int id) {
         if (!s[id]) {
             double r = b[id];
-            if (x) r = r - apply_A<DIM, double>(g, s, x, i, j, k, id, st.idx2, st.idy2, st.idz2,
-                                                st.diag, st.dirichlet);
+            if (x && DIM == 2 && st.vd) {
+                const double vc = x[id], wall = st.dirichlet ? -vc : vc;
+                const double vL = i > 1 ? (!s[id - 1] ? x[id - 1] : vc) : wall;
+                const double vR = i < g.nx ? (!s[id + 1] ? x[id + 1] : vc) : wall;
+                const double vB = j > 1 ? (!s[id - g.sx] ? x[id - g.sx] : vc) : wall;
+                const double vT = j < g.ny ? (!s[id + g.sx] ? x[id + g.sx] : vc) : wall;
+                r = r - var_op<double>(st, i, j, vc, vL, vR, vB, vT);
+            } else if (x) {
+                r = r - apply_A<DIM, double>(g, s, x, i, j, k, id, st.idx2, st.idy2, st.idz2,
+                                             st.diag, st.dirichlet);
+            }
             if (rw) rw[id] = (T)r;
             acc[0] += r * r;
         } else if (rw) {
@@ -499,6 +542,8 @@ __global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __rest
                 const double vF = (c & 32u) ? xm : (k > 1 ? xc : wall);
                 const double vK = (c & 16u) ? xp : (k < g.nz ? xc : wall);
                 ax = diag * xc - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
+            } else if (st.vd) {
+                ax = (c & kActive) ? var_op<double>(st, i, j, xc, vL, vR, vB, vT) : 0.0;
             } else {
                 ax = diag * xc - (vL + vR) * idx2 - (vB + vT) * idy2;
             }
@@ -518,6 +563,59 @@ __global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __rest
             cg->status = CG_MAXITER;
             cg->done = 1;
         }
+    }
+}
+
+// 2D search direction with the variable-coefficient operator, the same fused step
+// as the z march k_pmatvec (march.cuh): p = (z - m) + beta p_old on fluid cells
+// (pcg.cpp:113-122), Ap = d p_C + ox (p_L + p_R) + oy (p_B + p_T) (pcg.cpp:35-46)
+// from the new p of the neighbours, formed on the fly (a solid or out-of-domain
+// neighbour reads p_C), p.Ap reduced; the last block sets alpha = rz_old / p.Ap or
+// stops on breakdown (pcg.cpp:97-99).  FP64 evaluates the reference's expression on
+// its arrays; FP32 the difference form on FP32 copies (st.fs, fx, fy).  A warp owns
+// 32 cells of a row; the neighbours' z and p_old come from L1 / L2.  p_old and
+// p_new are distinct buffers.
+template <class T>
+__global__ void k_pmatvec_var(Geom g, const uint8_t* __restrict__ code, const T* __restrict__ z,
+                              const T* __restrict__ pold, T* __restrict__ pnew, T* __restrict__ ap,
+                              Stencil st, double* partials, CGState* cg) {
+    if (cg->done) return;
+    const T m = (T)cg->mean_z, beta = (T)cg->beta;
+    auto pv = [&](int q) -> T { return (z[q] - m) + beta * pold[q]; };
+    double acc[1] = {0.0};
+    for_cells<2>(g, [&](int i, int j, int, int id) {
+        const uint32_t c = code[id];
+        if (!(c & kActive)) {
+            pnew[id] = T(0);
+            ap[id] = T(0);
+            return;
+        }
+        const T p0 = pv(id);
+        const T wall = st.dirichlet ? -p0 : p0;
+        const T vL = (c & 2u) ? pv(id - 1) : (i > 1 ? p0 : wall);
+        const T vR = (c & 1u) ? pv(id + 1) : (i < g.nx ? p0 : wall);
+        const T vB = (c & 8u) ? pv(id - g.sx) : (j > 1 ? p0 : wall);
+        const T vT = (c & 4u) ? pv(id + g.sx) : (j < g.ny ? p0 : wall);
+        T a;
+        if constexpr (sizeof(T) == 8) {
+            a = var_op<T>(st, i, j, p0, vL, vR, vB, vT);
+        } else {
+            // the same operator as (d + 2 ox + 2 oy) p_C - ox ((p_C - p_L) + (p_C - p_R))
+            // - oy (...): no cancellation of O(1/h^2) terms in FP32
+            a = st.fs[id] * p0 - st.fx[id] * ((p0 - vL) + (p0 - vR)) -
+                st.fy[id] * ((p0 - vB) + (p0 - vT));
+        }
+        pnew[id] = p0;
+        ap[id] = a;
+        acc[0] += (double)p0 * (double)a;
+    });
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
+        const double pap = tot[0];
+        cg->pap = pap;
+        if (!(pap == pap)) { cg->status = CG_NAN; cg->done = 1; }
+        else if (pap < cg->breakdown) { cg->status = CG_BREAKDOWN; cg->done = 1; }
+        else cg->alpha = cg->rz_old / pap;
     }
 }
 

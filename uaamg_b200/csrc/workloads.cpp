@@ -11,6 +11,8 @@
 //   wl_obstacle_flow_2d  2D disk obstacle, uniform inflow + random Fourier modes;
 //                        RHS = div(u)/dt at fluid cells (the 2D projection workload)
 //   wl_obstacle_flow_3d  3D sphere obstacle, same velocity model
+//   wl_layered_lap_2d    variable-coefficient Laplacian of a layered medium
+//                        (lap_diag / lap_off_x / lap_off_y of a 2D grid)
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -402,6 +404,41 @@ WL_API long wl_obstacle_flow_3d(int nx, int ny, int nz, double dx, double dy, do
 // A request at step t of the id uses rhs0 + (t / 20) rhs1 (an evolving field).
 // Both are zero at solids with zero fluid mean.  Separable evaluation: the
 // per-axis cosine/sine tables combine per row, so a cell costs 6 flops per mode.
+// Coefficients of the 2D operator A v = d v_C + ox (v_L + v_R) + oy (v_B + v_T)
+// (the lap_* form PCG::solve takes, pcg.cpp:35-46) for a layered medium: the x
+// conductivity varies with the row, kx(j) = 1 + amp sin(2 pi (j - 1/2) / ny), the y
+// conductivity with the column, ky(i) = 1 + amp cos(2 pi (i - 1/2) / nx), so the
+// coupling between two cells is the same from either side (A symmetric) and every
+// row sums to zero (the constant is A's null vector, as for the uniform operator).
+// ox = -kx/dx^2, oy = -ky/dy^2, d = 2 kx/dx^2 + 2 ky/dy^2 on fluid cells; solid
+// cells get d = 1e15 and no couplings (never read: solid rows are 0); ghosts 0.
+// Returns the number of fluid cells.
+WL_API long wl_layered_lap_2d(int nx, int ny, double dx, double dy, double amp,
+                              const uint8_t* solid, double* diag, double* ox, double* oy) {
+    const double pi = 3.14159265358979323846;
+    const size_t n = (size_t)(nx + 2) * (ny + 2);
+    std::memset(diag, 0, n * sizeof(double));
+    std::memset(ox, 0, n * sizeof(double));
+    std::memset(oy, 0, n * sizeof(double));
+    const double ix = 1.0 / (dx * dx), iy = 1.0 / (dy * dy);
+    long fluid = 0;
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            const size_t c = pid(nx, ny, i, j, 0);
+            if (solid[c]) {
+                diag[c] = 1e15;
+                continue;
+            }
+            const double kx = 1.0 + amp * std::sin(2.0 * pi * (j - 0.5) / ny);
+            const double ky = 1.0 + amp * std::cos(2.0 * pi * (i - 0.5) / nx);
+            ox[c] = -kx * ix;
+            oy[c] = -ky * iy;
+            diag[c] = 2.0 * kx * ix + 2.0 * ky * iy;
+            ++fluid;
+        }
+    return fluid;
+}
+
 WL_API long wl_serve_fields(int dim, int n, int kmax, uint64_t seed, uint8_t* solid, double* rhs0,
                             double* rhs1) {
     const int nz = dim == 3 ? n : 0;

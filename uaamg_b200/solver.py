@@ -43,6 +43,20 @@ class Grid:
         self.v = np.zeros((ny + 1, nx + 2))
         self.p = np.zeros((ny + 2, nx + 2))
         self.solid = np.zeros((ny + 2, nx + 2), np.uint8)
+        # variable-coefficient Laplacian (include/core/grid.h:23-31): empty until
+        # init_variable_lap(); PCG::solve then uses them (pcg.cpp:35-46)
+        self.lap_diag = np.zeros(0)
+        self.lap_off_x = np.zeros(0)
+        self.lap_off_y = np.zeros(0)
+
+    def init_variable_lap(self):
+        """Zero padded coefficient arrays (Grid::init_variable_lap, grid.cpp:12-17)."""
+        self.lap_diag = np.zeros(self.p.shape)
+        self.lap_off_x = np.zeros(self.p.shape)
+        self.lap_off_y = np.zeros(self.p.shape)
+
+    def has_variable_lap(self):
+        return self.lap_diag.size != 0
 
     @property
     def nz(self):
@@ -118,6 +132,18 @@ class Handle:
         """0 / False: z marches + the single-block small-level kernel (default);
         1 / True: per-colour sweep kernels; 2: z marches on every level."""
         self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(mode)), "vcycle")
+
+    def set_variable_laplacian(self, lap_diag=None, lap_off_x=None, lap_off_y=None):
+        """The outer CG's variable-coefficient operator for the current 2D problem
+        (uaamg_set_variable_laplacian); no arguments: back to the uniform one."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in (lap_diag, lap_off_x, lap_off_y)]
+        for a in arrs:
+            if a is not None and self.shape is not None and a.shape != tuple(self.shape):
+                raise ValueError(f"coefficient shape {a.shape} != padded grid {self.shape}")
+        st = self.lib.uaamg_set_variable_laplacian(
+            self.h, *(_ptr(a) if a is not None else None for a in arrs))
+        self._check(st, "set_variable_laplacian")
 
     def set_dirichlet_walls(self, on: bool):
         self._check(self.lib.uaamg_set_dirichlet_walls(self.h, int(bool(on))), "dirichlet")
@@ -435,6 +461,7 @@ class GpuUAAMGPCG(Solver):
         self.handle = Handle(device)
         self._key = None
         self._solid = None
+        self._var = False
         self.last_stats = None
 
     def _sync_problem(self, g):
@@ -443,6 +470,15 @@ class GpuUAAMGPCG(Solver):
             self.handle.set_problem(g.solid, g.dx, g.dy, getattr(g, "dz", 1.0))
             self._key = key
             self._solid = np.array(g.solid, dtype=np.uint8, copy=True)
+            self._var = False
+        # the grid's variable-coefficient Laplacian, sent on every call (the caller
+        # may change the arrays in place), as PCG::solve reads them each time
+        var = bool(getattr(g, "has_variable_lap", lambda: False)())
+        if var:
+            self.handle.set_variable_laplacian(g.lap_diag, g.lap_off_x, g.lap_off_y)
+        elif self._var:
+            self.handle.set_variable_laplacian()
+        self._var = var
 
     def solve(self, g, rhs, max_iter, tol):
         self._sync_problem(g)

@@ -9,6 +9,9 @@ Every generator returns padded numpy arrays in the reference's memory order
 * ``obstacle_2d``: 2048 x 1024, dx = 1e-3, dy = 1.5e-3, disk of radius 0.05*Ly at
   (0.25 Lx, 0.5 Ly); u = 1 + Fourier modes |k| <= 16 with N(0,1)/|k|^2
   amplitudes, v = modes; RHS = div(u)/dt, dt = 1e-3; seed 20260202.
+* ``layered_2d``: the obstacle_2d grid, mask and RHS, solved with the 2D
+  variable-coefficient operator (lap_diag / lap_off_x / lap_off_y) of a layered
+  medium: x conductivity 1 + 0.5 sin(2 pi y / Ly), y conductivity 1 + 0.5 cos(2 pi x / Lx).
 * ``batch96``: 64 2D problems with nx, ny uniform on {64, 128, ..., 1024} and 32 3D
   problems with nx, ny, nz uniform on {32, 48, 64, 96, 128}; h = 1/max(dims);
   random solid boxes up to a coverage U[0, 0.2]; smoothed-noise RHS; seed 20260404.
@@ -45,6 +48,8 @@ def _load():
         L.wl_obstacle_flow_2d.restype = C.c_long
         L.wl_obstacle_flow_3d.argtypes = [i, i, i, d, d, d, d, i, u64, d, p, p, p, p, p]
         L.wl_obstacle_flow_3d.restype = C.c_long
+        L.wl_layered_lap_2d.argtypes = [i, i, d, d, d, p, p, p, p]
+        L.wl_layered_lap_2d.restype = C.c_long
         L.wl_serve_fields.argtypes = [i, i, i, u64, p, p, p]
         L.wl_serve_fields.restype = C.c_long
         _lib = L
@@ -92,6 +97,16 @@ def obstacle_flow_3d(nx, ny, nz, dx, dy, dz, dt=1e-3, kmax=8, seed=20260505, t=0
     return solid, u, v, w, rhs
 
 
+def layered_lap_2d(solid, dx, dy, amp=0.5):
+    """(lap_diag, lap_off_x, lap_off_y) of a layered medium on a padded 2D mask,
+    see wl_layered_lap_2d: symmetric, zero row sums, conductivities in [1-amp, 1+amp]."""
+    solid = np.ascontiguousarray(solid, dtype=np.uint8)
+    ny, nx = (s - 2 for s in solid.shape)
+    lap = tuple(np.zeros(solid.shape) for _ in range(3))
+    _load().wl_layered_lap_2d(nx, ny, dx, dy, amp, _p(solid), *(_p(a) for a in lap))
+    return lap
+
+
 def spheres_256():
     """The 256^3 mixed-precision workload: (solid, rhs, h)."""
     s, r = spheres_3d(256, 256, 256)
@@ -103,6 +118,14 @@ def obstacle_2d():
     dx, dy, dt = 1.0e-3, 1.5e-3, 1.0e-3
     s, u, v, r = obstacle_flow_2d(2048, 1024, dx, dy, dt)
     return s, u, v, r, dx, dy, dt
+
+
+def layered_2d(amp=0.5):
+    """The obstacle_2d grid, mask and RHS with the variable-coefficient Laplacian of
+    a layered medium (layered_lap_2d, conductivities in [0.5, 1.5]):
+    (solid, rhs, dx, dy, (lap_diag, lap_off_x, lap_off_y))."""
+    s, _, _, r, dx, dy, _ = obstacle_2d()
+    return s, r, dx, dy, layered_lap_2d(s, dx, dy, amp)
 
 
 def serve_fields(dim, n, seed, kmax=None):
