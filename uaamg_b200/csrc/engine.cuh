@@ -312,10 +312,11 @@ private:
 
     int max_reduce_blocks() const { return 4 * num_sms_; }
 
-    // grid of the variable-coefficient search-direction kernel: rows of 32 cells,
-    // eight per block, up to 8 blocks per SM (within the partials' capacity)
+    // grid of the variable-coefficient search-direction kernel: 32 column pairs of
+    // two rows a warp, eight warps a block, up to 8 blocks per SM (within the
+    // partials' capacity)
     dim3 var_grid(const Geom& g) const {
-        const long long items = (long long)g.ny * ((g.nx + 31) / 32);
+        const long long items = (long long)((g.ny + 1) / 2) * ((g.nx + 31) / 32);
         long long nb = std::min<long long>((items + 7) / 8, 8LL * num_sms_);
         nb = std::min<long long>(nb, reduce_blocks_);
         return dim3((unsigned)(nb < 1 ? 1 : nb));

@@ -572,43 +572,95 @@ __global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __rest
 // from the new p of the neighbours, formed on the fly (a solid or out-of-domain
 // neighbour reads p_C), p.Ap reduced; the last block sets alpha = rz_old / p.Ap or
 // stops on breakdown (pcg.cpp:97-99).  FP64 evaluates the reference's expression on
-// its arrays; FP32 the difference form on FP32 copies (st.fs, fx, fy).  A warp owns
-// 32 cells of a row; the neighbours' z and p_old come from L1 / L2.  p_old and
+// its arrays; FP32 the difference form on FP32 copies (st.fs, fx, fy).
+// A thread owns the vertical pair (i, j), (i, j+1) -- j odd -- and a warp 32 such
+// columns; every load of a step (z and p_old of the pair, its side neighbours and
+// the rows below and above, codes, coefficients) is issued before any is used, the
+// pair sharing its vertical neighbours.  Reads of ghost or solid cells are harmless
+// (the padded arrays hold them) and discarded by the neighbour rule.  p_old and
 // p_new are distinct buffers.
 template <class T>
-__global__ void k_pmatvec_var(Geom g, const uint8_t* __restrict__ code, const T* __restrict__ z,
-                              const T* __restrict__ pold, T* __restrict__ pnew, T* __restrict__ ap,
-                              Stencil st, double* partials, CGState* cg) {
+__global__ void __launch_bounds__(256) k_pmatvec_var(Geom g, const uint8_t* __restrict__ code,
+                                                     const T* __restrict__ z,
+                                                     const T* __restrict__ pold,
+                                                     T* __restrict__ pnew, T* __restrict__ ap,
+                                                     Stencil st, double* partials, CGState* cg) {
     if (cg->done) return;
     const T m = (T)cg->mean_z, beta = (T)cg->beta;
-    auto pv = [&](int q) -> T { return (z[q] - m) + beta * pold[q]; };
     double acc[1] = {0.0};
-    for_cells<2>(g, [&](int i, int j, int, int id) {
-        const uint32_t c = code[id];
-        if (!(c & kActive)) {
-            pnew[id] = T(0);
-            ap[id] = T(0);
-            return;
+    const int sx = g.sx;
+    const int nxc = (g.nx + 31) >> 5;
+    const long long nitems = (long long)((g.ny + 1) >> 1) * nxc;
+    for (long long it = (long long)blockIdx.x * blockDim.y + threadIdx.y; it < nitems;
+         it += (long long)gridDim.x * blockDim.y) {
+        const int pr = (int)(it / nxc);
+        const int ch = (int)(it - (long long)pr * nxc);
+        const int i = 1 + (ch << 5) + (int)threadIdx.x;
+        if (i > g.nx) continue;
+        const int j = 1 + 2 * pr;
+        const bool hb = j < g.ny;  // (i, j+1) is an interior cell
+        const int id = cidx(g, i, j, 0);
+        const int sb = hb ? sx : 0;            // second cell, or the first again
+        const int s2 = hb ? 2 * sx : sx;       // the row above the pair (a ghost at most)
+        // 0: below A, 1: A, 2: B (above A), 3: above B, 4/5: A -x/+x, 6/7: B -x/+x
+        const int off[8] = {-sx, 0, sb, s2, -1, 1, sb - 1, sb + 1};
+        T zz[8], qq[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            zz[e] = z[id + off[e]];
+            qq[e] = pold[id + off[e]];
         }
-        const T p0 = pv(id);
-        const T wall = st.dirichlet ? -p0 : p0;
-        const T vL = (c & 2u) ? pv(id - 1) : (i > 1 ? p0 : wall);
-        const T vR = (c & 1u) ? pv(id + 1) : (i < g.nx ? p0 : wall);
-        const T vB = (c & 8u) ? pv(id - g.sx) : (j > 1 ? p0 : wall);
-        const T vT = (c & 4u) ? pv(id + g.sx) : (j < g.ny ? p0 : wall);
-        T a;
+        const uint32_t cc[2] = {code[id], code[id + sb]};
+        T k0[2], kx[2], ky[2];
         if constexpr (sizeof(T) == 8) {
-            a = var_op<T>(st, i, j, p0, vL, vR, vB, vT);
+            const long long q = i + (long long)j * st.vsx, qb = hb ? st.vsx : 0;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                k0[e] = st.vd[q + e * qb];
+                kx[e] = st.vox[q + e * qb];
+                ky[e] = st.voy[q + e * qb];
+            }
         } else {
-            // the same operator as (d + 2 ox + 2 oy) p_C - ox ((p_C - p_L) + (p_C - p_R))
-            // - oy (...): no cancellation of O(1/h^2) terms in FP32
-            a = st.fs[id] * p0 - st.fx[id] * ((p0 - vL) + (p0 - vR)) -
-                st.fy[id] * ((p0 - vB) + (p0 - vT));
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                k0[e] = st.fs[id + e * sb];
+                kx[e] = st.fx[id + e * sb];
+                ky[e] = st.fy[id + e * sb];
+            }
         }
-        pnew[id] = p0;
-        ap[id] = a;
-        acc[0] += (double)p0 * (double)a;
-    });
+        T pp[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) pp[e] = (zz[e] - m) + beta * qq[e];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            if (e == 1 && !hb) break;
+            const uint32_t c = cc[e];
+            const int jj = j + e, cid = id + e * sx;
+            if (!(c & kActive)) {
+                pnew[cid] = T(0);
+                ap[cid] = T(0);
+                continue;
+            }
+            const T p0 = pp[1 + e];
+            const T wall = st.dirichlet ? -p0 : p0;
+            const T vL = (c & 2u) ? pp[4 + 2 * e] : (i > 1 ? p0 : wall);
+            const T vR = (c & 1u) ? pp[5 + 2 * e] : (i < g.nx ? p0 : wall);
+            const T vB = (c & 8u) ? pp[e] : (jj > 1 ? p0 : wall);
+            const T vT = (c & 4u) ? pp[2 + e] : (jj < g.ny ? p0 : wall);
+            T a;
+            if constexpr (sizeof(T) == 8) {
+                // the reference's expression and order
+                a = k0[e] * p0 + kx[e] * (vL + vR) + ky[e] * (vB + vT);
+            } else {
+                // the same operator as (d + 2 ox + 2 oy) p_C - ox ((p_C - p_L) + (p_C - p_R))
+                // - oy (...): no cancellation of O(1/h^2) terms in FP32
+                a = k0[e] * p0 - kx[e] * ((p0 - vL) + (p0 - vR)) - ky[e] * ((p0 - vB) + (p0 - vT));
+            }
+            pnew[cid] = p0;
+            ap[cid] = a;
+            acc[0] += (double)p0 * (double)a;
+        }
+    }
     double tot[1];
     if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
         const double pap = tot[0];
