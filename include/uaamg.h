@@ -123,7 +123,7 @@ UAAMG_API uaamg_status uaamg_set_problem_device(uaamg_handle* h, int dim, int nx
  * on fluid cells (a solid or out-of-domain neighbour reads v_C; solid rows 0) for its
  * search directions and FP64 residuals; the UAAMG V-cycle keeps its uniform
  * couplings, as the reference's does.  All three NULL: back to the uniform
- * operator.  UAAMG_INVALID_ARG for a 3D problem (Grid3D has no such arrays) or when
+ * operator.  uaamg_solve_batch and the server keep the uniform operator.  UAAMG_INVALID_ARG for a 3D problem (Grid3D has no such arrays) or when
  * only some are NULL; UAAMG_NO_PROBLEM before uaamg_set_problem_*, which clears the
  * coefficients. */
 UAAMG_API uaamg_status uaamg_set_variable_laplacian(uaamg_handle* h, const double* lap_diag,

@@ -64,3 +64,51 @@ def test_workloads_are_deterministic_and_shaped():
     sb, rb = workloads.boxes(2, 128, 64, 0, 0.15, seed=11)
     frac = sb[1:-1, 1:-1].mean()
     assert 0.15 <= frac < 0.5
+
+
+def test_variable_lap_mirror_and_solver_sync(monkeypatch):
+    """Grid.init_variable_lap mirrors Grid::init_variable_lap (grid.cpp:12-17), and
+    GpuUAAMGPCG sends the grid's lap_* arrays on every call (PCG::solve reads them
+    each time), clears them once they are gone and re-sends after a new mask."""
+    import uaamg_b200.solver as S
+
+    g = Grid(6, 4, 1.0, 1.0)
+    assert not g.has_variable_lap()
+    g.init_variable_lap()
+    assert g.has_variable_lap() and g.lap_diag.shape == g.p.shape
+    assert not g.lap_diag.any() and not g.lap_off_x.any() and not g.lap_off_y.any()
+
+    calls = []
+
+    class FakeHandle:
+        options = staticmethod(S.Handle.options)
+
+        def __init__(self, device=0):
+            pass
+
+        def set_problem(self, solid, dx, dy, dz=1.0):
+            calls.append("problem")
+
+        def set_variable_laplacian(self, *arrs):
+            calls.append("lap" if arrs else "clear")
+
+        def solve(self, rhs, p, opts, strict=False):
+            calls.append("solve")
+            return None
+
+    monkeypatch.setattr(S, "Handle", FakeHandle)
+    solver = S.GpuUAAMGPCG("fp64")
+    rhs = np.zeros(g.p.shape)
+    solver.solve(g, rhs, 10, 1e-6)
+    solver.solve(g, rhs, 10, 1e-6)
+    assert calls == ["problem", "lap", "solve", "lap", "solve"]
+    calls.clear()
+    g.lap_diag = g.lap_off_x = g.lap_off_y = np.zeros(0)
+    solver.solve(g, rhs, 10, 1e-6)
+    solver.solve(g, rhs, 10, 1e-6)
+    assert calls == ["clear", "solve", "solve"]
+    calls.clear()
+    g.init_variable_lap()
+    g.solid[2, 3] = 1
+    solver.solve(g, rhs, 10, 1e-6)
+    assert calls == ["problem", "lap", "solve"]
