@@ -312,10 +312,10 @@ private:
 
     int max_reduce_blocks() const { return 4 * num_sms_; }
 
-    // grid of the variable-coefficient search-direction kernel: 32 column pairs of
-    // two rows a warp, eight warps a block, up to 8 blocks per SM (within the
-    // partials' capacity)
-    dim3 var_grid(const Geom& g) const {
+    // grid of the 2D search-direction kernel (kernels.cuh k_pmatvec_2d): 32 column
+    // pairs of two rows a warp, eight warps a block, up to 8 blocks per SM (within
+    // the partials' capacity)
+    dim3 flat2d_grid(const Geom& g) const {
         const long long items = (long long)((g.ny + 1) / 2) * ((g.nx + 31) / 32);
         long long nb = std::min<long long>((items + 7) / 8, 8LL * num_sms_);
         nb = std::min<long long>(nb, reduce_blocks_);
@@ -938,11 +938,12 @@ private:
         const Geom& g = lv_[0].g;
         const Stencil st = stencil();
         T* pnew = from_p ? p2_ : p_;
-        if (DIM == 2 && st.vd) {
-            // z, p_old, codes, the three coefficients in; p, Ap out
-            UAAMG_LAUNCH((KTag{K_PMATVEC, 0, cells(g) * (7.0 * sizeof(T) + 1.0)}), k_pmatvec_var<T>,
-                         var_grid(g), dim3(32, 8), g, lv_[0].code, z_, from_p ? p_ : p2_, pnew, ap_,
-                         st, partials_, cg_);
+        if (DIM == 2) {
+            // z, p_old, codes (and the three coefficients) in; p, Ap out
+            const double nb = st.vd ? 7.0 * sizeof(T) + 1.0 : 4.0 * sizeof(T) + 1.0;
+            UAAMG_LAUNCH((KTag{K_PMATVEC, 0, cells(g) * nb}), k_pmatvec_2d<T>, flat2d_grid(g),
+                         dim3(32, 8), g, lv_[0].code, z_, from_p ? p_ : p2_, pnew, ap_, st,
+                         partials_, cg_);
         } else {
             MarchMaps pm = maps<DIM>(0, true, false);  // z and the current search direction
             pm.v[0] = lv_[0].mx;

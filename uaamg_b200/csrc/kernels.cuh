@@ -566,13 +566,15 @@ __global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __rest
     }
 }
 
-// 2D search direction with the variable-coefficient operator, the same fused step
-// as the z march k_pmatvec (march.cuh): p = (z - m) + beta p_old on fluid cells
-// (pcg.cpp:113-122), Ap = d p_C + ox (p_L + p_R) + oy (p_B + p_T) (pcg.cpp:35-46)
-// from the new p of the neighbours, formed on the fly (a solid or out-of-domain
-// neighbour reads p_C), p.Ap reduced; the last block sets alpha = rz_old / p.Ap or
-// stops on breakdown (pcg.cpp:97-99).  FP64 evaluates the reference's expression on
-// its arrays; FP32 the difference form on FP32 copies (st.fs, fx, fy).
+// 2D search direction, the same fused step as the z march k_pmatvec (march.cuh):
+// p = (z - m) + beta p_old on fluid cells (pcg.cpp:113-122), Ap from the new p of
+// the neighbours, formed on the fly (a solid or out-of-domain neighbour reads p_C;
+// pcg.cpp:47-59), p.Ap reduced; the last block sets alpha = rz_old / p.Ap or stops
+// on breakdown (pcg.cpp:97-99).  The operator is the uniform one, or with st.vd the
+// variable-coefficient one, Ap = d p_C + ox (p_L + p_R) + oy (p_B + p_T)
+// (pcg.cpp:35-46).  FP64 evaluates the reference's expressions (on its arrays);
+// FP32 the difference forms (the variable one on FP32 copies st.fs, fx, fy).  In 2D
+// a march has a single plane to pipeline, and this flat walk is the faster kernel.
 // A thread owns the vertical pair (i, j), (i, j+1) -- j odd -- and a warp 32 such
 // columns; every load of a step (z and p_old of the pair, its side neighbours and
 // the rows below and above, codes, coefficients) is issued before any is used, the
@@ -580,13 +582,14 @@ __global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __rest
 // (the padded arrays hold them) and discarded by the neighbour rule.  p_old and
 // p_new are distinct buffers.
 template <class T>
-__global__ void __launch_bounds__(256) k_pmatvec_var(Geom g, const uint8_t* __restrict__ code,
+__global__ void __launch_bounds__(256) k_pmatvec_2d(Geom g, const uint8_t* __restrict__ code,
                                                      const T* __restrict__ z,
                                                      const T* __restrict__ pold,
                                                      T* __restrict__ pnew, T* __restrict__ ap,
                                                      Stencil st, double* partials, CGState* cg) {
     if (cg->done) return;
     const T m = (T)cg->mean_z, beta = (T)cg->beta;
+    const T idx2 = (T)st.idx2, idy2 = (T)st.idy2, diag = (T)st.diag;
     double acc[1] = {0.0};
     const int sx = g.sx;
     const int nxc = (g.nx + 31) >> 5;
@@ -611,8 +614,10 @@ __global__ void __launch_bounds__(256) k_pmatvec_var(Geom g, const uint8_t* __re
             qq[e] = pold[id + off[e]];
         }
         const uint32_t cc[2] = {code[id], code[id + sb]};
-        T k0[2], kx[2], ky[2];
-        if constexpr (sizeof(T) == 8) {
+        const bool var = st.vd != nullptr;  // the same for the whole launch
+        T k0[2] = {T(0), T(0)}, kx[2] = {T(0), T(0)}, ky[2] = {T(0), T(0)};
+        if (!var) {
+        } else if constexpr (sizeof(T) == 8) {
             const long long q = i + (long long)j * st.vsx, qb = hb ? st.vsx : 0;
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
@@ -648,7 +653,11 @@ __global__ void __launch_bounds__(256) k_pmatvec_var(Geom g, const uint8_t* __re
             const T vB = (c & 8u) ? pp[e] : (jj > 1 ? p0 : wall);
             const T vT = (c & 4u) ? pp[2 + e] : (jj < g.ny ? p0 : wall);
             T a;
-            if constexpr (sizeof(T) == 8) {
+            if (!var) {
+                // the march's expressions: the reference's in FP64, differences in FP32
+                a = sizeof(T) == 8 ? diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2
+                                   : ((p0 - vL) + (p0 - vR)) * idx2 + ((p0 - vB) + (p0 - vT)) * idy2;
+            } else if constexpr (sizeof(T) == 8) {
                 // the reference's expression and order
                 a = k0[e] * p0 + kx[e] * (vL + vR) + ky[e] * (vB + vT);
             } else {
