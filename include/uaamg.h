@@ -251,7 +251,7 @@ UAAMG_API uaamg_status uaamg_device_bytes(uaamg_handle* h, size_t* bytes);
 UAAMG_API const char* uaamg_last_error(uaamg_handle* h);
 UAAMG_API const char* uaamg_status_string(int status);
 
-/* ---- Batched uneven solves (uaamg_solve_batch) -------------------
+/* ---- Batched uneven solves (uaamg_solve_batch) ---------------------------------
  * One problem of a batch: HOST arrays in the reference layout of Grid / Grid3D
  * (include/core/mesh.h:35, mesh_3d.h:38), padded, column-major i-fastest.  p
  * follows Solver::solve (include/solver/solver.h:18-34): 0 on entry, or the
@@ -281,7 +281,7 @@ UAAMG_API uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_pro
  * No reference counterpart (the reference's kernels have fixed shapes). */
 UAAMG_API uaamg_status uaamg_set_autotune(uaamg_handle* h, int on);
 
-/* ---- Serving (uaamg_server_{start,submit,poll,stop}) ------------
+/* ---- Serving (uaamg_server_{start,submit,poll,stop}) --------------------------
  * A device-resident request loop on one GPU.  Requests carry a simulation id; the
  * server keeps each id's hierarchy and FP64 pressure on the device and
  * warm-starts the id's next request from it.  Requests are admitted while fewer

@@ -1,7 +1,7 @@
 // Test infrastructure only: a C-ABI shim around the reference's own CPU solver
 // classes, compiled together with the reference's unmodified source files by
 // oracle/Makefile into oracle/_ref/libuaamg_ref.so.  Nothing in the product links
-// this; tests, smoke() and the bench's CPU-baseline leg load it as the checker.
+// this; tests, smoke() and the bench's CPU-baseline leg load it as the oracle.
 //
 // Reference classes driven here:
 //   PCG / PCG3D                    src/solver/pcg.cpp:18-126, src/solver/pcg_3d.cpp:18-125

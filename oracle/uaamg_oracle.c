@@ -1,6 +1,6 @@
 /* Test infrastructure only — the oracle.  A plain-C restatement of the reference's
  * CPU UAAMG-preconditioned CG (A-006/UAAMGPCG), used by tests/, smoke() and the
- * bench's CPU-baseline leg as the checker.  The product never links it.
+ * bench's CPU-baseline leg as the oracle.  The product never links it.
  *
  * Every function follows a reference function line by line in ARITHMETIC ORDER
  * (loop nesting i→j→k for reductions, the same left-to-right sums), so that with
