@@ -1,7 +1,7 @@
 // Tensor-memory-accelerator (TMA) tile loads for the stencil kernels: host-side
 // tensor-map encoding of a level array in the pitched layout, and the device-side
 // mbarrier + cp.async.bulk.tensor sequence that stages a halo box in shared
-// memory.  Loads only, from this GPU's own memory, never with .multicast.
+// memory.  Loads only, each block fetching its own boxes from this GPU's own memory.
 //
 // Alignment rules honoured here (checked on the host before encoding):
 //   * array base 16-byte aligned (cudaMalloc: 256), row pitch a multiple of
