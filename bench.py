@@ -144,8 +144,48 @@ def _dist():
     return ws, rank, local
 
 
+def run_reference_gpu(args):
+    """The reference's own CUDA solver (CudaPCG3D::solve_optimized, FP64, and
+    solve_mixed, FP32 V-cycle; compiled unchanged for sm_100a into
+    oracle/_ref/libuaamg_ref_gpu.so) on the 256^3 workload on this GPU, rank 0 only:
+    one full solve a step, CUDA events around it.  Its result is checked with the
+    FP64 true residual on the host."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from uaamg_b200 import workloads
+
+    if not O.have_ref_gpu():
+        print(json.dumps({"impl": "reference-gpu",
+                          "unavailable": "oracle/_ref/libuaamg_ref_gpu.so not built"}))
+        return 0
+    solid, rhs, h = workloads.spheres_256()
+    out = {}
+    for name, mode in (("solve_optimized_fp64", 0), ("solve_mixed", 1)):
+        p, ms, it, rel = O.ref_gpu_pcg3d(solid, rhs, h, h, h, max_iter=500, tol=1e-6, mode=mode,
+                                         reps=args.steps)
+        res, bn = O.true_residual(solid, rhs, p, h, h, h)
+        out[name] = {"ms": round(ms, 3), "iterations": it, "reported_rel_residual": rel,
+                     "true_rel_residual": res / bn}
+    best = min(v["ms"] for v in out.values())
+    line = {
+        "impl": "reference-gpu", "metric": METRIC, "value": best, "unit": "ms",
+        "n_gpus": 1, "steps": args.steps, "warmup": 1, "higher_is_better": False,
+        "dtype": "f64 / f32 V-cycle", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "tol": 1e-6, "max_iter": 500,
+                   "solver": "reference CudaPCG3D (src/solver/cuda/cuda_pcg_3d_opt.cu)"},
+        "solves": out,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     """The reference's CPU PCG3D+UAAMG3D on the host cores (rank 0 only)."""
+    if getattr(args, "reference_gpu", False):
+        return run_reference_gpu(args)
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
@@ -771,6 +811,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="with --impl reference: time the reference's own CUDA solver "
+                         "(oracle/_ref/libuaamg_ref_gpu.so) on this GPU instead of its CPU one")
     ap.add_argument("--no-beside", action="store_true")
     ap.add_argument("--workload", default="spheres_256",
                     choices=["spheres_256", "obstacle_2d", "layered_2d", "batch96", "serve10k"])

@@ -8,6 +8,8 @@ Two libraries, both built by ``oracle/Makefile``:
 * ``_ref/libuaamg_ref.so`` -- the reference's OWN CPU source files compiled
   unchanged, behind ``ref_shim.cpp``.  Present only where the reference tree was
   available at build time (it then travels with the repository snapshot).
+* ``_ref/libuaamg_ref_gpu.so`` -- the reference's OWN CUDA 3D solver (CudaPCG3D)
+  compiled unchanged for sm_100a, behind ``ref_gpu_shim.cu`` (same conditions).
 
 Only tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
 this module.  Arrays are numpy, padded and column-major with i fastest, stored
@@ -24,6 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(HERE, "liboracle.so")
 _REF = os.path.join(HERE, "_ref", "libuaamg_ref.so")
+_REF_GPU = os.path.join(HERE, "_ref", "libuaamg_ref_gpu.so")
 
 _d = C.c_double
 _i = C.c_int
@@ -295,6 +298,40 @@ def smooth_cylinder(solid, dx, dy, cx, cy, r, tw=0.0, inside=False):
 
 
 # --- the reference itself (compiled from its own sources) -------------------
+
+
+def have_ref_gpu() -> bool:
+    return os.path.exists(_REF_GPU)
+
+
+_ref_gpu = None
+
+
+def ref_gpu_pcg3d(solid, rhs, dx, dy, dz, max_iter=500, tol=1e-6, mode=0, reps=1):
+    """The reference's CUDA CudaPCG3D on the current GPU: mode 0 solve_optimized (FP64),
+    1 solve_mixed (FP32 V-cycle); stop ||r|| / ||r0|| < tol.  One untimed solve, then
+    `reps` timed ones.  Returns (p, mean ms a solve, iterations, relative residual)."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not have_ref_gpu():
+            raise FileNotFoundError(f"{_REF_GPU} missing: run `make -C oracle ref-gpu` where "
+                                    "the reference tree is present")
+        _ref_gpu = _load(_REF_GPU)
+        _ref_gpu.ref_gpu_pcg3d.restype = _i
+        _ref_gpu.ref_gpu_pcg3d.argtypes = [_i, _i, _i, _d, _d, _d, _p, _p, _p, _i, _d, _i, _i,
+                                           C.POINTER(_d), C.POINTER(_i), C.POINTER(_d)]
+    solid = _c8(solid)
+    dim, nx, ny, nz = _dims(solid.shape)
+    if dim != 3:
+        raise ValueError("ref_gpu_pcg3d takes a 3D problem")
+    rhs = _cd(rhs)
+    p = np.zeros_like(rhs)
+    ms, it, rr = _d(), _i(), _d()
+    e = _ref_gpu.ref_gpu_pcg3d(nx, ny, nz, dx, dy, dz, _ptr(solid), _ptr(rhs), _ptr(p), max_iter,
+                               tol, mode, reps, C.byref(ms), C.byref(it), C.byref(rr))
+    if e != 0:
+        raise RuntimeError(f"reference GPU solve: CUDA error {e}")
+    return p, ms.value, it.value, rr.value
 
 
 def ref_pcg_var(solid, lap, rhs, dx, dy, max_iter=200, tol=1e-6, precond=True):

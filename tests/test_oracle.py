@@ -234,3 +234,13 @@ def test_layered_coefficients_generator():
     assert abs(np.sum(y * ax) - np.sum(x * ay)) <= 1e-12 * np.sum(np.abs(y * ax))
     one = np.where(fl, 1.0, 0.0)
     assert np.abs(O.matvec_var(solid, lap, one)).max() <= 1e-9 * np.abs(lap[0][fl]).max()
+
+
+@pytest.mark.skipif(not O.have_ref_gpu(), reason="reference CUDA solver (oracle/_ref) not built")
+def test_reference_gpu_library_loads_and_exports():
+    """The reference's own CUDA 3D solver, compiled for sm_100a behind ref_gpu_shim.cu,
+    loads without a GPU and exports its entry point (it runs only under
+    bench.py --impl reference --reference-gpu)."""
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libuaamg_ref_gpu.so"))
+    assert hasattr(lib, "ref_gpu_pcg3d")
