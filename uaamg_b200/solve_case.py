@@ -2,10 +2,12 @@
 Poisson problem with seeded solid spheres and a smoothed-noise right-hand side
 (the 256^3 benchmark problem at n = 256), through the C-ABI.  With
 --workload obstacle_2d --project: one device-side pressure projection (divergence,
-solve, face correction) of the 2048 x 1024 obstacle flow.
+solve, face correction) of the 2048 x 1024 obstacle flow; --workload layered_2d: the
+same grid solved with the variable-coefficient operator of a layered medium.
 
     python -m uaamg_b200.solve_case --n 256 --precision mixed --max-iter 90
     python -m uaamg_b200.solve_case --workload obstacle_2d --project
+    python -m uaamg_b200.solve_case --workload layered_2d --max-iter 10
 
 Prints one line with the status, iterations, FP64 true relative residual and the
 wall time of the solve.  Used as the profiling target of the kernel summaries
@@ -30,13 +32,16 @@ def main(argv=None):
     ap.add_argument("--max-iter", type=int, default=500)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--repeat", type=int, default=1)
-    ap.add_argument("--workload", default="spheres", choices=["spheres", "obstacle_2d"])
+    ap.add_argument("--workload", default="spheres",
+                    choices=["spheres", "obstacle_2d", "layered_2d"])
     ap.add_argument("--project", action="store_true")
     a = ap.parse_args(argv)
-    if a.workload == "obstacle_2d":
+    if a.workload in ("obstacle_2d", "layered_2d"):
         solid, u0, v0, rhs, dx, dy, dt = workloads.obstacle_2d()
         hd = Handle(0)
         hd.set_problem(solid, dx, dy)
+        if a.workload == "layered_2d":
+            hd.set_variable_laplacian(*workloads.layered_lap_2d(solid, dx, dy, 0.5))
         opts = hd.options(a.precision, a.tol, a.max_iter, "rel")
         for _ in range(a.repeat):
             p = np.zeros_like(rhs)
@@ -44,7 +49,7 @@ def main(argv=None):
             t0 = time.perf_counter()
             st = hd.project(u, v, None, p, dt, opts) if a.project else hd.solve(rhs, p, opts)
             ms = (time.perf_counter() - t0) * 1e3
-        print(json.dumps({"workload": "obstacle_2d", "project": a.project, "precision": a.precision,
+        print(json.dumps({"workload": a.workload, "project": a.project, "precision": a.precision,
                           "status": st.status, "iterations": st.iterations,
                           "true_rel_residual": st.rel_residual, "ms": round(ms, 3)}))
         hd.close()
