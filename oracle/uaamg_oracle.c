@@ -322,6 +322,40 @@ void oh_vcycle(oh_hier* h, const double* r, double* z) {
             }
 }
 
+/* oh_vcycle with the top level's intermediate states captured (for stage-by-stage
+ * checks of a finest-level implementation): x after the forward sweep, the coarse
+ * b after the restriction, the coarse solution before the prolongation, and z.
+ * Each pointer may be NULL; with a single level only z is written. */
+void oh_vcycle_stages(oh_hier* h, const double* r, double* x_fwd, double* b1, double* x1,
+                      double* z) {
+    olevel* L0 = &h->L[0];
+    for (int i = 1; i <= L0->nx; i++)
+        for (int j = 1; j <= L0->ny; j++)
+            for (int k = KLO(L0); k <= KHI(L0); k++) {
+                long id = cid(L0, i, j, k);
+                L0->b[id] = r[id];
+            }
+    for (int l = 0; l < h->nl; l++) {
+        memset(h->L[l].p, 0, sizeof(double) * (size_t)h->L[l].n);
+        if (l > 0) memset(h->L[l].b, 0, sizeof(double) * (size_t)h->L[l].n);
+    }
+    if (h->nl == 1) {
+        vcycle(h, 0);
+    } else {
+        olevel* C = &h->L[1];
+        smooth(L0, 0);
+        if (x_fwd) memcpy(x_fwd, L0->p, sizeof(double) * (size_t)L0->n);
+        restrict_residual(L0, C);
+        if (b1) memcpy(b1, C->b, sizeof(double) * (size_t)C->n);
+        memset(C->p, 0, sizeof(double) * (size_t)C->n);
+        vcycle(h, 1);
+        if (x1) memcpy(x1, C->p, sizeof(double) * (size_t)C->n);
+        prolongate_add(C, L0);
+        smooth(L0, 1);
+    }
+    if (z) memcpy(z, L0->p, sizeof(double) * (size_t)L0->n);
+}
+
 /* ------------------------------------------------------------------------- */
 /* PCG (pcg_3d.cpp:18-125, pcg.cpp:18-126)                                    */
 

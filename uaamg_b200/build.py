@@ -32,8 +32,8 @@ UNITS = [
     ("noalloc.cu", ["-fmad=false"]),
     ("project.cu", ["-fmad=false"]),
 ]
-HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "tail.cuh", "vec.cuh", "tma.cuh", "engine.cuh",
-           "engine.h", "handle.h"]
+HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "flat2d.cuh", "tail.cuh", "vec.cuh", "tma.cuh",
+           "engine.cuh", "engine.h", "handle.h"]
 
 
 def _nvcc() -> str:

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "flat2d.cuh"
 #include "kernels.cuh"
 #include "tail.cuh"
 #include "tma.cuh"
@@ -208,6 +209,16 @@ public:
     void set_graphs(bool on) override { graphs_ = on; }
     void set_autotune(bool on) override { autotune_ = on; }
     void set_small_levels(bool on) override { tail_on_ = on; }
+    void set_flat2d(bool on) override {
+        if (on == flat2d_) return;
+        if (gexec_) {  // a captured step holds the other kernels
+            cudaStreamSynchronize(st_);
+            cudaGraphExecDestroy(gexec_);
+            gexec_ = nullptr;
+        }
+        gkey_ = -1;
+        flat2d_ = on;
+    }
     void set_operator(const double* d, const double* ox, const double* oy, int sx,
                       long version) override {
         vver_ = version;
@@ -296,6 +307,7 @@ private:
     bool graphs_ = true;   // replay the PCG step as a CUDA graph
     bool autotune_ = false;  // time the marches' z-chunk lengths at set-up
     bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
+    bool flat2d_ = false;    // 2D finest level as flat walks (flat2d.cuh) instead of marches
     int tail_lt_ = 0;        // first level of the small-level kernel
     int tail_nc_ = 0;        // 1: the hierarchy has a tail (0: it does not fit the kernel)
     size_t tail_smem_ = 0;   // its dynamic shared memory (x and b of every tail level)
@@ -810,12 +822,31 @@ private:
         return m;
     }
 
+    // grid of a flat 2D walk (flat2d.cuh) over rows of `rows` items of 32 columns:
+    // eight rows a block, up to 8 blocks per SM (within the partials' capacity)
+    dim3 flat_grid(long long rows, int cols) const {
+        const long long items = rows * ((cols + 31) / 32);
+        long long nb = std::min<long long>((items + 7) / 8, 8LL * num_sms_);
+        nb = std::min<long long>(nb, reduce_blocks_);
+        return dim3((unsigned)(nb < 1 ? 1 : nb));
+    }
+
     template <int DIM, bool FINE>
     void down_level(int l, const int* done) {
         const LevelBuf<T, CS>& L = lv_[l];
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CS) + t;  // couplings + diagonal
+        if (DIM == 2 && FINE && flat2d_) {
+            // b (= r), code in; x out / b, x, code in; coarse b out
+            UAAMG_LAUNCH((KTag{K_FWD, l, c * (2.0 * t + 1.0)}), (k_fwd_flat2d<T, CS>),
+                         flat_grid((L.g.ny + 1) / 2, L.g.nx), dim3(32, 8), mlevel(l), L.code, r_,
+                         z_, done);
+            UAAMG_LAUNCH((KTag{K_RES, l, c * (2.0 * t + 1.0) + cc * t}), (k_res_flat2d<T, CS>),
+                         flat_grid(Cl.g.ny, Cl.g.nx), dim3(32, 8), mlevel(l), L.code, r_, z_,
+                         Cl.code, Cl.b, done);
+            return;
+        }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
         UAAMG_LAUNCH_SMEM((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_smooth<DIM, T, FINE, CS>),
@@ -832,6 +863,19 @@ private:
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CS) + t;  // couplings + diagonal
+        if (DIM == 2 && FINE && flat2d_) {
+            const dim3 fg = flat_grid((L.g.ny + 1) / 2, L.g.nx), fb(32, 8);
+            // b, code, coarse x in; x out / b, x, code in; odd x out
+            UAAMG_LAUNCH((KTag{K_UPE, l, c * (2.0 * t + 1.0) + cc * t}), (k_upe_flat2d<T, CS>), fg,
+                         fb, mlevel(l), L.code, r_, Cl.x, z_, done);
+            if (zdot)
+                UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0)}), (k_upo_flat2d<T, CS, true>), fg,
+                             fb, mlevel(l), L.code, r_, z_, done, partials_, cg_);
+            else
+                UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0)}), (k_upo_flat2d<T, CS, false>),
+                             fg, fb, mlevel(l), L.code, r_, z_, done, partials_, cg_);
+            return;
+        }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
         UAAMG_LAUNCH_SMEM((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),

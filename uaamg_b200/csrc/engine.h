@@ -87,6 +87,9 @@ public:
     // Marches: run the small levels and the coarsest solve as one single-block
     // kernel (default on; off: marches on every level).
     virtual void set_small_levels(bool on) = 0;
+    // 2D problems: the finest level's four V-cycle steps as flat walks over the level
+    // (flat2d.cuh) instead of z marches (default off).
+    virtual void set_flat2d(bool on) = 0;
     // 2D variable-coefficient outer-CG operator (the lap_diag / lap_off_x / lap_off_y
     // branch of PCG::solve, pcg.cpp:35-46): device arrays in the caller's padded
     // layout with row stride sx, read in place by every solve until changed;

@@ -1,0 +1,376 @@
+// The finest level of a 2D V-cycle as flat walks over the level (no TMA ring): the
+// four z marches of march.cuh -- forward sweep from x = 0, residual + restriction,
+// prolongation + even colour, odd colour (+ the CG's z sums) -- for a level that is
+// a single plane, where a march has nothing to pipeline.  Each kernel walks items
+// (vertical cell pairs (i, j), (i, j+1) with j odd, or coarse cells) grid-stride, a
+// warp over 32 consecutive columns, and issues every load of an item before using
+// any.  The per-item arithmetic is the march's finest-level arithmetic operand for
+// operand and in its order (march.cuh presmooth, nbsum, mdiag, fp32_ax, the
+// restriction's (di, dj) sum), written as __host__ __device__ functions so that a
+// host build of the same code can be checked against the oracle stage by stage; the
+// FP64 instantiation compiled with -fmad=false reproduces the reference bit for bit.
+//
+// Bounds: an item's reads stay in the padded level -- rows j-1 .. j+2 (the row above
+// the pair is clamped to j+1 when j = ny, whose row j+1 is the ghost row), columns
+// i-1 .. i+1, and for the prolongation the parents ((i+1)/2, (j+1)/2) of those
+// cells, at most (nx+2)/2 = cnx+1 and cny+1 (the coarse ghost ring).
+#pragma once
+#include <cstdint>
+#include <type_traits>
+
+#include "march.cuh"
+
+namespace uaamg {
+namespace {
+
+// num / d as the march's mdiv: the fast reciprocal in the mixed form (couplings
+// stored in FP16), IEEE division otherwise.  The host copy divides exactly and is
+// used for the FP64 and FP32 forms only.
+template <class T, class CS>
+__host__ __device__ __forceinline__ T f2_div(T num, T d) {
+#ifdef __CUDA_ARCH__
+    if constexpr (!std::is_same<CS, T>::value) return __fdividef(num, d);
+    else return num / d;
+#else
+    return num / d;
+#endif
+}
+
+// Finest-level diagonal of a cell with code c (the march's table entry, summed in
+// the reference's order +x, -x, +y, -y), plus the Dirichlet wall share.
+template <class T>
+__host__ __device__ __forceinline__ T f2_diag(const MLevel<T>& L, uint32_t c, int i, int j) {
+    T d = ((c & 1u) ? L.idx2 : T(0)) + ((c & 2u) ? L.idx2 : T(0)) + ((c & 4u) ? L.idy2 : T(0)) +
+          ((c & 8u) ? L.idy2 : T(0));
+    if (L.dirichlet) {
+        T w = T(0);
+        if (i == 1) w += T(2) * L.idx2;
+        if (i == L.g.nx) w += T(2) * L.idx2;
+        if (j == 1) w += T(2) * L.idy2;
+        if (j == L.g.ny) w += T(2) * L.idy2;
+        d = d + w;
+    }
+    return d;
+}
+
+// sum c_n v_n of a finest-level cell in the reference's order (+x, -x, +y, -y).
+template <class T>
+__host__ __device__ __forceinline__ T f2_nb(const MLevel<T>& L, T vr, T vl, T vt, T vb) {
+    return L.idx2 * vr + L.idx2 * vl + L.idy2 * vt + L.idy2 * vb;
+}
+
+// Pre-smoothed value of a cell from x = 0: (b + 0)/d for an active odd cell (0 when
+// d < 1e-30), 0 for every other cell.
+template <class T, class CS>
+__host__ __device__ __forceinline__ T f2_pre(const MLevel<T>& L, uint32_t c, T b, int i, int j) {
+    if ((c & (kActive | kOdd)) != (kActive | kOdd)) return T(0);
+    const T d = f2_diag(L, c, i, j);
+    if (d < T(1e-30)) return T(0);
+    return f2_div<T, CS>(b + T(0), d);
+}
+
+// A x of an active finest-level cell: the reference's expression in FP64, the sum of
+// couplings times differences in FP32 (as march.cuh fp32_ax).
+template <class T>
+__host__ __device__ __forceinline__ T f2_ax(const MLevel<T>& L, uint32_t c, T d, T x, T xr, T xl,
+                                            T xt, T xb) {
+    if constexpr (sizeof(T) == 8) {
+        return d * x - L.idx2 * xr - L.idx2 * xl - L.idy2 * xt - L.idy2 * xb;
+    } else {
+        const T tx = ((c & 1u) ? x - xr : T(0)) + ((c & 2u) ? x - xl : T(0));
+        const T ty = ((c & 4u) ? x - xt : T(0)) + ((c & 8u) ? x - xb : T(0));
+        const T ax = tx * L.idx2 + ty * L.idy2;
+        const T sum = ((c & 1u) ? L.idx2 : T(0)) + ((c & 2u) ? L.idx2 : T(0)) +
+                      ((c & 4u) ? L.idy2 : T(0)) + ((c & 8u) ? L.idy2 : T(0));
+        return ax + (d - sum) * x;
+    }
+}
+
+// The eight cells an item of a pair reads: 0 below A, 1 A = (i, j), 2 B = (i, j+1),
+// 3 above B (B again when j = ny), 4 / 5 left / right of A, 6 / 7 left / right of B.
+struct F2Pair {
+    int id;          // A's index
+    bool hb;         // B is an interior cell
+    int off[8];      // index offsets from A
+    int di[8], dj[8];
+};
+
+__host__ __device__ __forceinline__ F2Pair f2_pair(const Geom& g, int i, int j) {
+    F2Pair p;
+    const int sx = g.sx;
+    p.id = i + j * sx;
+    p.hb = j < g.ny;
+    const int s2 = p.hb ? 2 * sx : sx;
+    const int off[8] = {-sx, 0, sx, s2, -1, 1, sx - 1, sx + 1};
+    const int di[8] = {0, 0, 0, 0, -1, 1, -1, 1};
+    const int dj[8] = {-1, 0, 1, p.hb ? 2 : 1, 0, 0, 1, 1};
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        p.off[e] = off[e];
+        p.di[e] = di[e];
+        p.dj[e] = dj[e];
+    }
+    return p;
+}
+
+// Neighbour slots of the pair's cell e (0: A, 1: B) among the eight: +x, -x, +y, -y.
+__host__ __device__ __forceinline__ int f2_r(int e) { return e ? 7 : 5; }
+__host__ __device__ __forceinline__ int f2_l(int e) { return e ? 6 : 4; }
+__host__ __device__ __forceinline__ int f2_t(int e) { return e ? 3 : 2; }
+__host__ __device__ __forceinline__ int f2_b(int e) { return e ? 1 : 0; }
+
+// Forward sweep from x = 0 of one pair (k_fwd_smooth): the odd cell gets its
+// pre-smoothed value, the even cell (b + sum c_n x_n)/d from its odd neighbours'
+// pre-smoothed values (0 when inactive or d < 1e-30); x written on both cells.
+template <class T, class CS>
+__host__ __device__ __forceinline__ void f2_fwd_pair(const MLevel<T>& L, const uint8_t* code,
+                                                     const T* b, T* x, int i, int j) {
+    const F2Pair p = f2_pair(L.g, i, j);
+    uint32_t cc[8];
+    T bb[8], pv[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        cc[e] = code[p.id + p.off[e]];
+        bb[e] = b[p.id + p.off[e]];
+    }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) pv[e] = f2_pre<T, CS>(L, cc[e], bb[e], i + p.di[e], j + p.dj[e]);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        if (e == 1 && !p.hb) break;
+        const int s = 1 + e;
+        T v = T(0);
+        if ((i + j + e) & 1) {
+            v = pv[s];
+        } else if (cc[s] & kActive) {
+            const T d = f2_diag(L, cc[s], i, j + e);
+            if (!(d < T(1e-30)))
+                v = f2_div<T, CS>(bb[s] + f2_nb(L, pv[f2_r(e)], pv[f2_l(e)], pv[f2_t(e)], pv[f2_b(e)]),
+                                  d);
+        }
+        x[p.id + e * L.g.sx] = v;
+    }
+}
+
+// Residual b - A x of the four children of coarse cell (ic, jc) and their sum in the
+// reference's (di, dj) order (k_restrict_res); 0 for an inactive coarse cell.
+template <class T>
+__host__ __device__ __forceinline__ void f2_res_cell(const MLevel<T>& L, const uint8_t* code,
+                                                     const T* b, const T* x, const uint8_t* ccode,
+                                                     T* cb, int ic, int jc) {
+    const int sx = L.g.sx;
+    const int i0 = 2 * ic - 1, j0 = 2 * jc - 1;
+    const int id0 = i0 + j0 * sx;
+    // x on rows j0-1 .. j0+2 and columns i0-1 .. i0+2 (the corners unused)
+    T xv[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            xv[r][q] = ((r == 0 || r == 3) && (q == 0 || q == 3)) ? T(0)
+                                                                  : x[id0 + (r - 1) * sx + (q - 1)];
+    uint32_t c[2][2];
+    T bv[2][2];
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj) {
+            c[di][dj] = code[id0 + di + dj * sx];
+            bv[di][dj] = b[id0 + di + dj * sx];
+        }
+    const uint32_t cc = ccode[ic + jc * L.cg.sx];
+    T rv[2][2];
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj) {
+            rv[di][dj] = T(0);
+            if (c[di][dj] & kActive) {
+                const int r = 1 + dj, q = 1 + di;
+                const T d = f2_diag(L, c[di][dj], i0 + di, j0 + dj);
+                rv[di][dj] = bv[di][dj] - f2_ax(L, c[di][dj], d, xv[r][q], xv[r][q + 1], xv[r][q - 1],
+                                                xv[r + 1][q], xv[r - 1][q]);
+            }
+        }
+    T s = T(0);
+    s += rv[0][0];
+    s += rv[0][1];
+    s += rv[1][0];
+    s += rv[1][1];
+    cb[ic + jc * L.cg.sx] = (cc & kActive) ? s : T(0);
+}
+
+// Prolongation and the even colour of the reverse sweep for one pair (k_up_even):
+// an active odd cell holds its pre-smoothed value plus 2 x_parent, the even cell
+// (b + sum c_n x_n)/d from those (0 + 2 x_parent when d < 1e-30); inactive cells 0.
+template <class T, class CS>
+__host__ __device__ __forceinline__ void f2_upe_pair(const MLevel<T>& L, const uint8_t* code,
+                                                     const T* b, const T* xc, T* x, int i, int j) {
+    const F2Pair p = f2_pair(L.g, i, j);
+    const int csx = L.cg.sx;
+    uint32_t cc[8];
+    T bb[8], xp[8], ov[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        cc[e] = code[p.id + p.off[e]];
+        bb[e] = b[p.id + p.off[e]];
+        xp[e] = xc[((i + p.di[e] + 1) >> 1) + ((j + p.dj[e] + 1) >> 1) * csx];
+    }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        ov[e] = T(0);
+        if ((cc[e] & (kActive | kOdd)) == (kActive | kOdd)) {
+            const T d = f2_diag(L, cc[e], i + p.di[e], j + p.dj[e]);
+            const T pre = d < T(1e-30) ? T(0) : f2_div<T, CS>(bb[e] + T(0), d);
+            ov[e] = pre + T(2) * xp[e];
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        if (e == 1 && !p.hb) break;
+        const int s = 1 + e;
+        T v = T(0);
+        if ((i + j + e) & 1) {
+            v = ov[s];
+        } else if (cc[s] & kActive) {
+            const T d = f2_diag(L, cc[s], i, j + e);
+            if (d < T(1e-30))
+                v = T(0) + T(2) * xp[s];
+            else
+                v = f2_div<T, CS>(bb[s] + f2_nb(L, ov[f2_r(e)], ov[f2_l(e)], ov[f2_t(e)], ov[f2_b(e)]),
+                                  d);
+        }
+        x[p.id + e * L.g.sx] = v;
+    }
+}
+
+// The odd colour of the reverse sweep for one pair, in place (k_up_odd): the odd cell
+// reads only even neighbours, which nothing writes here.  With zdot, the fluid sums
+// of z (the cells' new x), r z and r (r = b) are added to acc.
+template <class T, class CS, bool ZDOT>
+__host__ __device__ __forceinline__ void f2_upo_pair(const MLevel<T>& L, const uint8_t* code,
+                                                     const T* b, T* x, int i, int j,
+                                                     double (&acc)[3]) {
+    const F2Pair p = f2_pair(L.g, i, j);
+    T xx[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) xx[e] = x[p.id + p.off[e]];
+    const uint32_t ca = code[p.id], cb = code[p.id + L.g.sx];
+    const T ba = b[p.id], bb = b[p.id + L.g.sx];
+    // the odd cell (A when i + j is odd) and its neighbours, selected without
+    // run-time indexing so that everything stays in registers
+    const bool ao = ((i + j) & 1) != 0;
+    const uint32_t co = ao ? ca : cb;
+    const T bo = ao ? ba : bb;
+    const T vr = ao ? xx[5] : xx[7], vl = ao ? xx[4] : xx[6];
+    const T vt = ao ? xx[2] : xx[3], vb = ao ? xx[0] : xx[1];
+    T za = xx[1], zb = xx[2];
+    if ((ao || p.hb) && (co & kActive)) {
+        const T d = f2_diag(L, co, i, ao ? j : j + 1);
+        if (!(d < T(1e-30))) {
+            const T v = f2_div<T, CS>(bo + f2_nb(L, vr, vl, vt, vb), d);
+            x[p.id + (ao ? 0 : L.g.sx)] = v;
+            if (ao) za = v;
+            else zb = v;
+        }
+    }
+    if (ZDOT) {
+        if (ca & kActive) {
+            const double zv = (double)za, rv = (double)ba;
+            acc[0] += zv;
+            acc[1] += rv * zv;
+            acc[2] += rv;
+        }
+        if ((cb & kActive) && p.hb) {
+            const double zv = (double)zb, rv = (double)bb;
+            acc[0] += zv;
+            acc[1] += rv * zv;
+            acc[2] += rv;
+        }
+    }
+}
+
+// ---- kernels: grid-stride walks over the items, (32, 8) blocks -------------------
+
+// Item `it` of a walk over rows of 32 items: (row, column).
+__device__ __forceinline__ void f2_item(long long it, int ncol, int& row, int& col) {
+    row = (int)(it / ncol);
+    col = (int)(it - (long long)row * ncol);
+}
+
+template <class T, class CS>
+__global__ void __launch_bounds__(256) k_fwd_flat2d(MLevel<T> L, const uint8_t* __restrict__ code,
+                                                    const T* __restrict__ b, T* __restrict__ x,
+                                                    const int* __restrict__ done) {
+    if (done && *done) return;
+    const int nxc = (L.g.nx + 31) >> 5;
+    const long long n = (long long)((L.g.ny + 1) >> 1) * nxc;
+    for (long long it = (long long)blockIdx.x * blockDim.y + threadIdx.y; it < n;
+         it += (long long)gridDim.x * blockDim.y) {
+        int pr, ch;
+        f2_item(it, nxc, pr, ch);
+        const int i = 1 + (ch << 5) + (int)threadIdx.x;
+        if (i <= L.g.nx) f2_fwd_pair<T, CS>(L, code, b, x, i, 1 + 2 * pr);
+    }
+}
+
+template <class T, class CS>
+__global__ void __launch_bounds__(256) k_res_flat2d(MLevel<T> L, const uint8_t* __restrict__ code,
+                                                    const T* __restrict__ b,
+                                                    const T* __restrict__ x,
+                                                    const uint8_t* __restrict__ ccode,
+                                                    T* __restrict__ cb, const int* __restrict__ done) {
+    if (done && *done) return;
+    const int ncx = (L.cg.nx + 31) >> 5;
+    const long long n = (long long)L.cg.ny * ncx;
+    for (long long it = (long long)blockIdx.x * blockDim.y + threadIdx.y; it < n;
+         it += (long long)gridDim.x * blockDim.y) {
+        int row, ch;
+        f2_item(it, ncx, row, ch);
+        const int ic = 1 + (ch << 5) + (int)threadIdx.x;
+        if (ic <= L.cg.nx) f2_res_cell<T>(L, code, b, x, ccode, cb, ic, 1 + row);
+    }
+}
+
+template <class T, class CS>
+__global__ void __launch_bounds__(256) k_upe_flat2d(MLevel<T> L, const uint8_t* __restrict__ code,
+                                                    const T* __restrict__ b,
+                                                    const T* __restrict__ xc, T* __restrict__ x,
+                                                    const int* __restrict__ done) {
+    if (done && *done) return;
+    const int nxc = (L.g.nx + 31) >> 5;
+    const long long n = (long long)((L.g.ny + 1) >> 1) * nxc;
+    for (long long it = (long long)blockIdx.x * blockDim.y + threadIdx.y; it < n;
+         it += (long long)gridDim.x * blockDim.y) {
+        int pr, ch;
+        f2_item(it, nxc, pr, ch);
+        const int i = 1 + (ch << 5) + (int)threadIdx.x;
+        if (i <= L.g.nx) f2_upe_pair<T, CS>(L, code, b, xc, x, i, 1 + 2 * pr);
+    }
+}
+
+// x is read and written in place (odd cells from even neighbours): not restrict.
+template <class T, class CS, bool ZDOT>
+__global__ void __launch_bounds__(256) k_upo_flat2d(MLevel<T> L, const uint8_t* __restrict__ code,
+                                                    const T* __restrict__ b, T* x,
+                                                    const int* __restrict__ done, double* partials,
+                                                    CGState* cg) {
+    if (done && *done) return;
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int nxc = (L.g.nx + 31) >> 5;
+    const long long n = (long long)((L.g.ny + 1) >> 1) * nxc;
+    for (long long it = (long long)blockIdx.x * blockDim.y + threadIdx.y; it < n;
+         it += (long long)gridDim.x * blockDim.y) {
+        int pr, ch;
+        f2_item(it, nxc, pr, ch);
+        const int i = 1 + (ch << 5) + (int)threadIdx.x;
+        if (i <= L.g.nx) f2_upo_pair<T, CS, ZDOT>(L, code, b, x, i, 1 + 2 * pr, acc);
+    }
+    if (ZDOT) {
+        double tot[3];
+        if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
+    }
+}
+
+}  // namespace
+}  // namespace uaamg

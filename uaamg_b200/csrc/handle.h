@@ -28,7 +28,8 @@ struct uaamg_handle {
     int last_iters = 0;
     uaamg::Engine* eng[3] = {nullptr, nullptr, nullptr};
     bool ready[3] = {false, false, false};
-    int sweeps = 0;  // V-cycle kernels: 0 marches + small-level kernel, 1 sweeps, 2 marches
+    int sweeps = 0;  // V-cycle kernels: 0 marches + small-level kernel, 1 sweeps, 2 marches,
+                     // 3 as 0 with a 2D finest level as flat walks
     int autotune = 0;
     std::string err;
     struct BatchPool* batch = nullptr;  // runtime.cpp: per-problem slots of uaamg_solve_batch

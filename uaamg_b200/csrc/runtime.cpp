@@ -189,7 +189,8 @@ uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_problem* prob
         int e = d.prepare(opts.precision, p.dim, p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, h->dirichlet);
         if (e == E_OK) {
             d.eng->set_vcycle_sweeps(h->sweeps == 1);
-            d.eng->set_small_levels(h->sweeps == 0);
+            d.eng->set_small_levels(h->sweeps == 0 || h->sweeps == 3);
+            d.eng->set_flat2d(h->sweeps == 3);
             d.eng->set_autotune(h->autotune != 0);
             e = d.build(p.solid);
         }
