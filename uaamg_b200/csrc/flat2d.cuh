@@ -113,11 +113,19 @@ __host__ __device__ __forceinline__ F2Pair f2_pair(const Geom& g, int i, int j) 
     return p;
 }
 
-// Neighbour slots of the pair's cell e (0: A, 1: B) among the eight: +x, -x, +y, -y.
-__host__ __device__ __forceinline__ int f2_r(int e) { return e ? 7 : 5; }
-__host__ __device__ __forceinline__ int f2_l(int e) { return e ? 6 : 4; }
-__host__ __device__ __forceinline__ int f2_t(int e) { return e ? 3 : 2; }
-__host__ __device__ __forceinline__ int f2_b(int e) { return e ? 1 : 0; }
+// Every thread owns one cell of each colour (A and B have opposite colours), so a
+// warp never splits on the red-black parity: the even cell of the pair is B when A
+// is odd ((i + j) odd), else A, and its four neighbours are odd.  Their slots among
+// the eight, selected by ao = "A is odd": +x 7 / 5, -x 6 / 4, +y 3 / 2, -y 1 / 0; the
+// pair's odd cell is the even cell's -y neighbour (A) or its +y neighbour (B).
+template <class V>
+__host__ __device__ __forceinline__ void f2_pick(bool ao, const V (&v)[8], V& r, V& l, V& t,
+                                                 V& b) {
+    r = ao ? v[7] : v[5];
+    l = ao ? v[6] : v[4];
+    t = ao ? v[3] : v[2];
+    b = ao ? v[1] : v[0];
+}
 
 // Forward sweep from x = 0 of one pair (k_fwd_smooth): the odd cell gets its
 // pre-smoothed value, the even cell (b + sum c_n x_n)/d from its odd neighbours'
@@ -126,30 +134,39 @@ template <class T, class CS>
 __host__ __device__ __forceinline__ void f2_fwd_pair(const MLevel<T>& L, const uint8_t* code,
                                                      const T* b, T* x, int i, int j) {
     const F2Pair p = f2_pair(L.g, i, j);
+    const bool ao = ((i + j) & 1) != 0;
     uint32_t cc[8];
-    T bb[8], pv[8];
+    T bb[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         cc[e] = code[p.id + p.off[e]];
         bb[e] = b[p.id + p.off[e]];
     }
+    int ci[8], cj[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) pv[e] = f2_pre<T, CS>(L, cc[e], bb[e], i + p.di[e], j + p.dj[e]);
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-        if (e == 1 && !p.hb) break;
-        const int s = 1 + e;
-        T v = T(0);
-        if ((i + j + e) & 1) {
-            v = pv[s];
-        } else if (cc[s] & kActive) {
-            const T d = f2_diag(L, cc[s], i, j + e);
-            if (!(d < T(1e-30)))
-                v = f2_div<T, CS>(bb[s] + f2_nb(L, pv[f2_r(e)], pv[f2_l(e)], pv[f2_t(e)], pv[f2_b(e)]),
-                                  d);
-        }
-        x[p.id + e * L.g.sx] = v;
+    for (int e = 0; e < 8; ++e) {
+        ci[e] = i + p.di[e];
+        cj[e] = j + p.dj[e];
     }
+    // the even cell's four odd neighbours: codes, b and coordinates
+    uint32_t cr, cl, ct, cb;
+    T br, bl, bt, bbm;
+    int ir, il, it, ib, jr, jl, jt, jb;
+    f2_pick(ao, cc, cr, cl, ct, cb);
+    f2_pick(ao, bb, br, bl, bt, bbm);
+    f2_pick(ao, ci, ir, il, it, ib);
+    f2_pick(ao, cj, jr, jl, jt, jb);
+    const T pr = f2_pre<T, CS>(L, cr, br, ir, jr), pl = f2_pre<T, CS>(L, cl, bl, il, jl);
+    const T pt = f2_pre<T, CS>(L, ct, bt, it, jt), pb = f2_pre<T, CS>(L, cb, bbm, ib, jb);
+    const T vo = ao ? pb : pt;  // the pair's odd cell
+    const uint32_t ce = ao ? cc[2] : cc[1];
+    T ve = T(0);
+    if (ce & kActive) {
+        const T d = f2_diag(L, ce, i, ao ? j + 1 : j);
+        if (!(d < T(1e-30))) ve = f2_div<T, CS>((ao ? bb[2] : bb[1]) + f2_nb(L, pr, pl, pt, pb), d);
+    }
+    x[p.id] = ao ? vo : ve;
+    if (p.hb) x[p.id + L.g.sx] = ao ? ve : vo;
 }
 
 // Residual b - A x of the four children of coarse cell (ic, jc) and their sum in the
@@ -208,40 +225,47 @@ __host__ __device__ __forceinline__ void f2_upe_pair(const MLevel<T>& L, const u
                                                      const T* b, const T* xc, T* x, int i, int j) {
     const F2Pair p = f2_pair(L.g, i, j);
     const int csx = L.cg.sx;
+    const bool ao = ((i + j) & 1) != 0;
     uint32_t cc[8];
-    T bb[8], xp[8], ov[8];
+    T bb[8], xp[8];
+    int ci[8], cj[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
+        ci[e] = i + p.di[e];
+        cj[e] = j + p.dj[e];
         cc[e] = code[p.id + p.off[e]];
         bb[e] = b[p.id + p.off[e]];
-        xp[e] = xc[((i + p.di[e] + 1) >> 1) + ((j + p.dj[e] + 1) >> 1) * csx];
+        xp[e] = xc[((ci[e] + 1) >> 1) + ((cj[e] + 1) >> 1) * csx];
     }
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-        ov[e] = T(0);
-        if ((cc[e] & (kActive | kOdd)) == (kActive | kOdd)) {
-            const T d = f2_diag(L, cc[e], i + p.di[e], j + p.dj[e]);
-            const T pre = d < T(1e-30) ? T(0) : f2_div<T, CS>(bb[e] + T(0), d);
-            ov[e] = pre + T(2) * xp[e];
-        }
+    // odd value of a cell: pre-smoothed + prolongation when active and odd, else 0
+    auto oddval = [&](uint32_t c, T bv, T xpv, int ii, int jj) -> T {
+        if ((c & (kActive | kOdd)) != (kActive | kOdd)) return T(0);
+        const T d = f2_diag(L, c, ii, jj);
+        const T pre = d < T(1e-30) ? T(0) : f2_div<T, CS>(bv + T(0), d);
+        return pre + T(2) * xpv;
+    };
+    uint32_t cr, cl, ct, cb;
+    T br, bl, bt, bbm, xr, xl, xt, xbm;
+    int ir, il, it, ib, jr, jl, jt, jb;
+    f2_pick(ao, cc, cr, cl, ct, cb);
+    f2_pick(ao, bb, br, bl, bt, bbm);
+    f2_pick(ao, xp, xr, xl, xt, xbm);
+    f2_pick(ao, ci, ir, il, it, ib);
+    f2_pick(ao, cj, jr, jl, jt, jb);
+    const T orr = oddval(cr, br, xr, ir, jr), ol = oddval(cl, bl, xl, il, jl);
+    const T ot = oddval(ct, bt, xt, it, jt), ob = oddval(cb, bbm, xbm, ib, jb);
+    const T vo = ao ? ob : ot;  // the pair's odd cell
+    const uint32_t ce = ao ? cc[2] : cc[1];
+    T ve = T(0);
+    if (ce & kActive) {
+        const T d = f2_diag(L, ce, i, ao ? j + 1 : j);
+        if (d < T(1e-30))
+            ve = T(0) + T(2) * (ao ? xp[2] : xp[1]);
+        else
+            ve = f2_div<T, CS>((ao ? bb[2] : bb[1]) + f2_nb(L, orr, ol, ot, ob), d);
     }
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-        if (e == 1 && !p.hb) break;
-        const int s = 1 + e;
-        T v = T(0);
-        if ((i + j + e) & 1) {
-            v = ov[s];
-        } else if (cc[s] & kActive) {
-            const T d = f2_diag(L, cc[s], i, j + e);
-            if (d < T(1e-30))
-                v = T(0) + T(2) * xp[s];
-            else
-                v = f2_div<T, CS>(bb[s] + f2_nb(L, ov[f2_r(e)], ov[f2_l(e)], ov[f2_t(e)], ov[f2_b(e)]),
-                                  d);
-        }
-        x[p.id + e * L.g.sx] = v;
-    }
+    x[p.id] = ao ? vo : ve;
+    if (p.hb) x[p.id + L.g.sx] = ao ? ve : vo;
 }
 
 // The odd colour of the reverse sweep for one pair, in place (k_up_odd): the odd cell
