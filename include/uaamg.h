@@ -142,7 +142,7 @@ UAAMG_API uaamg_status uaamg_set_dirichlet_walls(uaamg_handle* h, int on);
  * 1 = one kernel per colour sweep, restriction and prolongation, step by step as
  * UAAMGPreconditioner3D::vCycle (uaamg_preconditioner_3d.cpp:183-196);
  * 2 = z marches on every level and a separate coarsest-level kernel;
- * 3 = as 0, with the finest level of a 2D problem as four flat walks over the level
+ * 3 = as 0, with every march level of a 2D problem as four flat walks over the level
  * instead of marches (a 2D level is one plane: nothing to pipeline).
  * All give identical results in FP64; 1 and 2 exist to cross-check 0. */
 UAAMG_API uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps);

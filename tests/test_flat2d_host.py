@@ -1,13 +1,16 @@
-"""The flat 2D finest-level V-cycle steps (uaamg_b200/csrc/flat2d.cuh) built for the
-host and checked against the oracle's V-cycle stage by stage, on the CPU:
+"""The flat 2D V-cycle steps (uaamg_b200/csrc/flat2d.cuh) built for the host and
+checked against the oracle's V-cycle stage by stage, on the CPU, on every level that
+runs as marches (the finest, with couplings from the cell codes, and the coarse ones,
+with their stored Galerkin couplings and diagonal):
 
-  forward sweep from x = 0         == the oracle's level-0 x after smooth(forward)
-  residual + restriction           == its level-1 b after restrict_residual
-  prolongation + reverse sweep     == its final z, given its level-1 solution
+  forward sweep from x = 0         == the oracle's x after smooth(forward)
+  residual + restriction           == the next level's b after restrict_residual
+  prolongation + reverse sweep     == the level's x on exit, given the next level's x
 
 bit for bit in FP64 (the GPU instantiation is compiled with -fmad=false and uses the
 same functions); FP32 within 1e-5 relative of the FP64 stages.  The CG's z sums of the
-odd-colour step are checked against numpy.  Needs nvcc (the header is CUDA source).
+finest level's odd-colour step are checked against numpy.  Needs nvcc (the header is
+CUDA source).
 """
 import ctypes as C
 import os
@@ -38,14 +41,9 @@ def f2h(tmp_path_factory):
     lib = C.CDLL(out)
     p, i, d = C.c_void_p, C.c_int, C.c_double
     for t in ("f64", "f32"):
-        getattr(lib, f"f2h_fwd_{t}").argtypes = [i, i, d, d, i, p, p, p]
-        getattr(lib, f"f2h_res_{t}").argtypes = [i, i, i, i, d, d, i, p, p, p, p, p]
-        getattr(lib, f"f2h_up_{t}").argtypes = [i, i, i, i, d, d, i, p, p, p, p, p]
+        getattr(lib, f"f2h_step_{t}").argtypes = [i, i, i, i, i, i, d, d, i, p, p, p, p, p, p, p,
+                                                  p, p, p]
     return lib
-
-
-def _p(a):
-    return a.ctypes.data_as(C.c_void_p)
 
 
 def codes(solid, fine=True):
@@ -85,49 +83,68 @@ def case(seed):
     return solid, r, dx, dy, seed % 4 == 3
 
 
+def run(f2h, t, step, lvl, b, x=None, ccode=None, cb=None, xc=None):
+    """One flat step on level `lvl` (a dict of the level's data) in type t."""
+    dt = np.float64 if t == "f64" else np.float32
+    cast = (lambda a: None if a is None else np.ascontiguousarray(a, dtype=dt))
+    dg, cx, cy = (cast(a) for a in lvl["op"])
+    b = cast(b)
+    x = cast(x) if x is not None else np.zeros(b.shape, dt)
+    cb = cast(cb) if cb is not None else None
+    xc = cast(xc)
+    sums = np.zeros(3)
+    getattr(f2h, f"f2h_step_{t}")(step, int(lvl["fine"]), lvl["nx"], lvl["ny"], lvl["cnx"],
+                                  lvl["cny"], lvl["dx"], lvl["dy"], lvl["dir"], _p(dg), _p(cx),
+                                  _p(cy), _p(lvl["code"]), _p(b), _p(x), _p(ccode), _p(cb),
+                                  _p(xc), _p(sums))
+    return x, cb, sums
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
 @pytest.mark.parametrize("seed", range(12))
 def test_flat2d_steps_equal_oracle_stages(f2h, seed):
+    """Every level that runs as marches: the finest (couplings from the codes, the
+    CG's z sums) and the coarse ones (stored Galerkin couplings and diagonal)."""
     solid, r, dx, dy, dirichlet = case(seed)
-    ny, nx = solid.shape[0] - 2, solid.shape[1] - 2
     H = O.Hierarchy(solid, dx, dy, 1.0, dirichlet=dirichlet)
     if H.nlevels < 2:
-        pytest.skip("a single level: no finest-level marches")
-    x_fwd, b1, x1, z = H.vcycle_stages(r)
-    cny, cnx = b1.shape[0] - 2, b1.shape[1] - 2
-    c0 = codes(solid)
-    c1 = codes(H.level_solid(1), fine=False)
-    dr = int(dirichlet)
+        pytest.skip("a single level: no marches")
     inner = (slice(1, -1), slice(1, -1))
+    for l in range(H.nlevels - 1):
+        b_l, x_fwd, b1, x1, x_out = H.vcycle_stages(r, l)
+        nx, ny, _ = H.dims(l)
+        cnx, cny, _ = H.dims(l + 1)
+        sl = H.level_solid(l)
+        cx, cy, _, dg = H.level_coeffs(l)
+        lvl = dict(fine=l == 0, nx=nx, ny=ny, cnx=cnx, cny=cny, dx=dx, dy=dy,
+                   dir=int(dirichlet and l == 0), code=codes(sl, fine=l == 0),
+                   op=(dg, cx, cy) if l > 0 else (None, None, None))
+        c1 = codes(H.level_solid(l + 1), fine=False)
 
-    # FP64: bit for bit
-    x = np.zeros_like(r)
-    f2h.f2h_fwd_f64(nx, ny, dx, dy, dr, _p(c0), _p(r), _p(x))
-    assert np.array_equal(x[inner], x_fwd[inner])
-    cb = np.zeros_like(b1)
-    f2h.f2h_res_f64(nx, ny, cnx, cny, dx, dy, dr, _p(c0), _p(r), _p(x_fwd), _p(c1), _p(cb))
-    assert np.array_equal(cb[inner], b1[inner])
-    xu = np.zeros_like(r)
-    sums = np.zeros(3)
-    f2h.f2h_up_f64(nx, ny, cnx, cny, dx, dy, dr, _p(c0), _p(r), _p(x1), _p(xu), _p(sums))
-    assert np.array_equal(xu[inner], z[inner])
-    fl = np.zeros(solid.shape, bool)
-    fl[inner] = solid[inner] == 0
-    want = np.array([z[fl].sum(), (r[fl] * z[fl]).sum(), r[fl].sum()])
-    np.testing.assert_allclose(sums, want, rtol=1e-10, atol=1e-10 * np.abs(z[fl]).sum())
+        # FP64: bit for bit
+        x, _, _ = run(f2h, "f64", 0, lvl, b_l)
+        assert np.array_equal(x[inner], x_fwd[inner]), f"level {l}: forward sweep"
+        _, cb, _ = run(f2h, "f64", 1, lvl, b_l, x=x_fwd, ccode=c1, cb=np.zeros_like(b1))
+        assert np.array_equal(cb[inner], b1[inner]), f"level {l}: restriction"
+        xu, _, sums = run(f2h, "f64", 2, lvl, b_l, xc=x1)
+        assert np.array_equal(xu[inner], x_out[inner]), f"level {l}: prolongation + reverse sweep"
+        if l == 0:
+            fl = np.zeros(solid.shape, bool)
+            fl[inner] = solid[inner] == 0
+            z = x_out
+            want = np.array([z[fl].sum(), (r[fl] * z[fl]).sum(), r[fl].sum()])
+            np.testing.assert_allclose(sums, want, rtol=1e-10, atol=1e-10 * np.abs(z[fl]).sum())
 
-    # FP32: the same steps from the FP64 stages' inputs, within FP32 rounding
-    def rel(a, b):
-        return np.linalg.norm(a[inner] - b[inner]) / max(np.linalg.norm(b[inner]), 1e-300)
+        # FP32: the same steps from the FP64 stages' inputs, within FP32 rounding
+        def rel(a, b):
+            return np.linalg.norm(a[inner] - b[inner]) / max(np.linalg.norm(b[inner]), 1e-300)
 
-    r32 = r.astype(np.float32)
-    x32 = np.zeros_like(r32)
-    f2h.f2h_fwd_f32(nx, ny, dx, dy, dr, _p(c0), _p(r32), _p(x32))
-    assert rel(x32.astype(np.float64), x_fwd) <= 1e-5
-    cb32 = np.zeros(b1.shape, np.float32)
-    xf32 = x_fwd.astype(np.float32)
-    f2h.f2h_res_f32(nx, ny, cnx, cny, dx, dy, dr, _p(c0), _p(r32), _p(xf32), _p(c1), _p(cb32))
-    assert rel(cb32.astype(np.float64), b1) <= 1e-4
-    xu32 = np.zeros_like(r32)
-    x132 = x1.astype(np.float32)
-    f2h.f2h_up_f32(nx, ny, cnx, cny, dx, dy, dr, _p(c0), _p(r32), _p(x132), _p(xu32), _p(sums))
-    assert rel(xu32.astype(np.float64), z) <= 1e-5
+        x, _, _ = run(f2h, "f32", 0, lvl, b_l)
+        assert rel(x.astype(np.float64), x_fwd) <= 1e-5
+        _, cb, _ = run(f2h, "f32", 1, lvl, b_l, x=x_fwd, ccode=c1, cb=np.zeros_like(b1))
+        assert rel(cb.astype(np.float64), b1) <= 1e-4
+        xu, _, _ = run(f2h, "f32", 2, lvl, b_l, xc=x1)
+        assert rel(xu.astype(np.float64), x_out) <= 1e-5

@@ -822,6 +822,15 @@ private:
         return m;
     }
 
+    // The coarse operator of level l as the flat 2D walks read it (flat2d.cuh).
+    F2Op<T, CS> flat_op(int l) const {
+        F2Op<T, CS> op;
+        op.dg = l > 0 ? lv_[l].dg : nullptr;
+        op.cx = l > 0 ? lv_[l].hcx : nullptr;
+        op.cy = l > 0 ? lv_[l].hcy : nullptr;
+        return op;
+    }
+
     // grid of a flat 2D walk (flat2d.cuh) over rows of `rows` items of 32 columns:
     // eight rows a block, up to 8 blocks per SM (within the partials' capacity)
     dim3 flat_grid(long long rows, int cols) const {
@@ -837,14 +846,18 @@ private:
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CS) + t;  // couplings + diagonal
-        if (DIM == 2 && FINE && flat2d_) {
-            // b (= r), code in; x out / b, x, code in; coarse b out
-            UAAMG_LAUNCH((KTag{K_FWD, l, c * (2.0 * t + 1.0)}), (k_fwd_flat2d<T, CS>),
-                         flat_grid((L.g.ny + 1) / 2, L.g.nx), dim3(32, 8), mlevel(l), L.code, r_,
-                         z_, done);
-            UAAMG_LAUNCH((KTag{K_RES, l, c * (2.0 * t + 1.0) + cc * t}), (k_res_flat2d<T, CS>),
-                         flat_grid(Cl.g.ny, Cl.g.nx), dim3(32, 8), mlevel(l), L.code, r_, z_,
-                         Cl.code, Cl.b, done);
+        if (DIM == 2 && flat2d_) {
+            // b, code (coarse levels: couplings, diagonal) in; x out / b, x, code in;
+            // coarse b out
+            const F2Op<T, CS> op = flat_op(l);
+            T* b = l == 0 ? r_ : L.b;
+            T* x = l == 0 ? z_ : L.x;
+            UAAMG_LAUNCH((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_flat2d<T, CS, FINE>),
+                         flat_grid((L.g.ny + 1) / 2, L.g.nx), dim3(32, 8), mlevel(l), op, L.code, b,
+                         x, done);
+            UAAMG_LAUNCH((KTag{K_RES, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
+                         (k_res_flat2d<T, CS, FINE>), flat_grid(Cl.g.ny, Cl.g.nx), dim3(32, 8),
+                         mlevel(l), op, L.code, b, x, Cl.code, Cl.b, done);
             return;
         }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
@@ -863,17 +876,22 @@ private:
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CS) + t;  // couplings + diagonal
-        if (DIM == 2 && FINE && flat2d_) {
+        if (DIM == 2 && flat2d_) {
             const dim3 fg = flat_grid((L.g.ny + 1) / 2, L.g.nx), fb(32, 8);
+            const F2Op<T, CS> op = flat_op(l);
+            T* b = l == 0 ? r_ : L.b;
+            T* x = l == 0 ? z_ : L.x;
             // b, code, coarse x in; x out / b, x, code in; odd x out
-            UAAMG_LAUNCH((KTag{K_UPE, l, c * (2.0 * t + 1.0) + cc * t}), (k_upe_flat2d<T, CS>), fg,
-                         fb, mlevel(l), L.code, r_, Cl.x, z_, done);
-            if (zdot)
-                UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0)}), (k_upo_flat2d<T, CS, true>), fg,
-                             fb, mlevel(l), L.code, r_, z_, done, partials_, cg_);
+            UAAMG_LAUNCH((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
+                         (k_upe_flat2d<T, CS, FINE>), fg, fb, mlevel(l), op, L.code, b, Cl.x, x, done);
+            if (FINE && zdot)
+                UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
+                             (k_upo_flat2d<T, CS, FINE, true>), fg, fb, mlevel(l), op, L.code, b, x,
+                             done, partials_, cg_);
             else
-                UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0)}), (k_upo_flat2d<T, CS, false>),
-                             fg, fb, mlevel(l), L.code, r_, z_, done, partials_, cg_);
+                UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
+                             (k_upo_flat2d<T, CS, FINE, false>), fg, fb, mlevel(l), op, L.code, b, x,
+                             done, partials_, cg_);
             return;
         }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);

@@ -87,8 +87,8 @@ public:
     // Marches: run the small levels and the coarsest solve as one single-block
     // kernel (default on; off: marches on every level).
     virtual void set_small_levels(bool on) = 0;
-    // 2D problems: the finest level's four V-cycle steps as flat walks over the level
-    // (flat2d.cuh) instead of z marches (default off).
+    // 2D problems: the four V-cycle steps of every march level as flat walks over the
+    // level (flat2d.cuh) instead of z marches (default off).
     virtual void set_flat2d(bool on) = 0;
     // 2D variable-coefficient outer-CG operator (the lap_diag / lap_off_x / lap_off_y
     // branch of PCG::solve, pcg.cpp:35-46): device arrays in the caller's padded

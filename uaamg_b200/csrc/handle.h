@@ -29,7 +29,7 @@ struct uaamg_handle {
     uaamg::Engine* eng[3] = {nullptr, nullptr, nullptr};
     bool ready[3] = {false, false, false};
     int sweeps = 0;  // V-cycle kernels: 0 marches + small-level kernel, 1 sweeps, 2 marches,
-                     // 3 as 0 with a 2D finest level as flat walks
+                     // 3 as 0 with 2D march levels as flat walks
     int autotune = 0;
     std::string err;
     struct BatchPool* batch = nullptr;  // runtime.cpp: per-problem slots of uaamg_solve_batch

@@ -131,7 +131,7 @@ class Handle:
     def set_vcycle_kernels(self, mode):
         """0 / False: z marches + the single-block small-level kernel (default);
         1 / True: per-colour sweep kernels; 2: z marches on every level; 3: as 0 with
-        the finest level of a 2D problem as flat walks."""
+        every march level of a 2D problem as flat walks."""
         self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(mode)), "vcycle")
 
     def set_variable_laplacian(self, lap_diag=None, lap_off_x=None, lap_off_y=None):
