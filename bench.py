@@ -274,6 +274,7 @@ def run_ours(args):
     h = dx
     hd = Handle(device)
     hd.set_autotune(bool(args.autotune))  # set-up only: chunk lengths timed before the solve
+    hd.set_vcycle_kernels(args.vcycle_kernels)
     hd.set_problem(solid, dx, dy, dz)
     if lap is not None:
         hd.set_variable_laplacian(*lap)
@@ -479,7 +480,7 @@ def run_ours(args):
                    "iterations": stats["iterations"],
                    "true_rel_residual": stats["rel_residual"],
                    "host_checked_rel_residual": res / bn,
-                   "autotune": bool(args.autotune),
+                   "autotune": bool(args.autotune), "vcycle_kernels": args.vcycle_kernels,
                    "l2": f"inputs larger than L2 (solve working set ~{hd.device_bytes() / 1e9:.2f} GB "
                          "vs 126 MB L2)",
                    "parallelism": f"replicas x{ws}"},
@@ -537,6 +538,7 @@ def run_batch(args):
     hd = Handle(device)
     if args.autotune:
         hd.set_autotune(True)
+    hd.set_vcycle_kernels(args.vcycle_kernels)
     opts = hd.options(args.precision, 1e-6, 500, "rel")
     ps = [np.zeros_like(r) for _, r, *_ in probs]
     items = [(s, r, p, dx, dy, dz) for (s, r, dx, dy, dz), p in zip(probs, ps)]
@@ -606,6 +608,7 @@ def run_batch(args):
         "config": {"workload": "batch96: 64 2D (sizes {64..1024}^2) + 32 3D (sizes {32..128}^3) "
                                "box-obstacle problems, smoothed-noise RHS (seed 20260404)",
                    "precision": args.precision, "cells": cells, "autotune": bool(args.autotune),
+                   "vcycle_kernels": args.vcycle_kernels,
                    "solves_per_s": round(96 / (ms * 1e-3), 1),
                    "iterations_min_median_max": [min(iters), int(statistics.median(iters)), max(iters)],
                    "worst_true_rel_residual": worst,
@@ -820,6 +823,8 @@ def main():
     ap.add_argument("--autotune", dest="autotune", action="store_true", default=True,
                     help="time the marches' z-chunk lengths at set-up (default on; outside the timing)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
+    ap.add_argument("--vcycle-kernels", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="uaamg_set_vcycle_kernels mode (0 default; 3: 2D levels as flat walks)")
     ap.add_argument("--serve-ids", type=int, default=500)
     ap.add_argument("--serve-steps", type=int, default=20)
     ap.add_argument("--serve-active", type=int, default=16)

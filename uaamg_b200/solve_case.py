@@ -35,10 +35,12 @@ def main(argv=None):
     ap.add_argument("--workload", default="spheres",
                     choices=["spheres", "obstacle_2d", "layered_2d"])
     ap.add_argument("--project", action="store_true")
+    ap.add_argument("--vcycle-kernels", type=int, default=0, choices=[0, 1, 2, 3])
     a = ap.parse_args(argv)
     if a.workload in ("obstacle_2d", "layered_2d"):
         solid, u0, v0, rhs, dx, dy, dt = workloads.obstacle_2d()
         hd = Handle(0)
+        hd.set_vcycle_kernels(a.vcycle_kernels)
         hd.set_problem(solid, dx, dy)
         if a.workload == "layered_2d":
             hd.set_variable_laplacian(*workloads.layered_lap_2d(solid, dx, dy, 0.5))
@@ -61,6 +63,7 @@ def main(argv=None):
         solid, rhs = workloads.spheres_3d(a.n, a.n, a.n, 32, 8.0 * r, 24.0 * r)
         h = 1.0 / a.n
     hd = Handle(0)
+    hd.set_vcycle_kernels(a.vcycle_kernels)
     hd.set_problem(solid, h, h, h)
     opts = hd.options(a.precision, a.tol, a.max_iter, "rel")
     for _ in range(a.repeat):
