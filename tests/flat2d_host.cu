@@ -37,24 +37,25 @@ MLevel<T> level(int nx, int ny, int cnx, int cny, double dx, double dy, int diri
     return L;
 }
 
-template <class T, bool FINE>
-void run(int step, const MLevel<T>& L, const F2Op<T, T>& op, const uint8_t* code, const T* b, T* x,
-         const uint8_t* ccode, T* cb, const T* xc, double* sums) {
+template <class T, class CS, bool FINE>
+void run(int step, const MLevel<T>& L, const F2Op<T, CS>& op, const uint8_t* code, const T* b,
+         T* x, const uint8_t* ccode, T* cb, const T* xc, double* sums) {
     if (step == 0) {
         for (int j = 1; j <= L.g.ny; j += 2)
-            for (int i = 1; i <= L.g.nx; ++i) uaamg::f2_fwd_pair<T, T, FINE>(L, op, code, b, x, i, j);
+            for (int i = 1; i <= L.g.nx; ++i)
+                uaamg::f2_fwd_pair<T, CS, FINE>(L, op, code, b, x, i, j);
     } else if (step == 1) {
         for (int jc = 1; jc <= L.cg.ny; ++jc)
             for (int ic = 1; ic <= L.cg.nx; ++ic)
-                uaamg::f2_res_cell<T, T, FINE>(L, op, code, b, x, ccode, cb, ic, jc);
+                uaamg::f2_res_cell<T, CS, FINE>(L, op, code, b, x, ccode, cb, ic, jc);
     } else {
         for (int j = 1; j <= L.g.ny; j += 2)
             for (int i = 1; i <= L.g.nx; ++i)
-                uaamg::f2_upe_pair<T, T, FINE>(L, op, code, b, xc, x, i, j);
+                uaamg::f2_upe_pair<T, CS, FINE>(L, op, code, b, xc, x, i, j);
         double acc[3] = {0.0, 0.0, 0.0};
         for (int j = 1; j <= L.g.ny; j += 2)
             for (int i = 1; i <= L.g.nx; ++i)
-                uaamg::f2_upo_pair<T, T, FINE, true>(L, op, code, b, x, i, j, acc);
+                uaamg::f2_upo_pair<T, CS, FINE, true>(L, op, code, b, x, i, j, acc);
         for (int q = 0; q < 3; ++q) sums[q] = acc[q];
     }
 }
@@ -68,8 +69,8 @@ void step_t(int step, int fine, int nx, int ny, int cnx, int cny, double dx, dou
     op.dg = dg;
     op.cx = cx;
     op.cy = cy;
-    if (fine) run<T, true>(step, L, op, code, b, x, ccode, cb, xc, sums);
-    else run<T, false>(step, L, op, code, b, x, ccode, cb, xc, sums);
+    if (fine) run<T, T, true>(step, L, op, code, b, x, ccode, cb, xc, sums);
+    else run<T, T, false>(step, L, op, code, b, x, ccode, cb, xc, sums);
 }
 
 }  // namespace
@@ -93,6 +94,22 @@ void f2h_step_f32(int step, int fine, int nx, int ny, int cnx, int cny, double d
                   double* sums) {
     step_t<float>(step, fine, nx, ny, cnx, cny, dx, dy, dir, dg, cx, cy, code, b, x, ccode, cb, xc,
                   sums);
+}
+
+// The mixed form's coarse level: FP32 values, couplings stored as FP16 face counts
+// (hcx, hcy) decoded as count * cs (csx, csy: the finest level's 1/h^2 per axis).
+void f2h_step_mixed(int step, int nx, int ny, int cnx, int cny, double csx, double csy,
+                    const float* dg, const uint16_t* hcx, const uint16_t* hcy, const uint8_t* code,
+                    const float* b, float* x, const uint8_t* ccode, float* cb, const float* xc,
+                    double* sums) {
+    MLevel<float> L = level<float>(nx, ny, cnx, cny, 1.0, 1.0, 0);
+    L.csx = (float)csx;
+    L.csy = (float)csy;
+    F2Op<float, __half> op;
+    op.dg = dg;
+    op.cx = reinterpret_cast<const __half*>(hcx);
+    op.cy = reinterpret_cast<const __half*>(hcy);
+    run<float, __half, false>(step, L, op, code, b, x, ccode, cb, xc, sums);
 }
 
 }  // extern "C"

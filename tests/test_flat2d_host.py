@@ -43,6 +43,7 @@ def f2h(tmp_path_factory):
     for t in ("f64", "f32"):
         getattr(lib, f"f2h_step_{t}").argtypes = [i, i, i, i, i, i, d, d, i, p, p, p, p, p, p, p,
                                                   p, p, p]
+    lib.f2h_step_mixed.argtypes = [i, i, i, i, i, d, d, p, p, p, p, p, p, p, p, p, p]
     return lib
 
 
@@ -148,3 +149,49 @@ def test_flat2d_steps_equal_oracle_stages(f2h, seed):
         assert rel(cb.astype(np.float64), b1) <= 1e-4
         xu, _, _ = run(f2h, "f32", 2, lvl, b_l, xc=x1)
         assert rel(xu.astype(np.float64), x_out) <= 1e-5
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_flat2d_coarse_fp16_couplings(f2h, seed):
+    """The mixed form's coarse levels: couplings stored as FP16 face counts (exact up
+    to 2048 faces) and decoded as count * (finest 1/h^2), FP32 values; within FP32
+    rounding of the oracle's FP64 stages (the host divides exactly where the GPU uses
+    the fast reciprocal)."""
+    solid, r, dx, dy, _ = case(seed)
+    H = O.Hierarchy(solid, dx, dy, 1.0)
+    if H.nlevels < 3:
+        pytest.skip("no coarse march level")
+    csx, csy = 1.0 / (dx * dx), 1.0 / (dy * dy)
+    inner = (slice(1, -1), slice(1, -1))
+    for l in range(1, H.nlevels - 1):
+        b_l, x_fwd, b1, x1, x_out = H.vcycle_stages(r, l)
+        nx, ny, _ = H.dims(l)
+        cnx, cny, _ = H.dims(l + 1)
+        cx, cy, _, dg = H.level_coeffs(l)
+        counts_x, counts_y = np.rint(cx / csx), np.rint(cy / csy)
+        assert np.array_equal(counts_x * csx, cx) or np.allclose(counts_x * csx, cx, rtol=1e-15)
+        hcx = counts_x.astype(np.float16).view(np.uint16).copy()
+        hcy = counts_y.astype(np.float16).view(np.uint16).copy()
+        code = codes(H.level_solid(l), fine=False)
+        c1 = codes(H.level_solid(l + 1), fine=False)
+        f32 = (lambda a: np.ascontiguousarray(a, dtype=np.float32))
+        dg32, b32 = f32(dg), f32(b_l)
+
+        def step(k, x=None, cb=None, xc=None):
+            x = f32(x) if x is not None else np.zeros(b32.shape, np.float32)
+            sums = np.zeros(3)
+            f2h.f2h_step_mixed(k, nx, ny, cnx, cny, csx, csy, _p(dg32), _p(hcx), _p(hcy), _p(code),
+                               _p(b32), _p(x), _p(c1), _p(cb), _p(f32(xc) if xc is not None else None),
+                               _p(sums))
+            return x, cb
+
+        def rel(a, b):
+            return np.linalg.norm(a[inner] - b[inner]) / max(np.linalg.norm(b[inner]), 1e-300)
+
+        x, _ = step(0)
+        assert rel(x.astype(np.float64), x_fwd) <= 1e-5, f"level {l}: forward sweep"
+        cb = np.zeros(b1.shape, np.float32)
+        step(1, x=x_fwd, cb=cb)
+        assert rel(cb.astype(np.float64), b1) <= 1e-4, f"level {l}: restriction"
+        xu, _ = step(2, xc=x1)
+        assert rel(xu.astype(np.float64), x_out) <= 1e-5, f"level {l}: reverse sweep"
