@@ -134,17 +134,21 @@ UAAMG_API uaamg_status uaamg_set_variable_laplacian(uaamg_handle* h, const doubl
  * Takes effect at the next uaamg_set_problem_*. */
 UAAMG_API uaamg_status uaamg_set_dirichlet_walls(uaamg_handle* h, int on);
 
-/* V-cycle kernels of this handle: 0 (default) = z marches, four per level (forward
- * sweep; residual + restriction; prolongation + even colour; odd colour), each
- * streaming the level's planes through TMA-filled shared memory, down to the first
- * level of at most 1024 cells; that level, the smaller ones and the coarsest
- * solve run as ONE single-block kernel with the levels in shared memory;
+/* V-cycle kernels of this handle: 0 (default) = z marches, two per level (the way
+ * down: forward sweep, residual and restriction; the way up: prolongation and the
+ * reverse sweep), each streaming the level's planes through TMA-filled shared
+ * memory, down to the first level of at most 1024 cells; that level, the smaller
+ * ones and the coarsest solve run as ONE single-block kernel with the levels in
+ * shared memory;
  * 1 = one kernel per colour sweep, restriction and prolongation, step by step as
  * UAAMGPreconditioner3D::vCycle (uaamg_preconditioner_3d.cpp:183-196);
- * 2 = z marches on every level and a separate coarsest-level kernel;
+ * 2 = the two-march levels on every level and a separate coarsest-level kernel;
  * 3 = as 0, with every march level of a 2D problem as four flat walks over the level
- * instead of marches (a 2D level is one plane: nothing to pipeline).
- * All give identical results in FP64; 1 and 2 exist to cross-check 0. */
+ * instead of marches (a 2D level is one plane: nothing to pipeline);
+ * 4 = as 0 with four marches per level (forward sweep; residual + restriction;
+ * prolongation + even colour; odd colour);
+ * 5 = four marches per level on every level and a separate coarsest-level kernel.
+ * All give identical results in FP64; 1, 2, 4 and 5 exist to cross-check 0. */
 UAAMG_API uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps);
 
 /* Solve lap(p) = rhs with HOST FP64 arrays (padded): the Solver::solve /

@@ -36,11 +36,14 @@ def rel_l2_meanfree(a, b, solid):
 # --- golden fixtures ---------------------------------------------------------
 
 
-@pytest.fixture(params=["march", "sweeps", "march_all"])
+@pytest.fixture(params=["fused", "sweeps", "fused_all", "flat2d", "march", "march_all"])
 def vkernels(request, handle):
-    """Every V-cycle implementation: z marches with the single-block small-level kernel,
-    per-colour sweeps, and z marches on every level."""
-    handle.set_vcycle_kernels({"march": 0, "sweeps": 1, "march_all": 2}[request.param])
+    """Every V-cycle implementation: two fused z marches a level with the single-block
+    small-level kernel, per-colour sweeps, fused marches on every level, flat walks on
+    the 2D march levels (fused marches on a 3D problem), four z marches a level with
+    the small-level kernel, and four marches on every level."""
+    handle.set_vcycle_kernels({"fused": 0, "sweeps": 1, "fused_all": 2, "flat2d": 3, "march": 4,
+                               "march_all": 5}[request.param])
     yield request.param
     handle.set_vcycle_kernels(0)
 
@@ -202,7 +205,7 @@ def test_pcg_fp64_random_vs_oracle(handle, vkernels, seed):
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed"])
 @pytest.mark.parametrize("seed", range(4))
-def test_reduced_precision_vs_fp64(handle, prec, seed):
+def test_reduced_precision_vs_fp64(handle, vkernels, prec, seed):
     rng = np.random.default_rng(seed)
     dim = 2 + seed % 2
     if dim == 3:
@@ -336,6 +339,61 @@ def test_spheres256_fp64_matches_reference_iterations(handle, spheres256):
     assert abs(st.rhs_norm - fx["rhs_norm"]) <= 1e-12 * fx["rhs_norm"]
     res, bn = O.true_residual(solid, rhs, p, h, h, h)
     assert res / bn <= 1e-6
+
+
+def _meanfree_rel_l2_at_reference_samples(p, solid):
+    """Relative L2 difference, over the reference's 32768 sampled fluid cells, of the
+    whole-field-mean-free pressure p against the reference's own 256^3 solution
+    (tests/golden/spheres_256_reference_p.npz, written by make_spheres_reference.py
+    from PCG3D::solve, pcg_3d.cpp:18-125)."""
+    import os
+    from conftest import GOLDEN
+    ref = np.load(os.path.join(GOLDEN, "spheres_256_reference_p.npz"))
+    fl = fluid_interior(solid)
+    mean = float(p[fl].mean())
+    pr = ref["p"] - float(ref["fluid_mean"])
+    pg = p.reshape(-1)[ref["idx"]] - mean
+    return float(np.linalg.norm(pg - pr) / np.linalg.norm(pr))
+
+
+def test_spheres256_pressure_matches_reference_solution(handle, spheres256):
+    """256^3 spheres (the benchmark problem): the FP64 GPU solve with the
+    reference's absolute tolerance agrees with the reference's own CPU solution to
+    1e-10 relative (same 82 iterations; only the order of the FP64 reductions
+    differs), and the mixed form at relative residual 1e-6 to 1e-5."""
+    import json, os
+    from conftest import GOLDEN
+    fx = json.load(open(os.path.join(GOLDEN, "spheres_256_reference.json")))
+    solid, rhs, h = spheres256
+    handle.set_problem(solid, h, h, h)
+    p = np.zeros_like(rhs)
+    handle.solve(rhs, p, handle.options("fp64", fx["tol_abs"], 500, "abs"), strict=True)
+    e64 = _meanfree_rel_l2_at_reference_samples(p, solid)
+    assert e64 <= 1e-10, e64
+    pm = np.zeros_like(rhs)
+    handle.solve(rhs, pm, handle.options("mixed", 1e-6, 500, "rel"), strict=True)
+    em = _meanfree_rel_l2_at_reference_samples(pm, solid)
+    assert em <= 1e-5, em
+
+
+def test_spheres256_mixed_couplings_are_galerkin_sums(handle, spheres256):
+    """The mixed form's coarse couplings (FP16 face counts where a level's counts
+    fit FP16's exact integers, FP32 on the levels whose counts exceed 2048) decode to
+    exactly the FP64 Galerkin couplings on every level of the 256^3 hierarchy
+    (uaamg_preconditioner_3d.cpp:81-116; h = 1/256 makes every coupling an integer
+    times 2^16)."""
+    solid, _, h = spheres256
+    handle.set_problem(solid, h, h, h)
+    nl = handle.num_levels()
+    assert nl == 7
+    for l in range(nl):
+        _, x64, y64, z64 = handle.copy_level(l, "fp64")
+        _, xm, ym, zm = handle.copy_level(l, "mixed")
+        assert np.array_equal(xm, x64) and np.array_equal(ym, y64) and np.array_equal(zm, z64), l
+    # the coarsest level holds face counts above 2048 (odd ones too): FP16 would round them
+    _, x6, _, _ = handle.copy_level(nl - 1, "fp64")
+    counts = x6 / 65536.0
+    assert counts.max() > 2048 and np.any((counts > 2048) & (counts % 2 == 1))
 
 
 def test_spheres256_mixed_and_fp32(handle, spheres256):

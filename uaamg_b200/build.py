@@ -32,7 +32,7 @@ UNITS = [
     ("noalloc.cu", ["-fmad=false"]),
     ("project.cu", ["-fmad=false"]),
 ]
-HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "flat2d.cuh", "tail.cuh", "vec.cuh", "tma.cuh",
+HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "fused.cuh", "flat2d.cuh", "tail.cuh", "vec.cuh", "tma.cuh",
            "engine.cuh", "engine.h", "handle.h"]
 
 

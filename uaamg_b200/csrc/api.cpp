@@ -99,9 +99,7 @@ uaamg_status engine_for(uaamg_handle* h, int p, uaamg::Engine** out) {
         if (!h->eng[p]) return fail(h, UAAMG_OOM, "engine allocation failed");
     }
     h->eng[p]->set_stream(h->stream);
-    h->eng[p]->set_vcycle_sweeps(h->sweeps == 1);
-    h->eng[p]->set_small_levels(h->sweeps == 0 || h->sweeps == 3);
-    h->eng[p]->set_flat2d(h->sweeps == 3);
+    uaamg::api::apply_vcycle_mode(h->eng[p], h->sweeps);
     h->eng[p]->set_autotune(h->autotune != 0);
     if (h->lap_on)
         h->eng[p]->set_operator(h->d_lap[0], h->d_lap[1], h->d_lap[2], h->nx + 2, h->lap_version);
@@ -252,7 +250,7 @@ uaamg_status uaamg_set_stream(uaamg_handle* h, void* stream) {
 
 uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps) {
     if (!h) return UAAMG_INVALID_ARG;
-    if (sweeps < 0 || sweeps > 3) return fail(h, UAAMG_INVALID_ARG, "V-cycle kernels: 0 to 3");
+    if (sweeps < 0 || sweeps > 5) return fail(h, UAAMG_INVALID_ARG, "V-cycle kernels: 0 to 5");
     h->sweeps = sweeps;
     return UAAMG_OK;
 }

@@ -24,6 +24,7 @@
 
 #include "engine.h"
 #include "flat2d.cuh"
+#include "fused.cuh"
 #include "kernels.cuh"
 #include "tail.cuh"
 #include "tma.cuh"
@@ -42,26 +43,35 @@ struct LevelBuf {
     T *x = nullptr, *b = nullptr;  // level >= 1 only (level 0 uses the CG's r and z)
     uint8_t* code = nullptr;       // cell codes (vec.cuh k_codes)
     int zc = 2;                    // planes per block of the z marches (march.cuh)
+    // FP32 couplings on a level of a mixed engine whose face counts exceed 2048 (3D
+    // levels 6 and down, 2D levels 12 and down): FP16 holds integers exactly only up
+    // to 2048 and overflows above 65504
+    bool c32 = false;
     // plane-box tensor maps of the marches: b, x, codes, couplings, diagonal, and x
     // as the parent box read by the next-finer level's prolongation
     CUtensorMap mb, mx, mcode, mcx, mcy, mcz, mdg, mxq;
+    // boxes with a 2-cell ring for the fused marches (fused.cuh): b, codes, diagonal,
+    // couplings
+    CUtensorMap fb, fcode, fdg, fcx, fcy, fcz;
 };
 
 // Kernel classes for the in-situ per-kernel timing (uaamg_profile_solve).
 enum KClass : int {
     K_SWEEP = 0, K_RESTRICT, K_PROLONG, K_COARSEST, K_PMATVEC, K_UPDATE, K_ZDOT, K_FWD, K_RES,
-    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_TAIL, K_NCLASS
+    K_UPE, K_UPO, K_TRUE_RESIDUAL, K_RHS, K_OUTPUT, K_CAST, K_SETUP, K_TAIL, K_REPLACE, K_DOWN,
+    K_UP, K_NCLASS
 };
 static const char* const kclass_names[K_NCLASS] = {
     "rbgs_sweep", "restrict_residual", "prolong_add", "coarsest_solve", "p_matvec_dot",
     "cg_update", "z_dot", "smooth_fwd", "residual_restrict", "prolong_smooth_even",
     "smooth_odd", "true_residual", "rhs_prepare", "output", "cast", "hierarchy_setup",
-    "small_levels"};
+    "small_levels", "residual_replacement", "level_down", "level_up"};
 
 struct KTag {
     int cls;
     int level;
-    double bytes;  // algorithmic (compulsory) bytes of this launch
+    double bytes;  // algorithmic (compulsory) bytes of this launch (K_REPLACE: of one
+                   // launch that performs the replacement; most launches return at once)
 };
 
 #define UAAMG_LAUNCH_SMEM(tag, kern, grid, block, smem, ...)              \
@@ -144,7 +154,25 @@ public:
     int solve_inflight() const override { return nstep_ - seen_; }
 
     int solve_end(SolveResult* res) override {
-        return dim_ == 3 ? end_impl<3>(res) : end_impl<2>(res);
+        int e = solve_end_enqueue();
+        return e != E_OK ? e : solve_end_collect(res);
+    }
+
+    int solve_end_enqueue() override { return dim_ == 3 ? end_enqueue<3>() : end_enqueue<2>(); }
+
+    int solve_end_collect(SolveResult* res) override {
+        int e = sync_check();
+        if (e != E_OK) return e;
+        const CGState& c = *cg_host_;
+        res->status = c.status;
+        res->iterations = c.iter;
+        res->replacements = c.replacements;
+        res->rr = c.rr;
+        res->rr_true = c.rr_true;
+        res->bnorm = c.bnorm;
+        res->r0 = c.r0;
+        res->tol_abs = c.tol_abs;
+        return E_OK;
     }
 
     // The whole solve: the host keeps two steps queued and polls one behind, so it
@@ -211,13 +239,13 @@ public:
     void set_small_levels(bool on) override { tail_on_ = on; }
     void set_flat2d(bool on) override {
         if (on == flat2d_) return;
-        if (gexec_) {  // a captured step holds the other kernels
-            cudaStreamSynchronize(st_);
-            cudaGraphExecDestroy(gexec_);
-            gexec_ = nullptr;
-        }
-        gkey_ = -1;
+        drop_graph();  // a captured step holds the other kernels
         flat2d_ = on;
+    }
+    void set_fused(bool on) override {
+        if (on == fused_) return;
+        drop_graph();
+        fused_ = on;
     }
     void set_operator(const double* d, const double* ox, const double* oy, int sx,
                       long version) override {
@@ -263,6 +291,12 @@ public:
             slot->launches += 1;
             slot->total_ms += ms;
         }
+        // the residual replacement kernel runs every iteration but works only when a
+        // replacement is due: its bytes per launch are those of the replacements
+        // performed, spread over all its launches
+        for (auto& kt : out)
+            if (kt.cls == K_REPLACE && kt.launches > 0)
+                kt.bytes = kt.bytes * (double)cg_host_->replacements / (double)kt.launches;
         return E_OK;
     }
 
@@ -308,6 +342,7 @@ private:
     bool autotune_ = false;  // time the marches' z-chunk lengths at set-up
     bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
     bool flat2d_ = false;    // 2D finest level as flat walks (flat2d.cuh) instead of marches
+    bool fused_ = true;      // two fused marches a level (fused.cuh) instead of four
     int tail_lt_ = 0;        // first level of the small-level kernel
     int tail_nc_ = 0;        // 1: the hierarchy has a tail (0: it does not fit the kernel)
     size_t tail_smem_ = 0;   // its dynamic shared memory (x and b of every tail level)
@@ -323,6 +358,15 @@ private:
     std::vector<KTag> prof_tag_;
 
     int max_reduce_blocks() const { return 4 * num_sms_; }
+
+    void drop_graph() {
+        if (gexec_) {
+            cudaStreamSynchronize(st_);
+            cudaGraphExecDestroy(gexec_);
+            gexec_ = nullptr;
+        }
+        gkey_ = -1;
+    }
 
     // grid of the 2D search-direction kernel (kernels.cuh k_pmatvec_2d): 32 column
     // pairs of two rows a warp, eight warps a block, up to 8 blocks per SM (within
@@ -440,14 +484,27 @@ private:
                    : E_CUDA;
     }
 
-    template <int DIM, bool FINE>
+    template <int DIM, bool FINE, class CSL>
     int march_attrs() {
         int e;
-        if ((e = smem_attr(k_fwd_smooth<DIM, T, FINE, CS>, FwdCfg<DIM, T, FINE, CS>::BYTES)) ||
-            (e = smem_attr(k_restrict_res<DIM, T, FINE, CS>, ResCfg<DIM, T, FINE, CS>::BYTES)) ||
-            (e = smem_attr(k_up_even<DIM, T, FINE, CS>, UpeCfg<DIM, T, FINE, CS>::BYTES)) ||
-            (e = smem_attr(k_up_odd<DIM, T, FINE, false, CS>, UpoCfg<DIM, T, FINE, CS>::BYTES)) ||
-            (e = smem_attr(k_up_odd<DIM, T, FINE, true, CS>, UpoCfg<DIM, T, FINE, CS>::BYTES)))
+        if ((e = smem_attr(k_fwd_smooth<DIM, T, FINE, CSL>, FwdCfg<DIM, T, FINE, CSL>::BYTES)) ||
+            (e = smem_attr(k_restrict_res<DIM, T, FINE, CSL>, ResCfg<DIM, T, FINE, CSL>::BYTES)) ||
+            (e = smem_attr(k_up_even<DIM, T, FINE, CSL>, UpeCfg<DIM, T, FINE, CSL>::BYTES)) ||
+            (e = smem_attr(k_up_odd<DIM, T, FINE, false, CSL>, UpoCfg<DIM, T, FINE, CSL>::BYTES)) ||
+            (e = smem_attr(k_up_odd<DIM, T, FINE, true, CSL>, UpoCfg<DIM, T, FINE, CSL>::BYTES)))
+            return e;
+        return E_OK;
+    }
+
+    template <int DIM, bool FINE, class CSL>
+    int fused_attrs() {
+        int e;
+        if ((e = smem_attr(k_level_fused<DIM, T, FINE, CSL, false, false>,
+                           FCfg<DIM, T, CSL, FINE, false>::BYTES)) ||
+            (e = smem_attr(k_level_fused<DIM, T, FINE, CSL, true, false>,
+                           FCfg<DIM, T, CSL, FINE, true>::BYTES)) ||
+            (e = smem_attr(k_level_fused<DIM, T, FINE, CSL, true, true>,
+                           FCfg<DIM, T, CSL, FINE, true>::BYTES)))
             return e;
         return E_OK;
     }
@@ -478,6 +535,8 @@ private:
         for (int l = 0; l < nl; ++l) {
             LevelBuf<T, CS>& L = lv_[l];
             L.zc = DIM == 3 ? pick_zc(L.g) : 2;
+            // largest face count of a level-l coupling: 4^l (3D), 2^l (2D)
+            L.c32 = kHalf && l > 0 && (DIM == 3 ? 2 * l : l) > 11;
             const size_t n = (size_t)L.g.n;
             if ((e = alloc(L.solid, n))) return e;
             if ((e = alloc(L.code, n))) return e;
@@ -490,8 +549,10 @@ private:
                 if ((e = alloc(L.b, n))) return e;
                 if ((e = alloc(L.dg, n))) return e;
                 if constexpr (kHalf) {
-                    if ((e = alloc(L.hcx, n)) || (e = alloc(L.hcy, n))) return e;
-                    if (DIM == 3 && (e = alloc(L.hcz, n))) return e;
+                    if (!L.c32) {
+                        if ((e = alloc(L.hcx, n)) || (e = alloc(L.hcy, n))) return e;
+                        if (DIM == 3 && (e = alloc(L.hcz, n))) return e;
+                    }
                 } else {
                     L.hcx = L.cx; L.hcy = L.cy; L.hcz = L.cz;
                 }
@@ -520,9 +581,13 @@ private:
         for (auto& ev : ev_)
             if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return E_CUDA;
         // dynamic shared memory of the marches
-        if ((e = march_attrs<DIM, true>()) || (e = march_attrs<DIM, false>()) ||
-            (e = smem_attr(k_pmatvec<DIM, T>, PmvCfg<DIM, T>::BYTES)))
+        if ((e = march_attrs<DIM, true, CS>()) || (e = march_attrs<DIM, false, CS>()) ||
+            (e = smem_attr(k_pmatvec<DIM, T>, PmvCfg<DIM, T>::BYTES)) ||
+            (e = fused_attrs<DIM, true, CS>()) || (e = fused_attrs<DIM, false, CS>()))
             return e;
+        if constexpr (kHalf) {  // levels with FP32 couplings
+            if ((e = march_attrs<DIM, false, T>()) || (e = fused_attrs<DIM, false, T>())) return e;
+        }
         // plane-box tensor maps
         constexpr int BW = PBox<T>::W, BH = PBox<T>::H;
         for (int l = 0; l < nl; ++l) {
@@ -534,12 +599,30 @@ private:
                       encode_level_map<uint8_t>(&L.mcode, L.code, L.g, DIM, PBox<uint8_t>::W,
                                                 PBox<uint8_t>::H, 1);
             constexpr int CW = PBox<CS>::W;
-            if (ok && l > 0)
+            if (ok && l > 0 && !L.c32)
                 ok = encode_level_map<CS>(&L.mcx, L.hcx, L.g, DIM, CW, BH, 1) &&
                      encode_level_map<CS>(&L.mcy, L.hcy, L.g, DIM, CW, BH, 1) &&
                      (DIM == 2 || encode_level_map<CS>(&L.mcz, L.hcz, L.g, DIM, CW, BH, 1)) &&
-                     encode_level_map<T>(&L.mdg, L.dg, L.g, DIM, BW, BH, 1) &&
+                     encode_level_map<CS>(&L.fcx, L.hcx, L.g, DIM, RBox<CS>::W, RBox<CS>::H, 1) &&
+                     encode_level_map<CS>(&L.fcy, L.hcy, L.g, DIM, RBox<CS>::W, RBox<CS>::H, 1) &&
+                     (DIM == 2 ||
+                      encode_level_map<CS>(&L.fcz, L.hcz, L.g, DIM, RBox<CS>::W, RBox<CS>::H, 1));
+            if (ok && l > 0 && L.c32)  // FP32 couplings read as T
+                ok = encode_level_map<T>(&L.mcx, L.cx, L.g, DIM, BW, BH, 1) &&
+                     encode_level_map<T>(&L.mcy, L.cy, L.g, DIM, BW, BH, 1) &&
+                     (DIM == 2 || encode_level_map<T>(&L.mcz, L.cz, L.g, DIM, BW, BH, 1)) &&
+                     encode_level_map<T>(&L.fcx, L.cx, L.g, DIM, RBox<T>::W, RBox<T>::H, 1) &&
+                     encode_level_map<T>(&L.fcy, L.cy, L.g, DIM, RBox<T>::W, RBox<T>::H, 1) &&
+                     (DIM == 2 ||
+                      encode_level_map<T>(&L.fcz, L.cz, L.g, DIM, RBox<T>::W, RBox<T>::H, 1));
+            if (ok && l > 0)
+                ok = encode_level_map<T>(&L.mdg, L.dg, L.g, DIM, BW, BH, 1) &&
+                     encode_level_map<T>(&L.fdg, L.dg, L.g, DIM, RBox<T>::W, RBox<T>::H, 1) &&
                      encode_level_map<T>(&L.mxq, L.x, L.g, DIM, QBox<T>::W, QBox<T>::H, 1);
+            if (ok)
+                ok = encode_level_map<T>(&L.fb, b, L.g, DIM, RBox<T>::W, RBox<T>::H, 1) &&
+                     encode_level_map<uint8_t>(&L.fcode, L.code, L.g, DIM, RBox<uint8_t>::W,
+                                               RBox<uint8_t>::H, 1);
             if (!ok) return E_CUDA;
         }
         if (!encode_level_map<T>(&map_p_, p_, g0, DIM, BW, BH, 1) ||
@@ -572,6 +655,7 @@ private:
         for (int l = 1; l < nl; ++l) {
             LevelBuf<T, CS>& Cl = lv_[l];
             if constexpr (kHalf) {  // FP16 face counts (after every level's Galerkin sums)
+              if (!Cl.c32) {
                 const Geom& g0 = lv_[0].g;
                 const float cs[3] = {(float)(1.0 / (lv_[0].hx * lv_[0].hx)),
                                      (float)(1.0 / (lv_[0].hy * lv_[0].hy)),
@@ -582,6 +666,7 @@ private:
                 for (int a = 0; a < DIM; ++a)
                     UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_coupling_half, max_reduce_blocks(), 256,
                                  (long long)Cl.g.n, src[a], dst[a], cs[a]);
+              }
             }
             UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_diag<DIM, T>), vec_grid(Cl.g), dim3(32, 8), Cl.g,
                          Cl.solid, Cl.cx, Cl.cy, Cl.cz, Cl.wd, Cl.dg);
@@ -670,7 +755,7 @@ private:
     template <int DIM>
     int tune() {
         static std::mutex mu;
-        static std::map<std::tuple<int, int, int, int, int, int>, int> cache;
+        static std::map<std::tuple<int, int, int, int, int, int, int>, int> cache;
         cudaEvent_t a = nullptr, b = nullptr;
         if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return E_CUDA;
         const bool prof = prof_on_;
@@ -680,7 +765,7 @@ private:
             if (use_tail() && l >= tail_lt_) break;  // the small-level kernel runs those levels
             LevelBuf<T, CS>& L = lv_[l];
             const auto key = std::make_tuple((int)sizeof(T), mixed_ ? 1 : 0, L.g.nx, L.g.ny, L.g.nz,
-                                             l == 0 ? 1 : 0);
+                                             l == 0 ? 1 : 0, fused_ ? 1 : 0);
             {
                 std::lock_guard<std::mutex> lk(mu);
                 auto it = cache.find(key);
@@ -793,9 +878,10 @@ private:
         v.idy2 = (T)(1.0 / (L.hy * L.hy));
         v.idz2 = L.g.nz ? (T)(1.0 / (L.hz * L.hz)) : T(0);
         // FP16 couplings are face counts times the finest level's 1/h^2 per axis
-        v.csx = kHalf ? (T)(1.0 / (lv_[0].hx * lv_[0].hx)) : T(1);
-        v.csy = kHalf ? (T)(1.0 / (lv_[0].hy * lv_[0].hy)) : T(1);
-        v.csz = kHalf ? (T)(1.0 / (lv_[0].hz * lv_[0].hz)) : T(1);
+        const bool half = kHalf && !L.c32;
+        v.csx = half ? (T)(1.0 / (lv_[0].hx * lv_[0].hx)) : T(1);
+        v.csy = half ? (T)(1.0 / (lv_[0].hy * lv_[0].hy)) : T(1);
+        v.csz = half ? (T)(1.0 / (lv_[0].hz * lv_[0].hz)) : T(1);
         v.dirichlet = dirichlet_;
         v.zc = L.zc;
         return v;
@@ -840,77 +926,140 @@ private:
         return dim3((unsigned)(nb < 1 ? 1 : nb));
     }
 
+    // Tensor maps of a fused march over level l (boxes with a 2-cell ring); up: with
+    // the next-coarser level's x as parent boxes.
+    FMaps fmaps(int l, bool up) const {
+        const LevelBuf<T, CS>& L = lv_[l];
+        FMaps m{};
+        m.b = L.fb;
+        m.code = L.fcode;
+        if (l > 0) {
+            m.dg = L.fdg;
+            m.cx = L.fcx;
+            m.cy = L.fcy;
+            m.cz = L.fcz;
+        }
+        if (up) m.xc = lv_[l + 1].mxq;
+        return m;
+    }
+
+    // The way down through level l: b (and on coarse levels the couplings) in,
+    // coarse b out.  CSL: the coupling storage of this level.
     template <int DIM, bool FINE>
     void down_level(int l, const int* done) {
+        if constexpr (kHalf && !FINE) {
+            if (lv_[l].c32) { down_level_cs<DIM, FINE, T>(l, done); return; }
+        }
+        down_level_cs<DIM, FINE, CS>(l, done);
+    }
+
+    template <int DIM, bool FINE, class CSL>
+    void down_level_cs(int l, const int* done) {
         const LevelBuf<T, CS>& L = lv_[l];
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
-        const double coef = FINE ? 0.0 : DIM * (double)sizeof(CS) + t;  // couplings + diagonal
-        if (DIM == 2 && flat2d_) {
-            // b, code (coarse levels: couplings, diagonal) in; x out / b, x, code in;
-            // coarse b out
-            const F2Op<T, CS> op = flat_op(l);
-            T* b = l == 0 ? r_ : L.b;
-            T* x = l == 0 ? z_ : L.x;
-            UAAMG_LAUNCH((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_flat2d<T, CS, FINE>),
-                         flat_grid((L.g.ny + 1) / 2, L.g.nx), dim3(32, 8), mlevel(l), op, L.code, b,
-                         x, done);
-            UAAMG_LAUNCH((KTag{K_RES, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
-                         (k_res_flat2d<T, CS, FINE>), flat_grid(Cl.g.ny, Cl.g.nx), dim3(32, 8),
-                         mlevel(l), op, L.code, b, x, Cl.code, Cl.b, done);
-            return;
+        const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
+        if constexpr (std::is_same<CSL, CS>::value) {
+            if (DIM == 2 && flat2d_) {
+                // b, code (coarse levels: couplings, diagonal) in; x out / b, x, code in;
+                // coarse b out
+                const F2Op<T, CS> op = flat_op(l);
+                T* b = l == 0 ? r_ : L.b;
+                T* x = l == 0 ? z_ : L.x;
+                UAAMG_LAUNCH((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_flat2d<T, CS, FINE>),
+                             flat_grid((L.g.ny + 1) / 2, L.g.nx), dim3(32, 8), mlevel(l), op, L.code, b,
+                             x, done);
+                UAAMG_LAUNCH((KTag{K_RES, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
+                             (k_res_flat2d<T, CS, FINE>), flat_grid(Cl.g.ny, Cl.g.nx), dim3(32, 8),
+                             mlevel(l), op, L.code, b, x, Cl.code, Cl.b, done);
+                return;
+            }
         }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
+        if (fused_) {
+            // b, code (coarse levels: diagonal, couplings) in; coarse code in, coarse b out
+            UAAMG_LAUNCH_SMEM((KTag{K_DOWN, l, c * (t + 1.0 + coef) + cc * (t + 1.0)}),
+                              (k_level_fused<DIM, T, FINE, CSL, false, false>), grid, blk,
+                              (FCfg<DIM, T, CSL, FINE, false>::BYTES), fmaps(l, false), mlevel(l),
+                              Cl.code, Cl.b, done, err_, partials_, cg_);
+            return;
+        }
         T* x = l == 0 ? z_ : L.x;
-        UAAMG_LAUNCH_SMEM((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_smooth<DIM, T, FINE, CS>),
-                          grid, blk, (FwdCfg<DIM, T, FINE, CS>::BYTES), maps<DIM>(l, false, false),
+        UAAMG_LAUNCH_SMEM((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_smooth<DIM, T, FINE, CSL>),
+                          grid, blk, (FwdCfg<DIM, T, FINE, CSL>::BYTES), maps<DIM>(l, false, false),
                           mlevel(l), x, done, err_);
         UAAMG_LAUNCH_SMEM((KTag{K_RES, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
-                          (k_restrict_res<DIM, T, FINE, CS>), grid, blk, (ResCfg<DIM, T, FINE, CS>::BYTES),
+                          (k_restrict_res<DIM, T, FINE, CSL>), grid, blk, (ResCfg<DIM, T, FINE, CSL>::BYTES),
                           maps<DIM>(l, true, false), mlevel(l), Cl.code, Cl.b, done, err_);
     }
 
+    // The way up through level l: coarse x in, x out (level 0 with zdot: also the
+    // CG's z sums).
     template <int DIM, bool FINE>
     void up_level(int l, const int* done, bool zdot) {
+        if constexpr (kHalf && !FINE) {
+            if (lv_[l].c32) { up_level_cs<DIM, FINE, T>(l, done, zdot); return; }
+        }
+        up_level_cs<DIM, FINE, CS>(l, done, zdot);
+    }
+
+    template <int DIM, bool FINE, class CSL>
+    void up_level_cs(int l, const int* done, bool zdot) {
         const LevelBuf<T, CS>& L = lv_[l];
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
-        const double coef = FINE ? 0.0 : DIM * (double)sizeof(CS) + t;  // couplings + diagonal
-        if (DIM == 2 && flat2d_) {
-            const dim3 fg = flat_grid((L.g.ny + 1) / 2, L.g.nx), fb(32, 8);
-            const F2Op<T, CS> op = flat_op(l);
-            T* b = l == 0 ? r_ : L.b;
-            T* x = l == 0 ? z_ : L.x;
-            // b, code, coarse x in; x out / b, x, code in; odd x out
-            UAAMG_LAUNCH((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
-                         (k_upe_flat2d<T, CS, FINE>), fg, fb, mlevel(l), op, L.code, b, Cl.x, x, done);
-            if (FINE && zdot)
-                UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
-                             (k_upo_flat2d<T, CS, FINE, true>), fg, fb, mlevel(l), op, L.code, b, x,
-                             done, partials_, cg_);
-            else
-                UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
-                             (k_upo_flat2d<T, CS, FINE, false>), fg, fb, mlevel(l), op, L.code, b, x,
-                             done, partials_, cg_);
-            return;
+        const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
+        if constexpr (std::is_same<CSL, CS>::value) {
+            if (DIM == 2 && flat2d_) {
+                const dim3 fg = flat_grid((L.g.ny + 1) / 2, L.g.nx), fb(32, 8);
+                const F2Op<T, CS> op = flat_op(l);
+                T* b = l == 0 ? r_ : L.b;
+                T* x = l == 0 ? z_ : L.x;
+                // b, code, coarse x in; x out / b, x, code in; odd x out
+                UAAMG_LAUNCH((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
+                             (k_upe_flat2d<T, CS, FINE>), fg, fb, mlevel(l), op, L.code, b, Cl.x, x, done);
+                if (FINE && zdot)
+                    UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
+                                 (k_upo_flat2d<T, CS, FINE, true>), fg, fb, mlevel(l), op, L.code, b, x,
+                                 done, partials_, cg_);
+                else
+                    UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
+                                 (k_upo_flat2d<T, CS, FINE, false>), fg, fb, mlevel(l), op, L.code, b, x,
+                                 done, partials_, cg_);
+                return;
+            }
         }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
+        if (fused_) {
+            // b, code (coarse levels: diagonal, couplings), coarse x in; x out
+            const KTag tag{K_UP, l, c * (2.0 * t + 1.0 + coef) + cc * t};
+            if (FINE && zdot)
+                UAAMG_LAUNCH_SMEM(tag, (k_level_fused<DIM, T, FINE, CSL, true, true>), grid, blk,
+                                  (FCfg<DIM, T, CSL, FINE, true>::BYTES), fmaps(l, true), mlevel(l),
+                                  (const uint8_t*)nullptr, x, done, err_, partials_, cg_);
+            else
+                UAAMG_LAUNCH_SMEM(tag, (k_level_fused<DIM, T, FINE, CSL, true, false>), grid, blk,
+                                  (FCfg<DIM, T, CSL, FINE, true>::BYTES), fmaps(l, true), mlevel(l),
+                                  (const uint8_t*)nullptr, x, done, err_, partials_, cg_);
+            return;
+        }
         UAAMG_LAUNCH_SMEM((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
-                          (k_up_even<DIM, T, FINE, CS>), grid, blk, (UpeCfg<DIM, T, FINE, CS>::BYTES),
+                          (k_up_even<DIM, T, FINE, CSL>), grid, blk, (UpeCfg<DIM, T, FINE, CSL>::BYTES),
                           maps<DIM>(l, false, true), mlevel(l), x, done, err_);
         if (zdot)
             UAAMG_LAUNCH_SMEM((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
-                              (k_up_odd<DIM, T, FINE, true, CS>), grid, blk, (UpoCfg<DIM, T, FINE, CS>::BYTES),
+                              (k_up_odd<DIM, T, FINE, true, CSL>), grid, blk, (UpoCfg<DIM, T, FINE, CSL>::BYTES),
                               maps<DIM>(l, true, false), mlevel(l), x, done, err_, partials_, cg_);
         else
             UAAMG_LAUNCH_SMEM((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
-                              (k_up_odd<DIM, T, FINE, false, CS>), grid, blk, (UpoCfg<DIM, T, FINE, CS>::BYTES),
+                              (k_up_odd<DIM, T, FINE, false, CSL>), grid, blk, (UpoCfg<DIM, T, FINE, CSL>::BYTES),
                               maps<DIM>(l, true, false), mlevel(l), x, done, err_, partials_, cg_);
     }
 
-    // z_ = M^{-1} r_ with four z marches per level (march.cuh); the finest level's
-    // last march also reduces the CG's z sums when zdot is set.
+    // z_ = M^{-1} r_ with marches on every level down to the small-level kernel (two
+    // fused marches a level, fused.cuh, or four, march.cuh); the finest level's last
+    // march also reduces the CG's z sums when zdot is set.
     template <int DIM>
     void vcycle_march(const int* done, bool zdot) {
         const int nl = (int)lv_.size();
@@ -1022,7 +1171,7 @@ private:
                      partials_, cg_, cur_.hist);
         if (mixed_) {
             // residual replacement (when due): b, x_hi, x_lo, codes in; r out
-            UAAMG_LAUNCH((KTag{K_TRUE_RESIDUAL, 0, cells(g) * (17.0 + 2.0 * sizeof(T))}),
+            UAAMG_LAUNCH((KTag{K_REPLACE, 0, cells(g) * (17.0 + 2.0 * sizeof(T))}),
                          (k_resid_x64<DIM, T>), resid_grid(g), dim3(32, 8), g, lv_[0].code, b64_, xd_,
                          xlo_, r_, st, kResidZc, partials_, cg_, 5, 1, cur_.tol, cur_.tol_mode);
         }
@@ -1147,7 +1296,7 @@ private:
     }
 
     template <int DIM>
-    int end_impl(SolveResult* res) {
+    int end_enqueue() {
         const Geom g = lv_[0].g;
         const dim3 vb(32, 8);
         const dim3 vg = vec_grid(g);
@@ -1172,17 +1321,6 @@ private:
         }
         if (cudaMemcpyAsync(cg_host_, cg_, sizeof(CGState), cudaMemcpyDeviceToHost, st_) != cudaSuccess)
             return E_CUDA;
-        int e = sync_check();
-        if (e != E_OK) return e;
-        const CGState& c = *cg_host_;
-        res->status = c.status;
-        res->iterations = c.iter;
-        res->replacements = c.replacements;
-        res->rr = c.rr;
-        res->rr_true = c.rr_true;
-        res->bnorm = c.bnorm;
-        res->r0 = c.r0;
-        res->tol_abs = c.tol_abs;
         return E_OK;
     }
 };

@@ -74,6 +74,12 @@ public:
     virtual int solve_poll(bool wait, bool* stopped) = 0;
     virtual int solve_inflight() const = 0;
     virtual int solve_end(SolveResult* res) = 0;
+    // solve_end in two halves for a caller that must not block: enqueue queues the
+    // exit work (FP64 true residual, solution export, state copy) on the engine's
+    // stream; collect reads the result once that work has completed (e.g. after an
+    // event recorded behind it reports done), and then does not wait.
+    virtual int solve_end_enqueue() = 0;
+    virtual int solve_end_collect(SolveResult* res) = 0;
     virtual int nlevels() const = 0;
     virtual void level_dims(int l, int* nx, int* ny, int* nz) const = 0;
     // Host copies of level l: mask and FP64 views of cx, cy, cz (nullable).
@@ -90,6 +96,10 @@ public:
     // 2D problems: the four V-cycle steps of every march level as flat walks over the
     // level (flat2d.cuh) instead of z marches (default off).
     virtual void set_flat2d(bool on) = 0;
+    // Marches: two fused marches per level (fused.cuh: down = forward sweep, residual
+    // and restriction; up = prolongation and reverse sweep) instead of four
+    // (march.cuh).  Default on.
+    virtual void set_fused(bool on) = 0;
     // 2D variable-coefficient outer-CG operator (the lap_diag / lap_off_x / lap_off_y
     // branch of PCG::solve, pcg.cpp:35-46): device arrays in the caller's padded
     // layout with row stride sx, read in place by every solve until changed;

@@ -1,0 +1,512 @@
+// Fused V-cycle level kernels: ONE z march for the way down through a level and
+// ONE for the way up (uaamg_preconditioner_3d.cpp:183-196; 2D
+// uaamg_preconditioner.cpp:162-175), instead of the four marches of march.cuh.
+//
+//   k_level_down  forward red-black sweep from x = 0 (smooth(L,1,false),
+//                 _3d.cpp:123-141), the residual b - A x (restrictResidual,
+//                 144-165) and its restriction to the coarse b.  The smoothed x
+//                 is never stored: odd cells hold b/d and even cells a function of
+//                 the b of their neighbours, so the block recomputes x on its tile
+//                 and a 2-cell ring from the staged b, and writes only the coarse b.
+//   k_level_up    prolongation x += 2 x_coarse (prolongateAdd, 168-181) and the
+//                 reverse sweep (even colour, then odd), writing the final x; on
+//                 the finest level also the CG's z sums (pcg_3d.cpp:112-123).
+//
+// Block: a 32 x 16 column tile (256 threads, each owning the cell pair (i, j),
+// (i, j+1) -- one cell of each colour), marching a chunk of z planes.  Every plane
+// of b, the cell codes (coarse levels: diagonal and couplings; way up: the parent
+// x) arrives by TMA as a box of the tile plus a 2-cell ring, into a ring of
+// shared-memory stages.  Step s of the march computes three things:
+//   1. the odd-colour value of plane s+1 (tile and 2-cell ring),
+//   2. the even-colour value of plane s (tile and 1-cell ring), from the odd
+//      values of plane s in shared memory and plane s +- 1 in registers,
+//   3. the final result of plane s-1 on the tile (way down: residual and
+//      restriction; way up: the odd colour of the reverse sweep and the store).
+// A z neighbour is the same column one step up or down, so each thread keeps its
+// column's recent values in registers; in-plane neighbours are read from three
+// shared x planes written one step earlier, so one block barrier per step
+// suffices.  The first 104 threads also own a pair of ring cells (50 pairs of
+// the 1-cell ring, 54 of the 2-cell ring).
+//
+// Arithmetic: every per-cell value is the reference's expression in its order
+// (the forward even update (b + sum c_n x_n)/d, the residual b - (d x - sum c_n
+// x_n), the restriction's child order), so the FP64 instantiation (built with
+// -fmad=false) reproduces the reference's V-cycle bit for bit.  The FP32 forms
+// take the residual of the forward sweep from its exact form: an even cell was
+// just relaxed, so its residual is 0, and an odd cell's is sum_n c_n x_n over its
+// (even) neighbours, since d x = b there; cells with d < 1e-30 (skipped by the
+// smoother) keep r = b.
+#pragma once
+#include "march.cuh"
+
+namespace uaamg {
+namespace {
+
+// Box of element type E around a tile with a 2-cell ring: cells
+// i in [i0-2, i0+33], j in [j0-2, j0+17] (i0 = 1 + 32 bx, j0 = 1 + 16 by) of one
+// plane.  The start column 32 bx - A is the 16-byte boundary at or below i0 - 2.
+template <class E>
+struct RBox {
+    static constexpr int A = 16 / (int)sizeof(E);          // elements per 16 bytes
+    static constexpr int W = (A + 35 + A - 1) / A * A;      // row width (elements)
+    static constexpr int H = kMY + 4;
+    static constexpr uint32_t BYTES = (uint32_t)(W * H * sizeof(E));
+    // position of the cell (i0 + di, j0 + dj), di in [-2, 33], dj in [-2, 17]
+    __host__ __device__ static constexpr int pos(int di, int dj) { return (dj + 2) * W + A + 1 + di; }
+};
+
+// Tensor maps of a fused march (boxes of RBox geometry; xc: the parent level's x
+// in QBox geometry).
+struct FMaps {
+    CUtensorMap b, code, dg, cx, cy, cz, xc;
+};
+
+// One ring stage: b, codes, [diagonal, couplings], [parent x].
+template <int DIM, class T, class CS, bool FINE, bool UP>
+struct FPlan {
+    static constexpr int NC = FINE ? 0 : (DIM == 3 ? 3 : 2);
+    static constexpr size_t OFF_B = 0;
+    static constexpr size_t OFF_CODE = align128(RBox<T>::BYTES);
+    static constexpr size_t OFF_DG = OFF_CODE + align128(RBox<uint8_t>::BYTES);
+    static constexpr size_t OFF_CX = OFF_DG + (FINE ? 0 : align128(RBox<T>::BYTES));
+    static constexpr size_t CB = align128(RBox<CS>::BYTES);
+    static constexpr size_t OFF_CY = OFF_CX + CB, OFF_CZ = OFF_CY + CB;
+    static constexpr size_t OFF_XC = OFF_CX + NC * CB;
+    static constexpr size_t STAGE = OFF_XC + (UP ? align128(QBox<T>::BYTES) : 0);
+    static constexpr uint32_t TX = RBox<T>::BYTES + RBox<uint8_t>::BYTES +
+                                   (FINE ? 0u : RBox<T>::BYTES + NC * RBox<CS>::BYTES) +
+                                   (UP ? QBox<T>::BYTES : 0u);
+};
+
+// Ring depth and shared memory.  LAG: planes behind the step that stay resident
+// (the coarse levels read the -z coupling of plane s-2 in step 3); S >= LAG + 3
+// keeps the plane of the next step in flight during the current one.
+template <int DIM, class T, class CS, bool FINE, bool UP>
+struct FCfg {
+    using P = FPlan<DIM, T, CS, FINE, UP>;
+    static constexpr int LAG = FINE ? 1 : 2;
+    static constexpr int S = DIM == 2 ? 1 : LAG + 3 + (FINE ? 3 : 1);
+    static constexpr int NXP = DIM == 2 ? 1 : 3;  // shared x planes
+    static constexpr size_t OFF_LUT = 128;          // after the stage barriers
+    static constexpr size_t OFF_RING = OFF_LUT + align128(64 * sizeof(T));
+    static constexpr size_t OFF_X = OFF_RING + S * P::STAGE;
+    static constexpr size_t XB = align128(RBox<T>::BYTES);
+    static constexpr size_t BYTES = OFF_X + NXP * XB;
+    static_assert(S <= 16, "stage barriers: 128 bytes");
+};
+
+// A cell of a task: box positions in the T, code and coupling boxes, the parent
+// box position, its indices and its global offset in a level plane.
+struct FCell {
+    int qt, qc, qs, qq;
+    int i, j;
+    int gid;
+};
+
+template <class T, class CS>
+__device__ __forceinline__ FCell fcell(const Geom& g, int i0, int j0, int di, int dj) {
+    FCell c;
+    c.qt = RBox<T>::pos(di, dj);
+    c.qc = RBox<uint8_t>::pos(di, dj);
+    c.qs = RBox<CS>::pos(di, dj);
+    c.qq = ((dj + 2) >> 1) * QBox<T>::W + ((di + 2) >> 1);
+    c.i = i0 + di;
+    c.j = j0 + dj;
+    c.gid = c.i + c.j * g.sx;
+    return c;
+}
+
+// The ring tasks: pair t (t < 104) of the 1-cell ring (t < 50) or the 2-cell ring;
+// both cells of a pair are neighbours, so they have opposite colours.
+__device__ __forceinline__ void ring_pair(int t, int& d1i, int& d1j, int& d2i, int& d2j) {
+    if (t < 17) { d1i = 2 * t - 1; d2i = 2 * t; d1j = d2j = -1; }
+    else if (t < 34) { const int u = t - 17; d1i = 2 * u - 1; d2i = 2 * u; d1j = d2j = kMY; }
+    else if (t < 42) { const int u = t - 34; d1i = d2i = -1; d1j = 2 * u; d2j = 2 * u + 1; }
+    else if (t < 50) { const int u = t - 42; d1i = d2i = kMX; d1j = 2 * u; d2j = 2 * u + 1; }
+    else if (t < 68) { const int u = t - 50; d1i = 2 * u - 2; d2i = 2 * u - 1; d1j = d2j = -2; }
+    else if (t < 86) { const int u = t - 68; d1i = 2 * u - 2; d2i = 2 * u - 1; d1j = d2j = kMY + 1; }
+    else if (t < 95) { const int u = t - 86; d1i = d2i = -2; d1j = 2 * u - 1; d2j = 2 * u; }
+    else { const int u = t - 95; d1i = d2i = kMX + 1; d1j = 2 * u - 1; d2j = 2 * u; }
+}
+constexpr int kRing1Tasks = 50, kRingTasks = 104;
+
+template <int DIM, class T, class CS, bool FINE, bool UP>
+__device__ __forceinline__ void f_issue(const FMaps& M, unsigned char* st, uint64_t* bar, int k) {
+    using P = FPlan<DIM, T, CS, FINE, UP>;
+    const int x0 = kMX * (int)blockIdx.x, y0 = kMY * (int)blockIdx.y - 1;
+    fence_proxy_async();
+    mbar_expect_tx(bar, P::TX);
+    tma_load<DIM>(st + P::OFF_B, &M.b, x0 - RBox<T>::A, y0, k, bar);
+    tma_load<DIM>(st + P::OFF_CODE, &M.code, x0 - RBox<uint8_t>::A, y0, k, bar);
+    if constexpr (!FINE) {
+        tma_load<DIM>(st + P::OFF_DG, &M.dg, x0 - RBox<T>::A, y0, k, bar);
+        tma_load<DIM>(st + P::OFF_CX, &M.cx, x0 - RBox<CS>::A, y0, k, bar);
+        tma_load<DIM>(st + P::OFF_CY, &M.cy, x0 - RBox<CS>::A, y0, k, bar);
+        if constexpr (DIM == 3) tma_load<DIM>(st + P::OFF_CZ, &M.cz, x0 - RBox<CS>::A, y0, k, bar);
+    }
+    if constexpr (UP)
+        tma_load<DIM>(st + P::OFF_XC, &M.xc, x0 / 2, (y0 + 1) / 2, (k + 1) >> 1, bar);
+}
+
+// Planes p0 .. plast pass through S stages; plane p uses stage (p - p0) mod S.
+// Thread 0 issues every load and is the only thread that waits on the barriers.
+template <int DIM, class T, class CS, bool FINE, bool UP, int S>
+struct FRing {
+    using P = FPlan<DIM, T, CS, FINE, UP>;
+    uint64_t* bars;
+    unsigned char* base;
+    int p0, plast;
+    // stage of plane p (p >= p0 - S; planes below p0 are never read)
+    __device__ unsigned char* at(int p) const {
+        return base + (size_t)((p - p0 + 2 * S) % S) * P::STAGE;
+    }
+    __device__ bool wait(int p) const {
+        const int u = p - p0;
+        return mbar_wait(&bars[u % S], (uint32_t)((u / S) & 1), kTmaWaitLimit);
+    }
+    __device__ void start(const FMaps& M) const {
+        for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        for (int p = p0; p < p0 + S && p <= plast; ++p)
+            f_issue<DIM, T, CS, FINE, UP>(M, at(p), &bars[(p - p0) % S], p);
+    }
+    // after a block barrier: plane `freed` is no longer read; load plane freed + S
+    __device__ void refill(const FMaps& M, int freed) const {
+        if (freed >= p0 && freed + S <= plast)
+            f_issue<DIM, T, CS, FINE, UP>(M, at(freed + S), &bars[(freed - p0) % S], freed + S);
+    }
+};
+
+// Recent values of one column: the last two odd-colour values and the last
+// even-colour value computed for it.
+template <class T>
+struct FHist {
+    T o1, o2, e1;
+};
+
+// The dynamic shared memory of a fused march (128-byte aligned; see march.cuh).
+#define UAAMG_FUSED_SMEM(sm, err)                                                 \
+    extern __shared__ __align__(128) unsigned char smem_raw[];                   \
+    unsigned char* sm = smem_raw;                                                \
+    if (smem_u32(sm) & 127u) {                                                   \
+        if (threadIdx.x == 0) atomicExch(err, 2);                                \
+        return;                                                                  \
+    }
+
+template <int DIM, class T, bool FINE, class CS, bool UP, bool ZDOT>
+__global__ void __launch_bounds__(kThreads)
+    k_level_fused(const __grid_constant__ FMaps M, MLevel<T> L, const uint8_t* __restrict__ ccode,
+                  T* __restrict__ out, const int* __restrict__ done, int* err, double* partials,
+                  CGState* cg) {
+    if (done && *done) return;
+    using C = FCfg<DIM, T, CS, FINE, UP>;
+    using P = typename C::P;
+    constexpr int S = C::S, WT = RBox<T>::W, WS = RBox<CS>::W;
+    constexpr bool kFull = sizeof(T) == 8;  // the reference's residual expression
+    UAAMG_FUSED_SMEM(sm, err)
+    T* lut = reinterpret_cast<T*>(sm + C::OFF_LUT);
+    const Geom& g = L.g;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int i0 = 1 + kMX * (int)blockIdx.x, j0 = 1 + kMY * (int)blockIdx.y;
+    if (FINE) build_lut<DIM, T>(lut, L.idx2, L.idy2, L.idz2);
+
+    // --- per-cell arithmetic --------------------------------------------------
+    auto code_at = [&](const unsigned char* st, const FCell& c) -> uint32_t {
+        return st[P::OFF_CODE + c.qc];
+    };
+    auto b_at = [&](const unsigned char* st, const FCell& c) -> T {
+        return reinterpret_cast<const T*>(st + P::OFF_B)[c.qt];
+    };
+    auto diag_of = [&](const unsigned char* st, const FCell& c, uint32_t code, int k) -> T {
+        if constexpr (FINE) {
+            T d = lut[code & 63u];
+            if (L.dirichlet) d = d + wall_diag_at<DIM, T>(L, c.i, c.j, k);
+            return d;
+        } else {
+            return reinterpret_cast<const T*>(st + P::OFF_DG)[c.qt];
+        }
+    };
+    // couplings +x, -x, +y, -y, +z, -z (stc: this plane, stm: the plane below)
+    auto coup = [&](const unsigned char* stc, const unsigned char* stm, const FCell& c, T (&cc)[6]) {
+        if constexpr (FINE) {
+            cc[0] = cc[1] = L.idx2;
+            cc[2] = cc[3] = L.idy2;
+            cc[4] = cc[5] = L.idz2;
+        } else {
+            const CS* cx = reinterpret_cast<const CS*>(stc + P::OFF_CX);
+            const CS* cy = reinterpret_cast<const CS*>(stc + P::OFF_CY);
+            cc[0] = coupling<T, CS>(cx[c.qs], L.csx);
+            cc[1] = coupling<T, CS>(cx[c.qs - 1], L.csx);
+            cc[2] = coupling<T, CS>(cy[c.qs], L.csy);
+            cc[3] = coupling<T, CS>(cy[c.qs - WS], L.csy);
+            if constexpr (DIM == 3) {
+                cc[4] = coupling<T, CS>(reinterpret_cast<const CS*>(stc + P::OFF_CZ)[c.qs], L.csz);
+                cc[5] = coupling<T, CS>(reinterpret_cast<const CS*>(stm + P::OFF_CZ)[c.qs], L.csz);
+            } else {
+                cc[4] = cc[5] = T(0);
+            }
+        }
+    };
+    // sum c_n v_n in the reference's order (v: a shared x plane)
+    auto nbsum2 = [&](const T (&cc)[6], const T* v, int q, T vp, T vm) -> T {
+        T nb = cc[0] * v[q + 1] + cc[1] * v[q - 1] + cc[2] * v[q + WT] + cc[3] * v[q - WT];
+        if (DIM == 3) nb = nb + cc[4] * vp + cc[5] * vm;
+        return nb;
+    };
+    auto prolong = [&](const unsigned char* st, const FCell& c) -> T {
+        return T(2) * reinterpret_cast<const T*>(st + P::OFF_XC)[c.qq];
+    };
+    // odd-colour value at plane k: pre-smoothed (b + 0)/d, plus the prolongation on
+    // the way up; 0 on cells that are not interior fluid
+    auto oval = [&](const unsigned char* st, const FCell& c, int k) -> T {
+        const uint32_t code = code_at(st, c);
+        if (!(code & kActive)) return T(0);
+        const T d = diag_of(st, c, code, k);
+        const T pre = d < T(1e-30) ? T(0) : mdiv<T, CS>(b_at(st, c) + T(0), d);
+        if constexpr (UP) return pre + prolong(st, c);
+        else return pre;
+    };
+    // even-colour value at plane k from the odd values around it: forward sweep
+    // (way down) or first colour of the reverse sweep (way up; a skipped cell keeps
+    // 0 + the prolongation)
+    auto evalc = [&](const unsigned char* st, const unsigned char* stm, const T* xv, const FCell& c,
+                     int k, T op, T om) -> T {
+        const uint32_t code = code_at(st, c);
+        if (!(code & kActive)) return T(0);
+        const T d = diag_of(st, c, code, k);
+        if (d < T(1e-30)) {
+            if constexpr (UP) return T(0) + prolong(st, c);
+            else return T(0);
+        }
+        T cc[6];
+        coup(st, stm, c, cc);
+        return mdiv<T, CS>(b_at(st, c) + nbsum2(cc, xv, c.qt, op, om), d);
+    };
+
+    // --- tasks ---------------------------------------------------------------
+    // tile pair: A = (i0 + lane, j0 + 2w), B = (i0 + lane, j0 + 2w + 1)
+    const FCell cA = fcell<T, CS>(g, i0, j0, lane, 2 * w);
+    const FCell cB = fcell<T, CS>(g, i0, j0, lane, 2 * w + 1);
+    const bool ring = tid < kRingTasks, ring1 = tid < kRing1Tasks;
+    FCell cR1, cR2;
+    {
+        int d1i = 0, d1j = 0, d2i = 0, d2j = 0;
+        if (ring) ring_pair(tid, d1i, d1j, d2i, d2j);
+        cR1 = fcell<T, CS>(g, i0, j0, d1i, d1j);
+        cR2 = fcell<T, CS>(g, i0, j0, d2i, d2j);
+    }
+    int kb, ke;
+    zrange<DIM>(g, L.zc, kb, ke);
+    T* xpl = reinterpret_cast<T*>(sm + C::OFF_X);
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int ic = kMX / 2 * (int)blockIdx.x + 1 + (lane >> 1);
+    const int jc = kMY / 2 * (int)blockIdx.y + 1 + w;
+    const bool writer = !UP && (lane & 1) == 0 && ic <= L.cg.nx && jc <= L.cg.ny;
+
+    // Final step on the tile pair at plane k, in colour order: cO / cE are the pair's
+    // odd and even cells there, vO / vE their x values, zp* / zm* their columns'
+    // values at k+1 and k-1; aOdd: A is the odd cell.  rlo: the way down's dk = 0
+    // residuals, kept from the odd plane below.
+    auto final_pair = [&](const unsigned char* st, const unsigned char* stm, const T* xv, int k,
+                          const FCell& cO, const FCell& cE, bool aOdd, T vO, T vE, T zpO, T zmO,
+                          T zpE, T zmE, T (&rlo)[2]) {
+        const uint32_t kO = code_at(st, cO), kE = code_at(st, cE);
+        T resO = UP ? vO : T(0), resE = UP ? vE : T(0);
+        if (kO & kActive) {  // odd cell: reverse-sweep update / residual
+            const T d = diag_of(st, cO, kO, k);
+            if constexpr (UP) {
+                if (!(d < T(1e-30))) {
+                    T cc[6];
+                    coup(st, stm, cO, cc);
+                    resO = mdiv<T, CS>(b_at(st, cO) + nbsum2(cc, xv, cO.qt, zpO, zmO), d);
+                }
+            } else if constexpr (kFull) {
+                T cc[6];
+                coup(st, stm, cO, cc);
+                T ax = d * vO - cc[0] * xv[cO.qt + 1] - cc[1] * xv[cO.qt - 1] -
+                       cc[2] * xv[cO.qt + WT] - cc[3] * xv[cO.qt - WT];
+                if (DIM == 3) ax = ax - cc[4] * zpO - cc[5] * zmO;
+                resO = b_at(st, cO) - ax;
+            } else {
+                if (d < T(1e-30)) {
+                    resO = b_at(st, cO);
+                } else {
+                    T cc[6];
+                    coup(st, stm, cO, cc);
+                    resO = nbsum2(cc, xv, cO.qt, zpO, zmO);
+                }
+            }
+        }
+        if constexpr (!UP) {
+            if (kE & kActive) {  // even cell: residual (0 after its relaxation in FP32)
+                const T d = diag_of(st, cE, kE, k);
+                if constexpr (kFull) {
+                    T cc[6];
+                    coup(st, stm, cE, cc);
+                    T ax = d * vE - cc[0] * xv[cE.qt + 1] - cc[1] * xv[cE.qt - 1] -
+                           cc[2] * xv[cE.qt + WT] - cc[3] * xv[cE.qt - WT];
+                    if (DIM == 3) ax = ax - cc[4] * zpE - cc[5] * zmE;
+                    resE = b_at(st, cE) - ax;
+                } else {
+                    if (d < T(1e-30)) resE = b_at(st, cE);
+                }
+            }
+        }
+        if constexpr (UP) {
+            const int base = k * g.sxy;
+            const bool inO = cO.i <= g.nx && cO.j <= g.ny, inE = cE.i <= g.nx && cE.j <= g.ny;
+            if (inO) out[cO.gid + base] = resO;
+            if (inE) out[cE.gid + base] = resE;
+            if (ZDOT) {
+                if ((kO & kActive) && inO) {
+                    const double zv = (double)resO, rv = (double)b_at(st, cO);
+                    acc[0] += zv;
+                    acc[1] += rv * zv;
+                    acc[2] += rv;
+                }
+                if ((kE & kActive) && inE) {
+                    const double zv = (double)resE, rv = (double)b_at(st, cE);
+                    acc[0] += zv;
+                    acc[1] += rv * zv;
+                    acc[2] += rv;
+                }
+            }
+        } else {
+            const T res[2] = {aOdd ? resO : resE, aOdd ? resE : resO};  // [dj]
+            // restriction: children dk = 0 on odd planes; the set is complete on the
+            // even plane that follows (2D: one plane)
+            if (DIM == 3 && (k & 1)) {
+                rlo[0] = res[0];
+                rlo[1] = res[1];
+            } else {
+                T pr[2][2];  // the di = 1 partner's values [dj][dk]
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    pr[e][0] = __shfl_down_sync(0xffffffffu, DIM == 3 ? rlo[e] : res[e], 1);
+                    pr[e][1] = __shfl_down_sync(0xffffffffu, res[e], 1);
+                }
+                if (writer) {
+                    const int kc = DIM == 3 ? k / 2 : 0;
+                    const int cid = cidx(L.cg, ic, jc, kc);
+                    T sum = T(0);
+                    if (DIM == 3) {
+                        sum += rlo[0]; sum += res[0]; sum += rlo[1]; sum += res[1];
+                        sum += pr[0][0]; sum += pr[0][1]; sum += pr[1][0]; sum += pr[1][1];
+                    } else {
+                        sum += res[0]; sum += res[1];
+                        sum += pr[0][1]; sum += pr[1][1];
+                    }
+                    out[cid] = (ccode[cid] & kActive) ? sum : T(0);
+                }
+            }
+        }
+    };
+
+    T rlo[2] = {T(0), T(0)};
+    if constexpr (DIM == 2) {
+        // one plane: odd values, barrier, even values, barrier, final
+        unsigned char* st = sm + C::OFF_RING;
+        uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+        bool ok = true;
+        if (tid == 0) {
+            mbar_init(bar, 1);
+            f_issue<DIM, T, CS, FINE, UP>(M, st, bar, 0);
+            ok = mbar_wait(bar, 0u, kTmaWaitLimit);
+        }
+        if (!step_barrier(ok, err)) return;
+        // A is odd when i + j is odd; ring pairs likewise
+        const bool oddA = ((cA.i + cA.j) & 1) != 0;
+        const FCell tO = oddA ? cA : cB, tE = oddA ? cB : cA;
+        const bool odd1 = ((cR1.i + cR1.j) & 1) != 0;
+        const FCell rO = odd1 ? cR1 : cR2, rE = odd1 ? cR2 : cR1;
+        const T ot = oval(st, tO, 0);
+        xpl[tO.qt] = ot;
+        if (ring) xpl[rO.qt] = oval(st, rO, 0);
+        __syncthreads();
+        const T et = evalc(st, st, xpl, tE, 0, T(0), T(0));
+        xpl[tE.qt] = et;
+        if (ring1) xpl[rE.qt] = evalc(st, st, xpl, rE, 0, T(0), T(0));
+        __syncthreads();
+        final_pair(st, st, xpl, 0, tO, tE, oddA, ot, et, T(0), T(0), T(0), T(0), rlo);
+    } else {
+        // steps s = kb-3 .. ke: odd values of planes kb-2 .. ke+1, even values of
+        // kb-1 .. ke, final results of kb .. ke-1
+        const int s0 = kb - 3;
+        FRing<DIM, T, CS, FINE, UP, S> R{reinterpret_cast<uint64_t*>(sm), sm + C::OFF_RING, kb - 2,
+                                         ke + 1};
+        bool ok = true;
+        if (tid == 0) {
+            R.start(M);
+            ok = R.wait(R.p0);
+        }
+        if (!step_barrier(ok, err)) return;
+        // role 0 is the cell that is even on planes s0, s0+2, ... (odd on s0+1, ...)
+        const bool aRole0 = ((cA.i + cA.j + s0) & 1) == 0;
+        const FCell t0 = aRole0 ? cA : cB, t1 = aRole0 ? cB : cA;
+        const bool r1Role0 = ((cR1.i + cR1.j + s0) & 1) == 0;
+        const FCell q0 = r1Role0 ? cR1 : cR2, q1 = r1Role0 ? cR2 : cR1;
+        FHist<T> ht[2] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
+        T hr[2] = {T(0), T(0)};  // ring columns: last odd value
+        auto xp_of = [&](int p) -> T* { return xpl + (size_t)((p + 3) % 3) * (C::XB / sizeof(T)); };
+        // one step; R0: the role whose cell is even at plane s (compile-time)
+        auto step = [&](int s, auto R0c) -> bool {
+            constexpr int RC = decltype(R0c)::value, RO = 1 - RC;
+            const FCell& tc = RC == 0 ? t0 : t1;
+            const FCell& qc = RC == 0 ? q0 : q1;
+            const unsigned char* sp1 = R.at(s + 1);
+            const unsigned char* s00 = R.at(s);
+            const unsigned char* sm1 = R.at(s - 1);
+            const unsigned char* sm2 = R.at(s - 2);
+            T* xn = xp_of(s + 1);
+            T* xc = xp_of(s);
+            const T* xo = xp_of(s - 1);
+            // 1. odd values of plane s+1
+            const T on = oval(sp1, tc, s + 1);
+            xn[tc.qt] = on;
+            T onr = T(0);
+            if (ring) {
+                onr = oval(sp1, qc, s + 1);
+                xn[qc.qt] = onr;
+            }
+            // 2. even values of plane s
+            T en = T(0);
+            if (s >= kb - 1) {
+                en = evalc(s00, sm1, xc, tc, s, on, ht[RC].o1);
+                xc[tc.qt] = en;
+                if (ring1) xc[qc.qt] = evalc(s00, sm1, xc, qc, s, onr, hr[RC]);
+            }
+            // 3. final results of plane s-1: the role-RC cell is odd there
+            if (s >= kb + 1) {
+                const int p = s - 1;
+                const T vR = ht[RC].o1, vO = ht[RO].e1;   // x at p
+                const T zpR = en, zmR = ht[RC].e1;         // role RC: even values at p+1, p-1
+                const T zpO = ht[RO].o1, zmO = ht[RO].o2;  // role RO: odd values at p+1, p-1
+                const FCell& to = RC == 0 ? t1 : t0;
+                final_pair(sm1, sm2, xo, p, tc, to, aRole0 == (RC == 0), vR, vO, zpR, zmR, zpO, zmO,
+                           rlo);
+            }
+            ht[RC].o2 = ht[RC].o1;
+            ht[RC].o1 = on;
+            ht[RC].e1 = en;
+            hr[RC] = onr;
+            bool okk = true;
+            if (tid == 0 && s + 2 <= R.plast) okk = R.wait(s + 2);
+            if (!step_barrier(okk, err)) return false;
+            if (tid == 0) R.refill(M, s - C::LAG);
+            return true;
+        };
+#pragma unroll 1
+        for (int s = s0; s <= ke; s += 2) {
+            if (!step(s, std::integral_constant<int, 0>())) return;
+            if (s + 1 <= ke && !step(s + 1, std::integral_constant<int, 1>())) return;
+        }
+    }
+    if constexpr (UP && ZDOT) {
+        double tot[3];
+        if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
+    }
+}
+
+#undef UAAMG_FUSED_SMEM
+
+}  // namespace
+}  // namespace uaamg

@@ -28,8 +28,10 @@ struct uaamg_handle {
     int last_iters = 0;
     uaamg::Engine* eng[3] = {nullptr, nullptr, nullptr};
     bool ready[3] = {false, false, false};
-    int sweeps = 0;  // V-cycle kernels: 0 marches + small-level kernel, 1 sweeps, 2 marches,
-                     // 3 as 0 with 2D march levels as flat walks
+    int sweeps = 0;  // V-cycle kernels (uaamg_set_vcycle_kernels): 0 fused marches +
+                     // small-level kernel, 1 sweeps, 2 fused marches on every level,
+                     // 3 as 0 with 2D march levels as flat walks, 4 four marches a level
+                     // + small-level kernel, 5 four marches on every level
     int autotune = 0;
     std::string err;
     struct BatchPool* batch = nullptr;  // runtime.cpp: per-problem slots of uaamg_solve_batch
@@ -46,6 +48,14 @@ uaamg_status map_engine(uaamg_handle* h, int e, const char* where,
 uaamg_status fill_stats(const uaamg::Engine* eng, const uaamg::SolveResult& r, uaamg_stats* st);
 // Frees the batch slots of a handle (runtime.cpp).
 void free_batch(uaamg_handle* h);
+
+// The engine flags of a V-cycle kernel mode (uaamg_set_vcycle_kernels).
+inline void apply_vcycle_mode(uaamg::Engine* e, int mode) {
+    e->set_vcycle_sweeps(mode == 1);
+    e->set_small_levels(mode == 0 || mode == 3 || mode == 4);
+    e->set_flat2d(mode == 3);
+    e->set_fused(mode == 0 || mode == 2 || mode == 3);
+}
 
 }  // namespace api
 }  // namespace uaamg

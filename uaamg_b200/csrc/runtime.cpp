@@ -188,9 +188,7 @@ uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_problem* prob
         DevProblem& d = slots[i];
         int e = d.prepare(opts.precision, p.dim, p.nx, p.ny, p.nz, p.dx, p.dy, p.dz, h->dirichlet);
         if (e == E_OK) {
-            d.eng->set_vcycle_sweeps(h->sweeps == 1);
-            d.eng->set_small_levels(h->sweeps == 0 || h->sweeps == 3);
-            d.eng->set_flat2d(h->sweeps == 3);
+            uaamg::api::apply_vcycle_mode(d.eng, h->sweeps);
             d.eng->set_autotune(h->autotune != 0);
             e = d.build(p.solid);
         }
@@ -280,14 +278,23 @@ struct Ticket {
     bool done = false;
     int slot = -1;
     SimState* sim = nullptr;
+    bool ending = false;     // exit work queued; waiting for the slot's event
+    int status = UAAMG_OK;   // result status once collected (the pressure copy may follow)
 };
 
-// Pinned host staging of one concurrent solve.
+// Pinned host staging of one concurrent solve, and the event recorded behind its
+// exit work and pressure copy.
 struct StageBuf {
     double* h = nullptr;
     size_t cap = 0;
     bool used = false;
+    cudaEvent_t ev = nullptr;
     bool ensure(size_t n) {
+        if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            ev = nullptr;
+            return false;
+        }
         if (n <= cap) return true;
         if (h) cudaFreeHost(h);
         h = nullptr;
@@ -326,6 +333,14 @@ struct uaamg_server {
     std::unordered_map<long long, uaamg::SimState*> sims;
     std::vector<uaamg::Ticket*> active;
     std::vector<uaamg::StageBuf> stage;
+    // results whose pressure is copied into the caller's p_out by the completion
+    // thread (from the pinned staging), so the worker never waits on a host copy
+    std::thread completer;
+    std::condition_variable cv_copy;
+    std::deque<uaamg::Ticket*> to_copy;  // under mu
+    std::deque<uaamg::Ticket*> copied;   // under mu; the worker finishes them
+    int copying = 0;                     // under mu: handed over, not yet finished
+    bool stop_copier = false;
     size_t resident_bytes = 0;
     int resident = 0;
     uint64_t tick = 0;
@@ -452,47 +467,96 @@ bool start_request(uaamg_server* s, Ticket* t) {
     return true;
 }
 
-// Advances one running request; true when it finished.
+// Advances one running request without blocking; true when it leaves the active
+// list (finished, or handed to the completion thread for its pressure copy).  A
+// stopped solve first queues its exit work and the pressure's device-to-host copy
+// into the slot's pinned staging, with the slot's event behind them; the result
+// is collected on a later pass, once the event reports done.
 bool advance(uaamg_server* s, Ticket* t) {
     DevProblem& d = t->sim->dp;
-    bool stopped = false;
-    int e = d.eng->solve_step();
-    if (e == E_OK) e = d.eng->solve_poll(false, &stopped);
-    if (e == E_OK && !stopped) return false;
+    StageBuf& b = s->stage[t->slot];
+    if (!t->ending) {
+        bool stopped = false;
+        int e = d.eng->solve_step();
+        if (e == E_OK) e = d.eng->solve_poll(false, &stopped);
+        if (e == E_OK && !stopped) return false;
+        if (e == E_OK) e = d.eng->solve_end_enqueue();
+        cudaError_t ce = cudaSuccess;
+        if (e == E_OK && t->req.p_out)
+            ce = cudaMemcpyAsync(b.h, d.d_p, d.n * sizeof(double), cudaMemcpyDeviceToHost, d.stream);
+        if (e == E_OK && ce == cudaSuccess) ce = cudaEventRecord(b.ev, d.stream);
+        if (e != E_OK || ce != cudaSuccess) {
+            t->sim->has_p = false;
+            finish(s, t, UAAMG_CUDA_ERROR);
+            return true;
+        }
+        t->ending = true;
+        return false;
+    }
+    const cudaError_t q = cudaEventQuery(b.ev);
+    if (q == cudaErrorNotReady) return false;
     SolveResult r;
     std::memset(&r, 0, sizeof(r));
-    if (e == E_OK) e = d.eng->solve_end(&r);
+    int e = q == cudaSuccess ? d.eng->solve_end_collect(&r) : E_CUDA;
     if (e != E_OK || d.eng->timed_out()) {
         t->sim->has_p = false;
         finish(s, t, e == E_OK ? UAAMG_TIMEOUT : UAAMG_CUDA_ERROR);
         return true;
     }
-    StageBuf& b = s->stage[t->slot];
-    cudaError_t ce = cudaSuccess;
-    if (t->req.p_out) {
-        ce = cudaMemcpyAsync(b.h, d.d_p, d.n * sizeof(double), cudaMemcpyDeviceToHost, d.stream);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(d.stream);
-        if (ce == cudaSuccess) std::memcpy(t->req.p_out, b.h, d.n * sizeof(double));
-    }
     uaamg_stats st;
-    const uaamg_status status = api::fill_stats(d.eng, r, &st);
+    t->status = api::fill_stats(d.eng, r, &st);
     t->res.iterations = st.iterations;
     t->res.rel_residual = st.rel_residual;
-    t->sim->has_p = ce == cudaSuccess;
-    finish(s, t, ce == cudaSuccess ? status : UAAMG_CUDA_ERROR);
+    t->sim->has_p = true;
+    if (!t->req.p_out) {
+        finish(s, t, t->status);
+        return true;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->to_copy.push_back(t);
+    s->copying += 1;
+    s->cv_copy.notify_one();
     return true;
+}
+
+// Completion thread: copies finished pressures from the pinned staging into the
+// callers' p_out; the worker then finishes those tickets (slot and id released).
+void copier_main(uaamg_server* s) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv_copy.wait(lk, [&] { return s->stop_copier || !s->to_copy.empty(); });
+        if (s->to_copy.empty()) return;  // stop_copier and nothing left
+        Ticket* t = s->to_copy.front();
+        s->to_copy.pop_front();
+        lk.unlock();
+        std::memcpy(t->req.p_out, s->stage[t->slot].h, t->sim->dp.n * sizeof(double));
+        lk.lock();
+        s->copied.push_back(t);
+        s->cv.notify_all();
+    }
 }
 
 void worker_main(uaamg_server* s) {
     cudaSetDevice(s->cfg.device);
     for (;;) {
+        // results whose pressure copy the completion thread has finished
+        std::deque<Ticket*> done_copies;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            done_copies.swap(s->copied);
+            s->copying -= (int)done_copies.size();
+        }
+        for (Ticket* t : done_copies) finish(s, t, t->status);
         // admission: FIFO over the queue; a request waits while its id is busy
         std::vector<Ticket*> admit;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             if (s->pending.empty() && s->active.empty()) {
-                if (s->stopping) break;
-                s->cv.wait(lk, [&] { return s->stopping || !s->pending.empty(); });
+                if (s->stopping && s->copying == 0) break;
+                s->cv.wait(lk, [&] {
+                    return (s->stopping && s->copying == 0) || !s->pending.empty() ||
+                           !s->copied.empty();
+                });
                 continue;
             }
             int room = s->cfg.max_active - (int)s->active.size();
@@ -570,6 +634,7 @@ uaamg_status uaamg_server_start(uaamg_server** out, const uaamg_server_config* c
     if (!s) return UAAMG_OOM;
     s->cfg = c;
     s->stage.resize(c.max_active);
+    s->completer = std::thread(uaamg::copier_main, s);
     s->worker = std::thread(uaamg::worker_main, s);
     *out = s;
     return UAAMG_OK;
@@ -641,14 +706,22 @@ uaamg_status uaamg_server_stop(uaamg_server* s) {
         s->cv.notify_all();
     }
     if (s->worker.joinable()) s->worker.join();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop_copier = true;
+        s->cv_copy.notify_all();
+    }
+    if (s->completer.joinable()) s->completer.join();
     cudaSetDevice(s->cfg.device);
     for (auto& kv : s->sims) {
         kv.second->dp.release();
         delete kv.second;
     }
     s->sims.clear();
-    for (auto& b : s->stage)
+    for (auto& b : s->stage) {
         if (b.h) cudaFreeHost(b.h);
+        if (b.ev) cudaEventDestroy(b.ev);
+    }
     // every ticket not yet released by a poll is in the map (queued or finished)
     for (auto& kv : s->tickets) delete kv.second;
     delete s;

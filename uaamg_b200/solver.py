@@ -129,9 +129,11 @@ class Handle:
         self._check(self.lib.uaamg_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
 
     def set_vcycle_kernels(self, mode):
-        """0 / False: z marches + the single-block small-level kernel (default);
-        1 / True: per-colour sweep kernels; 2: z marches on every level; 3: as 0 with
-        every march level of a 2D problem as flat walks."""
+        """0 / False: two fused z marches a level + the single-block small-level
+        kernel (default); 1 / True: per-colour sweep kernels; 2: fused marches on every
+        level; 3: as 0 with every march level of a 2D problem as four flat walks;
+        4: four z marches a level + the small-level kernel; 5: four marches on every
+        level."""
         self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(mode)), "vcycle")
 
     def set_variable_laplacian(self, lap_diag=None, lap_off_x=None, lap_off_y=None):
