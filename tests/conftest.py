@@ -24,7 +24,10 @@ def pytest_configure(config):
 
 
 def golden_names(prefix=""):
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith(prefix))
+    """Golden cases (one solve or V-cycle each); the 256^3 reference pressure samples
+    (spheres_256_reference_p.npz) are read by their own tests."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN)
+                  if f.endswith(".npz") and f.startswith(prefix) and not f.startswith("spheres_256_"))
 
 
 def load_golden(name):
