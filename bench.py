@@ -318,6 +318,7 @@ def run_ours(args):
     value = elapsed / (args.steps * ws)
     clocks = clk.summary()
     stats = st.as_dict()
+    dev_bytes = hd.device_bytes()
 
     # e2e: the host-array C-ABI call, pinned host buffers, copies inside the timing
     h_rhs = torch.from_numpy(rhs).pin_memory()
@@ -456,6 +457,68 @@ def run_ours(args):
             "note": "device_ms = divergence + solve + face correction with u, v, p on the GPU",
         }
 
+    # set-up cost, as paid when the solids move: a new problem (same shape, so the
+    # z-chunk choices are cached), its hierarchy, couplings, tensor maps and CUDA-graph
+    # capture, measured as the first solve after uaamg_set_problem minus a steady solve
+    setup = None
+    if rank == 0 and not args.no_beside:
+        torch.cuda.synchronize()
+        c0 = time.perf_counter()
+        hd.set_problem(solid, dx, dy, dz)
+        if lap is not None:
+            hd.set_variable_laplacian(*lap)
+        d_p.zero_()
+        hd.solve_device(d_rhs.data_ptr(), d_p.data_ptr(), opts)
+        torch.cuda.synchronize()
+        first = (time.perf_counter() - c0) * 1e3
+        setup = {"set_problem_plus_first_solve_ms": round(first, 2),
+                 "setup_ms": round(first - ms_per_step, 2),
+                 "note": "hierarchy, codes, couplings, tensor maps, graph capture; paid again "
+                         "whenever the mask changes"}
+
+    # error of the headline solution against an FP64 solve to 1e-10 (fluid-mean-free
+    # relative L2), and the reference's own CUDA solver on the same GPU
+    if rank == 0 and not args.no_beside:
+        d_p.zero_()
+        hd.solve_device(d_rhs.data_ptr(), d_p.data_ptr(), opts)
+        p_head = d_p.cpu().numpy()
+        d_p.zero_()
+        hd.solve_device(d_rhs.data_ptr(), d_p.data_ptr(), hd.options("fp64", 1e-10, 1000, "rel"))
+        p_64 = d_p.cpu().numpy()
+        fl = np.zeros(solid.shape, bool)
+        fl[(slice(1, -1),) * solid.ndim] = True
+        fl &= solid == 0
+        a_, b_ = p_head[fl] - p_head[fl].mean(), p_64[fl] - p_64[fl].mean()
+        beside["err_vs_fp64"] = float(np.linalg.norm(a_ - b_) / np.linalg.norm(b_))
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        if args.workload == "spheres_256" and ws == 1 and O.have_ref_gpu():
+            rg = {}
+            for name, mode in (("solve_optimized_fp64", 0), ("solve_mixed", 1)):
+                pr, msr, itr, relr = O.ref_gpu_pcg3d(solid, rhs, h, h, h, max_iter=500, tol=1e-6,
+                                                     mode=mode, reps=2)
+                ra, rb = O.true_residual(solid, rhs, pr, h, h, h)
+                rg[name] = {"ms": round(msr, 3), "iterations": itr,
+                            "reported_rel_residual": relr, "true_rel_residual": ra / rb}
+            rg["note"] = ("the reference's CudaPCG3D (cuda_pcg_3d_opt.cu), compiled for sm_100a, "
+                          "mean of 2 solves after one untimed, CUDA events, same GPU")
+            beside["reference_gpu"] = rg
+
+    # serving (config-5 mix, bounded): mixed and plain FP32, closed loop; mixed also
+    # open loop at 80 % of its capacity
+    served = None
+    if rank == 0 and ws == 1 and args.served_ids > 0 and not args.no_beside:
+        hd.close()
+        hd = None
+        torch.cuda.empty_cache()
+        forms, n_req = serve_forms(args, device, 0, 1, args.served_ids, args.serve_steps,
+                                   [args.precision, "fp32"])
+        served = {"requests": n_req, "simulation_ids": args.served_ids,
+                  "steps_per_id": args.serve_steps, "max_active": args.serve_active,
+                  "forms": forms,
+                  "note": "config-5 generator (serve10k) bounded to served_ids ids; latency = "
+                          "scheduled arrival -> result on the host"}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         if args.workload == "spheres_256" and os.path.exists(REF_ITER_FIXTURE):
@@ -481,7 +544,7 @@ def run_ours(args):
                    "true_rel_residual": stats["rel_residual"],
                    "host_checked_rel_residual": res / bn,
                    "autotune": bool(args.autotune), "vcycle_kernels": args.vcycle_kernels,
-                   "l2": f"inputs larger than L2 (solve working set ~{hd.device_bytes() / 1e9:.2f} GB "
+                   "l2": f"inputs larger than L2 (solve working set ~{dev_bytes / 1e9:.2f} GB "
                          "vs 126 MB L2)",
                    "parallelism": f"replicas x{ws}"},
         "roofline": roofline,
@@ -493,10 +556,15 @@ def run_ours(args):
         "kernels": kernels,
         "beside": beside,
     }
+    if setup is not None:
+        line["setup"] = setup
+    if served is not None:
+        line["served"] = served
     if projection is not None:
         line["projection"] = projection
     print(json.dumps(line), flush=True)
-    hd.close()
+    if hd is not None:
+        hd.close()
     return 0
 
 
@@ -709,25 +777,18 @@ def _serve_pass(srv, reqs, make, rate=None, max_outstanding=256, check=()):
     return results, wall, kept
 
 
-def run_serve(args):
-    """10,000 served requests (500 simulation ids x 20 steps): closed-loop capacity,
-    then open-loop Poisson arrivals at 80 % of it; p50/p99 latency, solves/s.  With N
-    GPUs each rank serves the simulation ids it owns (uaamg_b200.shard.owns) on its own
-    GPU; rates are summed over the ranks and latencies pooled."""
+def serve_forms(args, device, rank, ws, n_ids, steps, precs):
+    """Serves n_ids simulation ids x steps requests of the config-5 mix on this rank's
+    GPU (the ids it owns), per precision in precs: closed-loop capacity, and for
+    the first precision also open-loop Poisson arrivals at 80 % of it.  Returns
+    ({precision: summary}, number of requests of this rank)."""
     import concurrent.futures as cf
 
     import numpy as np
-    import torch
 
     from uaamg_b200 import shard, workloads
     from uaamg_b200.solver import Server
 
-    ws, rank, local = _dist()
-    device = local if ws > 1 else 0
-    if ws > 1:
-        _init_group(ws, local)
-    torch.cuda.set_device(device)
-    n_ids, steps = args.serve_ids, args.serve_steps
     plan = workloads.serve_plan(n_ids, steps)
     mine = [sid for sid in range(n_ids) if shard.owns(sid, rank, ws)]
     with cf.ThreadPoolExecutor(8) as ex:
@@ -753,14 +814,15 @@ def run_serve(args):
                 "all_ok": all(r["status"] == 0 for r in res)}
 
     out = {}
-    for prec in ([args.precision, "fp32"] if not args.no_beside else [args.precision]):
+    for prec in precs:
         srv = Server(device, prec, 1e-6, 500, max_active=args.serve_active)
         # warm-up: every id's hierarchy and graph, not timed
         _serve_pass(srv, [(sid, 0) for sid in mine], make)
-        closed, wall_c, _ = _serve_pass(srv, reqs, make)
+        closed, wall_c, kept_c = _serve_pass(srv, reqs, make, check=check)
         cap = len(reqs) / wall_c  # this rank's capacity
         entry = {"closed_loop": summary(shard.gather(closed), shard.reduce_sum(cap))}
-        if prec == args.precision:
+        kept = kept_c
+        if prec == precs[0]:
             srv.stop()
             srv = Server(device, prec, 1e-6, 500, max_active=args.serve_active)
             _serve_pass(srv, [(sid, 0) for sid in mine], make)
@@ -770,14 +832,32 @@ def run_serve(args):
             entry["open_loop"]["arrival_rate_per_s"] = round(shard.reduce_sum(0.8 * cap), 1)
             entry["clocks"] = clk.summary()
             entry["info"] = srv.info()
-            worst = 0.0
-            for i, (p, solid, rhs, h) in kept.items():
-                a, b = O.true_residual(solid, rhs, p, h, h, h if solid.ndim == 3 else 1.0)
-                worst = max(worst, a / b)
-            entry["checked_true_rel_residual_max"] = shard.reduce_max(worst)
-            entry["checked_requests"] = int(shard.reduce_sum(len(kept)))
+        worst = 0.0
+        for i, (p, solid, rhs, h) in kept.items():
+            a, b = O.true_residual(solid, rhs, p, h, h, h if solid.ndim == 3 else 1.0)
+            worst = max(worst, a / b)
+        entry["checked_true_rel_residual_max"] = shard.reduce_max(worst)
+        entry["checked_requests"] = int(shard.reduce_sum(len(kept)))
         srv.stop()
         out[prec] = entry
+    return out, len(reqs)
+
+
+def run_serve(args):
+    """10,000 served requests (500 simulation ids x 20 steps): closed-loop capacity,
+    then open-loop Poisson arrivals at 80 % of it; p50/p99 latency, solves/s.  With N
+    GPUs each rank serves the simulation ids it owns (uaamg_b200.shard.owns) on its own
+    GPU; rates are summed over the ranks and latencies pooled."""
+    import torch
+
+    ws, rank, local = _dist()
+    device = local if ws > 1 else 0
+    if ws > 1:
+        _init_group(ws, local)
+    torch.cuda.set_device(device)
+    n_ids, steps = args.serve_ids, args.serve_steps
+    precs = [args.precision, "fp32"] if not args.no_beside else [args.precision]
+    out, n_reqs = serve_forms(args, device, rank, ws, n_ids, steps, precs)
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -788,7 +868,7 @@ def run_serve(args):
     line = {
         "metric": "served pressure solves/s and p99 latency (1e-6 rel. residual)",
         "value": main_["open_loop"]["solves_per_s"], "unit": "solves/s", "n_gpus": ws,
-        "steps": len(reqs), "warmup": n_ids, "higher_is_better": True, "scaling": "weak",
+        "steps": n_reqs, "warmup": n_ids, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP64 reductions and solution)", "data": "synthetic",
         "config": {"workload": f"serve10k: {n_ids} simulation ids x {steps} steps, 70% 2D n^2 "
                                "(n lognormal median 384, [64, 2048]), 30% 3D n^3 (median 96, "
@@ -827,6 +907,9 @@ def main():
                     help="uaamg_set_vcycle_kernels mode (0 default: two fused marches a "
                          "level; 3: 2D levels as flat walks; 4: four marches a level)")
     ap.add_argument("--serve-ids", type=int, default=500)
+    ap.add_argument("--served-ids", type=int, default=100,
+                    help="simulation ids of the bounded serving run in the default line "
+                         "(0: none)")
     ap.add_argument("--serve-steps", type=int, default=20)
     ap.add_argument("--serve-active", type=int, default=16)
     args = ap.parse_args()

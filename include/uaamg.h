@@ -243,7 +243,8 @@ UAAMG_API uaamg_status uaamg_profile_solve(uaamg_handle* h, const double* d_rhs,
  * Scratch is a 16.4 KiB file-scope device array (held by every GPU that loads the
  * library until exit); grids of 2^31 padded cells or more are rejected.  The
  * first call on a device looks up that array and should come before any stream
- * capture; calls that overlap on the GPU share the array and race.
+ * capture (after a device reset, the first call in the new context looks it up
+ * again); calls that overlap on the GPU share the array and race.
  * This entry point has no counterpart in the reference. */
 UAAMG_API uaamg_status uaamg_residual_noalloc(int dim, int nx, int ny, int nz, double dx,
                                               double dy, double dz, const uint8_t* d_solid,

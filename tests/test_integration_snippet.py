@@ -25,22 +25,30 @@ LIB = os.path.join(ROOT, "uaamg_b200", "libuaamg_b200.so")
 def _snippet():
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     sec = text[text.index("## 2. The Solver subclass"):text.index("## 3.")]
-    header, factory = re.findall(r"```cpp\n(.*?)```", sec, re.S)[:2]
+    header, factory, factory3d, kind = re.findall(r"```cpp\n(.*?)```", sec, re.S)[:4]
     header = header.replace("#pragma once\n", "")
-    return header + """
+    return header + kind + """
 #include <memory>
 #include <string>
 #include "core/grid.h"
 #include "core/grid_3d.h"
+#include "solver/pcg_3d.h"
+#include "solver/preconditioner/uaamg_preconditioner_3d.h"
 
 std::unique_ptr<Solver> make_solver(const std::string& name) {
 """ + factory + """
     return nullptr;
 }
 
+std::unique_ptr<Solver3D> make_solver_3d(const std::string& name) {
+""" + factory3d + """
+    return nullptr;
+}
+
 int main(int argc, char**) {
-    if (argc > 1) {  // never taken in the test: building is the check
-        auto s = make_solver("pcg_uaamg_gpu");
+    if (argc > 1) {  // never taken in this test (tests/test_gpu_integration.py runs it)
+        auto s = make_solver(solver_key(solver_kind("pcg_uaamg_gpu")));
+        auto s3d = make_solver_3d("pcg_uaamg_gpu");
         Grid g(8, 4, 1.0, 0.5);
         g.init_variable_lap();
         s->solve(g, g.p, 10, 1e-6);
@@ -64,6 +72,8 @@ def test_integration_binding_compiles_and_links(tmp_path):
            "-I", os.path.join(REF_TREE, "include"), "-I", os.path.join(ROOT, "include"),
            str(src), os.path.join(REF_TREE, "src", "core", "grid.cpp"),
            os.path.join(REF_TREE, "src", "core", "grid_3d.cpp"),
+           os.path.join(REF_TREE, "src", "solver", "pcg_3d.cpp"),
+           os.path.join(REF_TREE, "src", "solver", "preconditioner", "uaamg_preconditioner_3d.cpp"),
            LIB, "-o", str(exe)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]

@@ -13,11 +13,16 @@
 //
 // Set-up: the first call on a device, with that device current, looks up the
 // array's device address (cudaGetSymbolAddress) once; make that first call before
-// any stream capture.  Every call on a device shares the one array and leaves its
+// any stream capture.  The address belongs to the device's current context: if the
+// application resets the device (cudaDeviceReset) or otherwise replaces its primary
+// context, the next call sees a new context id and looks the address up again
+// (again a set-up call: make it before any capture).  Every call on a device shares the one array and leaves its
 // contents behind; each call clears the counters it relies on before use.  Two
 // calls whose kernels overlap on the GPU (different streams, no ordering between
 // them) race on the array and give wrong results: order them on one stream.
 #include "../../include/uaamg.h"
+
+#include <cuda.h>
 
 #include <mutex>
 
@@ -37,6 +42,7 @@ constexpr int kScratchDoubles = kCounters + 2;
 
 constexpr int kMaxDevices = 64;
 double* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // context id the address belongs to
 std::mutex g_setup_mutex;
 
 }  // namespace
@@ -90,16 +96,49 @@ __global__ void k_na_residual(Geom g, const uint8_t* __restrict__ s, const doubl
     }
 }
 
-// Device address of the scratch array on the current device (looked up once).
+// Id of the current context (driver entry points looked up through the runtime);
+// 0 when it cannot be read.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(a);
+            get_id = reinterpret_cast<GetId>(b);
+        }
+        cudaGetLastError();
+        looked_up = true;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+        get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Device address of the scratch array on the current device, looked up once per
+// device and context.
 double* scratch_for(int dev) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_addr[dev] || ctx != g_scratch_ctx[dev]) {
         void* ptr = nullptr;
         if (cudaGetSymbolAddress(&ptr, g_uaamg_noalloc_scratch) != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
         g_scratch_addr[dev] = static_cast<double*>(ptr);
+        g_scratch_ctx[dev] = current_context_id();  // the lookup makes the context current
     }
     return g_scratch_addr[dev];
 }
