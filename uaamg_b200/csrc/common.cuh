@@ -85,6 +85,16 @@ struct CGState {
     unsigned int counter[8];  // last-block counters, one per reduction site
 };
 
+// Programmatic dependent launch: the engine launches its kernels so that each may
+// be scheduled while its predecessor on the stream is still finishing.  Every
+// kernel therefore first waits until the preceding grid has completed and its
+// memory operations are visible (a no-op when it was launched without the
+// attribute), and then lets its own successor be launched.
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Host-visible launch helpers ------------------------------------------------
 
 template <int DIM>

@@ -15,6 +15,7 @@
 // converted on the way in (rhs, warm-start p, preconditioner input) and out.
 #pragma once
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -74,12 +75,30 @@ struct KTag {
                    // launch that performs the replacement; most launches return at once)
 };
 
+// Kernel launch on the engine's stream.  Outside the per-kernel profiler every
+// launch carries the programmatic-stream-serialisation attribute (the kernels
+// begin with pdl_entry, common.cuh), so a kernel's launch and block scheduling
+// overlap the end of the one before it.
 #define UAAMG_LAUNCH_SMEM(tag, kern, grid, block, smem, ...)              \
     do {                                                                  \
         const KTag tg_ = (tag);                                           \
         cudaEvent_t e0_ = nullptr, e1_ = nullptr;                         \
         if (prof_on_) prof_begin(tg_, &e0_, &e1_);                        \
-        kern<<<(grid), (block), (smem), st_>>>(__VA_ARGS__);              \
+        if (pdl_ && !prof_on_) {                                          \
+            cudaLaunchConfig_t cf_ = {};                                  \
+            cudaLaunchAttribute at_[1];                                   \
+            at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization; \
+            at_[0].val.programmaticStreamSerializationAllowed = 1;        \
+            cf_.gridDim = dim3(grid);                                     \
+            cf_.blockDim = dim3(block);                                   \
+            cf_.dynamicSmemBytes = (smem);                                \
+            cf_.stream = st_;                                             \
+            cf_.attrs = at_;                                              \
+            cf_.numAttrs = 1;                                             \
+            cudaLaunchKernelEx(&cf_, kern, __VA_ARGS__);                  \
+        } else {                                                          \
+            kern<<<(grid), (block), (smem), st_>>>(__VA_ARGS__);          \
+        }                                                                 \
         if (prof_on_) cudaEventRecord(e1_, st_);                          \
         ++launches_;                                                      \
     } while (0)
@@ -93,7 +112,12 @@ class EngineT final : public Engine {
     static constexpr bool kHalf = !std::is_same<CS, T>::value;
 
 public:
-    explicit EngineT(bool mixed) : mixed_(mixed) {}
+    explicit EngineT(bool mixed) : mixed_(mixed) {
+        // UAAMG_NO_PDL=1 launches every kernel without the programmatic-dependent-launch
+        // attribute (fully serialised on the stream), for comparisons
+        const char* v = std::getenv("UAAMG_NO_PDL");
+        pdl_ = !(v && v[0] == '1');
+    }
     ~EngineT() override {
         release();
         if (cap_) cudaStreamDestroy(cap_);
@@ -343,6 +367,7 @@ private:
     bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
     bool flat2d_ = false;    // 2D finest level as flat walks (flat2d.cuh) instead of marches
     bool fused_ = true;      // two fused marches a level (fused.cuh) instead of four
+    bool pdl_ = true;        // programmatic dependent launch between the kernels
     int tail_lt_ = 0;        // first level of the small-level kernel
     int tail_nc_ = 0;        // 1: the hierarchy has a tail (0: it does not fit the kernel)
     size_t tail_smem_ = 0;   // its dynamic shared memory (x and b of every tail level)

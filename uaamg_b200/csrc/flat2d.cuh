@@ -392,6 +392,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_flat2d(MLevel<T> L, F2Op<T, CS> 
                                                     const uint8_t* __restrict__ code,
                                                     const T* __restrict__ b, T* __restrict__ x,
                                                     const int* __restrict__ done) {
+    pdl_entry();
     if (done && *done) return;
     const int nxc = (L.g.nx + 31) >> 5;
     const long long n = (long long)((L.g.ny + 1) >> 1) * nxc;
@@ -411,6 +412,7 @@ __global__ void __launch_bounds__(256) k_res_flat2d(MLevel<T> L, F2Op<T, CS> op,
                                                     const T* __restrict__ x,
                                                     const uint8_t* __restrict__ ccode,
                                                     T* __restrict__ cb, const int* __restrict__ done) {
+    pdl_entry();
     if (done && *done) return;
     const int ncx = (L.cg.nx + 31) >> 5;
     const long long n = (long long)L.cg.ny * ncx;
@@ -429,6 +431,7 @@ __global__ void __launch_bounds__(256, 2) k_upe_flat2d(MLevel<T> L, F2Op<T, CS> 
                                                     const T* __restrict__ b,
                                                     const T* __restrict__ xc, T* __restrict__ x,
                                                     const int* __restrict__ done) {
+    pdl_entry();
     if (done && *done) return;
     const int nxc = (L.g.nx + 31) >> 5;
     const long long n = (long long)((L.g.ny + 1) >> 1) * nxc;
@@ -448,6 +451,7 @@ __global__ void __launch_bounds__(256) k_upo_flat2d(MLevel<T> L, F2Op<T, CS> op,
                                                     const T* __restrict__ b, T* x,
                                                     const int* __restrict__ done, double* partials,
                                                     CGState* cg) {
+    pdl_entry();
     if (done && *done) return;
     double acc[3] = {0.0, 0.0, 0.0};
     const int nxc = (L.g.nx + 31) >> 5;

@@ -197,6 +197,7 @@ __global__ void __launch_bounds__(kThreads)
     k_level_fused(const __grid_constant__ FMaps M, MLevel<T> L, const uint8_t* __restrict__ ccode,
                   T* __restrict__ out, const int* __restrict__ done, int* err, double* partials,
                   CGState* cg) {
+    pdl_entry();
     if (done && *done) return;
     using C = FCfg<DIM, T, CS, FINE, UP>;
     using P = typename C::P;

@@ -103,6 +103,7 @@ __device__ __forceinline__ bool reduce_last(double (&v)[NV], double* partials,
 template <int DIM>
 __global__ void k_restrict_solid(Geom f, const uint8_t* __restrict__ fs, Geom c,
                                  uint8_t* __restrict__ cs) {
+    pdl_entry();
     int ic, jc, kc;
     if (!thread_cell<DIM>(c, ic, jc, kc)) return;
     const int i_f = 2 * ic - 1, j_f = 2 * jc - 1, k_f = DIM == 3 ? 2 * kc - 1 : 0;
@@ -123,6 +124,7 @@ __global__ void k_restrict_solid(Geom f, const uint8_t* __restrict__ fs, Geom c,
 template <int DIM, class T>
 __global__ void k_fine_coeffs(Geom g, const uint8_t* __restrict__ s, T* cx, T* cy, T* cz, T* wd,
                               T idx2, T idy2, T idz2) {
+    pdl_entry();
     int i, j, k;
     if (!thread_cell<DIM>(g, i, j, k)) return;
     const int id = cidx(g, i, j, k);
@@ -149,6 +151,7 @@ template <int DIM, class T>
 __global__ void k_galerkin(Geom f, const T* __restrict__ fcx, const T* __restrict__ fcy,
                            const T* __restrict__ fcz, const T* __restrict__ fwd, Geom c,
                            const uint8_t* __restrict__ cs, T* ccx, T* ccy, T* ccz, T* cwd) {
+    pdl_entry();
     int ic, jc, kc;
     if (!thread_cell<DIM>(c, ic, jc, kc)) return;
     const int id = cidx(c, ic, jc, kc);
@@ -204,6 +207,7 @@ __device__ __forceinline__ T diag_at(const LevelView<T>& L, int id) {
 // cells and diag < 1e-30.  One thread per x-pair of cells.
 template <int DIM, class T>
 __global__ void k_sweep(LevelView<T> L, int parity, const int* __restrict__ done) {
+    pdl_entry();
     if (done && *done) return;
     const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
@@ -228,6 +232,7 @@ __global__ void k_sweep(LevelView<T> L, int parity, const int* __restrict__ done
 template <int DIM, class T>
 __global__ void k_restrict(LevelView<T> F, Geom cg, const uint8_t* __restrict__ cs, T* cb,
                            const int* __restrict__ done) {
+    pdl_entry();
     if (done && *done) return;
     int ic, jc, kc;
     if (!thread_cell<DIM>(cg, ic, jc, kc)) return;
@@ -256,6 +261,7 @@ template <int DIM, class T>
 __global__ void k_prolong(Geom cg, const uint8_t* __restrict__ cs, const T* __restrict__ cx_,
                           Geom fg, const uint8_t* __restrict__ fs, T* fx,
                           const int* __restrict__ done) {
+    pdl_entry();
     if (done && *done) return;
     int ic, jc, kc;
     if (!thread_cell<DIM>(cg, ic, jc, kc)) return;
@@ -276,6 +282,7 @@ __global__ void k_prolong(Geom cg, const uint8_t* __restrict__ cs, const T* __re
 // block's global-memory writes visible to all its threads.
 template <int DIM, class T>
 __global__ void k_coarsest(LevelView<T> L, const int* __restrict__ done) {
+    pdl_entry();
     if (done && *done) return;
     const int nx = L.g.nx, ny = L.g.ny, nzi = DIM == 3 ? L.g.nz : 1;
     const int ncell = nx * ny * nzi;
@@ -375,6 +382,7 @@ __device__ __forceinline__ void for_cells(const Geom& g, F&& f) {
 // s = d + 2 ox + 2 oy (FP64), ox, oy of every interior cell as FP32 in the level's
 // layout, from the caller's padded arrays (reference layout, row stride st.vsx).
 __global__ void k_var_coeffs(Geom g, Stencil st, float* fs, float* fx, float* fy) {
+    pdl_entry();
     for_cells<2>(g, [&](int i, int j, int, int id) {
         const long long q = i + (long long)j * st.vsx;
         const double d = st.vd[q], ox = st.vox[q], oy = st.voy[q];
@@ -388,6 +396,7 @@ __global__ void k_var_coeffs(Geom g, Stencil st, float* fs, float* fx, float* fy
 template <int DIM>
 __global__ void k_sum_count(Geom g, const uint8_t* __restrict__ s, const double* __restrict__ v,
                             double* partials, CGState* cg, int slot) {
+    pdl_entry();
     double acc[2] = {0.0, 0.0};
     for_cells<DIM>(g, [&](int, int, int, int id) {
         if (!s[id]) { acc[0] += v[id]; acc[1] += 1.0; }
@@ -405,6 +414,7 @@ __global__ void k_sum_count(Geom g, const uint8_t* __restrict__ s, const double*
 template <int DIM>
 __global__ void k_rhs_negate(Geom g, const uint8_t* __restrict__ s, const double* rhs, double* b,
                              const CGState* cg) {
+    pdl_entry();
     double mean = cg->nfluid > 0.0 ? cg->sum0 / cg->nfluid : 0.0;
     if (cg->dirichlet) mean = 0.0;
     for_cells<DIM>(g, [&](int, int, int, int id) {
@@ -415,6 +425,7 @@ __global__ void k_rhs_negate(Geom g, const uint8_t* __restrict__ s, const double
 // v -= mean over fluid cells (pcg_3d.cpp:66-77), mean = sum0/nfluid.
 template <int DIM>
 __global__ void k_sub_mean(Geom g, const uint8_t* __restrict__ s, double* v, const CGState* cg) {
+    pdl_entry();
     if (cg->dirichlet) return;
     const double mean = cg->nfluid > 0.0 ? cg->sum0 / cg->nfluid : 0.0;
     for_cells<DIM>(g, [&](int, int, int, int id) {
@@ -466,6 +477,7 @@ template <int DIM, class T>
 __global__ void k_true_residual(Geom g, const uint8_t* __restrict__ s, const double* b,
                                 const double* __restrict__ x, T* rw, Stencil st, double* partials,
                                 CGState* cg, int slot, int mode, double tol, int tol_mode) {
+    pdl_entry();
     if (mode == 1 && !replacement_due(cg)) return;
     double acc[1] = {0.0};
     for_cells<DIM>(g, [&](int i, int j, int k, int id) {
@@ -510,6 +522,7 @@ __global__ void __launch_bounds__(256) k_resid_x64(Geom g, const uint8_t* __rest
                                                    const T* __restrict__ xlo, T* __restrict__ rw,
                                                    Stencil st, int zc, double* partials, CGState* cg,
                                                    int slot, int mode, double tol, int tol_mode) {
+    pdl_entry();
     if (mode == 1 && !replacement_due(cg)) return;
     double acc[1] = {0.0};
     const int tx = (g.nx + 31) / 32, ty = (g.ny + 7) / 8, tz = DIM == 3 ? (g.nz + zc - 1) / zc : 1;
@@ -587,6 +600,7 @@ __global__ void __launch_bounds__(256) k_pmatvec_2d(Geom g, const uint8_t* __res
                                                      const T* __restrict__ pold,
                                                      T* __restrict__ pnew, T* __restrict__ ap,
                                                      Stencil st, double* partials, CGState* cg) {
+    pdl_entry();
     if (cg->done) return;
     const T m = (T)cg->mean_z, beta = (T)cg->beta;
     const T idx2 = (T)st.idx2, idy2 = (T)st.idy2, diag = (T)st.diag;
@@ -684,6 +698,7 @@ __global__ void __launch_bounds__(256) k_pmatvec_2d(Geom g, const uint8_t* __res
 template <int DIM>
 __global__ void k_norm(Geom g, const uint8_t* __restrict__ s, const double* __restrict__ b,
                        double* partials, CGState* cg, int slot) {
+    pdl_entry();
     double acc[1] = {0.0};
     for_cells<DIM>(g, [&](int, int, int, int id) {
         if (!s[id]) acc[0] += b[id] * b[id];
@@ -713,6 +728,7 @@ __device__ __forceinline__ void finish_zdot(CGState* cg, const double (&tot)[3])
 template <int DIM, class T>
 __global__ void k_zdot(Geom g, const uint8_t* __restrict__ s, const T* __restrict__ r,
                        const T* __restrict__ z, double* partials, CGState* cg) {
+    pdl_entry();
     if (cg->done) return;
     double acc[3] = {0.0, 0.0, 0.0};
     for_cells<DIM>(g, [&](int, int, int, int id) {

@@ -449,6 +449,7 @@ template <int DIM, class T, bool FINE, class CS>
 __global__ void __launch_bounds__(kThreads) k_fwd_smooth(const __grid_constant__ MarchMaps M,
                                                          MLevel<T> L, T* __restrict__ x,
                                                          const int* __restrict__ done, int* err) {
+    pdl_entry();
     if (done && *done) return;
     using C = FwdCfg<DIM, T, FINE, CS>;
     using P = typename C::P;
@@ -550,6 +551,7 @@ __global__ void __launch_bounds__(kThreads) k_restrict_res(const __grid_constant
                                                            const uint8_t* __restrict__ ccode,
                                                            T* __restrict__ cb,
                                                            const int* __restrict__ done, int* err) {
+    pdl_entry();
     if (done && *done) return;
     using C = ResCfg<DIM, T, FINE, CS>;
     using P = typename C::P;
@@ -645,6 +647,7 @@ template <int DIM, class T, bool FINE, class CS>
 __global__ void __launch_bounds__(kThreads) k_up_even(const __grid_constant__ MarchMaps M,
                                                       MLevel<T> L, T* __restrict__ x,
                                                       const int* __restrict__ done, int* err) {
+    pdl_entry();
     if (done && *done) return;
     using C = UpeCfg<DIM, T, FINE, CS>;
     using P = typename C::P;
@@ -753,6 +756,7 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
                                                      MLevel<T> L, T* x,
                                                      const int* __restrict__ done, int* err,
                                                      double* partials, CGState* cg) {
+    pdl_entry();
     if (done && *done) return;
     using C = UpoCfg<DIM, T, FINE, CS>;
     using P = typename C::P;
@@ -836,6 +840,7 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
                                                       int zc, T* __restrict__ pnew,
                                                       T* __restrict__ ap, Stencil st,
                                                       double* partials, CGState* cg, int* err) {
+    pdl_entry();
     if (cg->done) return;
     using C = PmvCfg<DIM, T>;
     using P = typename C::P;

@@ -320,6 +320,7 @@ __device__ void tail_coarsest(const TailView<DIM, T>& V) {
 template <int DIM, class T>
 __global__ void __launch_bounds__(tail_threads<T>()) k_tail(const __grid_constant__ TailArgs<T> A,
                                                             const int* __restrict__ done) {
+    pdl_entry();
     if (done && *done) return;
     extern __shared__ __align__(16) unsigned char tail_smem[];
     T* sm = reinterpret_cast<T*>(tail_smem);

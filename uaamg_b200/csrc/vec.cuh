@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
                                                      const T* __restrict__ p,
                                                      const T* __restrict__ ap, double* xhi,
                                                      double* partials, CGState* cg, double* hist) {
+    pdl_entry();
     if (cg->done) return;
     using V = typename Vec16<T>::V;
     const T alpha = (T)cg->alpha;
@@ -136,10 +137,12 @@ __global__ void __launch_bounds__(256) k_update_flat(long long nvec, T* x, T* r,
 // Layout conversions between the reference's layout (gr) and the pitched one (g).
 template <int DIM, class T>
 __global__ void k_import(Geom g, Geom gr, const double* __restrict__ src, T* dst) {
+    pdl_entry();
     for_cells<DIM>(g, [&](int i, int j, int k, int id) { dst[id] = (T)src[cidx(gr, i, j, k)]; });
 }
 template <int DIM>
 __global__ void k_import_mask(Geom g, Geom gr, const uint8_t* __restrict__ src, uint8_t* dst) {
+    pdl_entry();
     for_cells<DIM>(g, [&](int i, int j, int k, int id) {
         dst[id] = src[cidx(gr, i, j, k)] ? 1 : 0;
     });
@@ -149,6 +152,7 @@ __global__ void k_import_mask(Geom g, Geom gr, const uint8_t* __restrict__ src, 
 template <int DIM, class T>
 __global__ void k_export_x(Geom g, Geom gr, const double* __restrict__ xhi, const T* __restrict__ xlo,
                            double* dst, int accumulate) {
+    pdl_entry();
     for_cells<DIM>(g, [&](int i, int j, int k, int id) {
         const double x = xhi && xlo ? xhi[id] + (double)xlo[id] : (xhi ? xhi[id] : (double)xlo[id]);
         const int rid = cidx(gr, i, j, k);
@@ -158,6 +162,7 @@ __global__ void k_export_x(Geom g, Geom gr, const double* __restrict__ xhi, cons
 // dst (reference layout) = src on interior cells (overwrite) or += src (accumulate).
 template <int DIM, class T>
 __global__ void k_export(Geom g, Geom gr, const T* __restrict__ src, double* dst, int accumulate) {
+    pdl_entry();
     for_cells<DIM>(g, [&](int i, int j, int k, int id) {
         const int rid = cidx(gr, i, j, k);
         dst[rid] = accumulate ? dst[rid] + (double)src[id] : (double)src[id];
@@ -170,6 +175,7 @@ __global__ void k_export(Geom g, Geom gr, const T* __restrict__ src, double* dst
 // exactly when the reference's coupling exists (uaamg_preconditioner_3d.cpp:50-66).
 template <int DIM>
 __global__ void k_codes(Geom g, const uint8_t* __restrict__ s, uint8_t* code, int fine) {
+    pdl_entry();
     for_cells<DIM>(g, [&](int i, int j, int k, int id) {
         uint32_t c = ((i + j + k) & 1) ? kOdd : 0u;
         if (!s[id]) {
@@ -195,6 +201,7 @@ template <int DIM, class T>
 __global__ void k_diag(Geom g, const uint8_t* __restrict__ s, const T* __restrict__ cx,
                        const T* __restrict__ cy, const T* __restrict__ cz,
                        const T* __restrict__ wd, T* dg) {
+    pdl_entry();
     for_cells<DIM>(g, [&](int, int, int, int id) {
         if (s[id]) return;
         T d = cx[id] + cx[id - 1] + cy[id] + cy[id - g.sx];
@@ -209,6 +216,7 @@ __global__ void k_diag(Geom g, const uint8_t* __restrict__ s, const T* __restric
 // coupling is replaced by its decoded value h * cs, so the diagonal (k_diag), the
 // step-by-step V-cycle and the marches all use the same values.
 __global__ void k_coupling_half(long long n, float* c, __half* h, float cs) {
+    pdl_entry();
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
         const __half v = __float2half_rn(rintf(c[t] / cs));
