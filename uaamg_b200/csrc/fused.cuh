@@ -507,6 +507,128 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// CG search direction fused with the operator, as a column march (3D): step s forms
+// p = (z - m) + beta p_old of plane s once per cell (tile and 1-cell ring) into a
+// shared plane and keeps each thread's own two columns in registers, then computes
+// A p of plane s-1 on the tile from the shared plane s-1 (in-plane neighbours) and
+// the registers (planes s and s-2), so each p is formed once and one block barrier
+// per plane suffices.  Same expressions and the same per-thread accumulation order
+// of p.Ap as k_pmatvec (march.cuh): a solid or out-of-domain neighbour reads p_C
+// (Neumann) or -p_C at a Dirichlet wall (pcg_3d.cpp:38-55); the last block sets
+// alpha = rz_old / p.Ap or stops on breakdown (pcg_3d.cpp:94-99).
+template <class T>
+struct PmcCfg {
+    using P = MPlan<3, T, true, false, false>;  // slots: z (b slot), p_old (x slot), codes
+    static constexpr int S = 4;
+    using Lay = MLayout<T, S, P>;
+    static constexpr size_t XB = align128(PBox<T>::BYTES);
+    static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * XB;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_pmatvec_col(const __grid_constant__ MarchMaps M, Geom g, int zc, T* __restrict__ pnew,
+                  T* __restrict__ ap, Stencil st, double* partials, CGState* cg, int* err) {
+    pdl_entry();
+    if (cg->done) return;
+    using C = PmcCfg<T>;
+    using P = typename C::P;
+    using Lay = typename C::Lay;
+    constexpr int S = C::S, W = PBox<T>::W, WC = PBox<uint8_t>::W;
+    UAAMG_FUSED_SMEM(sm, err)
+    const int tid = threadIdx.x;
+    const Pair o = own_pair<T>(g);
+    const T m = (T)cg->mean_z, beta = (T)cg->beta;
+    const T idx2 = (T)st.idx2, idy2 = (T)st.idy2, idz2 = (T)st.idz2, diag = (T)st.diag;
+    const bool dw = st.dirichlet != 0;
+    // ring cells of the 1-cell ring (box columns 0 and 33, rows 0 and 17): two per
+    // thread for the first 50 threads
+    const bool ring = tid < 50;
+    int ra0 = 0, rr0 = 0, ra1 = 0, rr1 = 0;
+    if (tid < 17) { ra0 = 2 * tid; ra1 = ra0 + 1; rr0 = rr1 = 0; }
+    else if (tid < 34) { ra0 = 2 * (tid - 17); ra1 = ra0 + 1; rr0 = rr1 = kMY + 1; }
+    else if (tid < 42) { ra0 = ra1 = 0; rr0 = 1 + 2 * (tid - 34); rr1 = rr0 + 1; }
+    else if (tid < 50) { ra0 = ra1 = kMX + 1; rr0 = 1 + 2 * (tid - 42); rr1 = rr0 + 1; }
+    const int rq0 = rr0 * W + ra0, rq1 = rr1 * W + ra1;
+    const int rc0 = rr0 * WC + ra0, rc1 = rr1 * WC + ra1;
+    int kb, ke;
+    zrange<3>(g, zc, kb, ke);
+    MRing<3, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING, kb - 1, ke};
+    bool ok = true;
+    if (tid == 0) {
+        R.start(M);
+        ok = R.wait(R.p0);
+    }
+    if (!step_barrier(ok, err)) return;
+    T* xb = reinterpret_cast<T*>(sm + Lay::OFF_EXTRA);
+    auto pv = [&](const unsigned char* stg, int q, int qc) -> T {
+        return (stg[P::OFF_CODE + qc] & kActive)
+                   ? (boxv<T>(stg, P::QB * P::VB, q) - m) + beta * boxv<T>(stg, P::QX * P::VB, q)
+                   : T(0);
+    };
+    double acc[1] = {0.0};
+    T pA1 = T(0), pB1 = T(0), pA2 = T(0), pB2 = T(0);  // own columns at planes s-1, s-2
+    uint32_t cA1 = 0, cB1 = 0;                          // their codes at plane s-1
+#pragma unroll 1
+    for (int s = R.p0; s <= ke; ++s) {
+        const unsigned char* stg = R.at(s);
+        T* xs = xb + (size_t)(s & 1) * (C::XB / sizeof(T));
+        const T* xo = xb + (size_t)((s + 1) & 1) * (C::XB / sizeof(T));
+        const uint32_t cA = stg[P::OFF_CODE + o.ca], cB = stg[P::OFF_CODE + o.ca + WC];
+        const T pA = pv(stg, o.qa, o.ca), pB = pv(stg, o.qa + W, o.ca + WC);
+        xs[o.qa] = pA;
+        xs[o.qa + W] = pB;
+        if (ring) {
+            xs[rq0] = pv(stg, rq0, rc0);
+            xs[rq1] = pv(stg, rq1, rc1);
+        }
+        if (s >= kb + 1) {  // A p of plane k = s - 1
+            const int k = s - 1;
+            const uint32_t cc[2] = {cA1, cB1};
+            const T p0s[2] = {pA1, pB1}, pup[2] = {pA, pB}, pdn[2] = {pA2, pB2};
+            T a_[2] = {T(0), T(0)};
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const uint32_t c = cc[e];
+                if (c & kActive) {
+                    const int q = o.qa + e * W, i = o.i, j = o.j + e;
+                    const T p0 = p0s[e];
+                    const T wall = dw ? -p0 : p0;
+                    const T vL = (c & 2u) ? xo[q - 1] : (i > 1 ? p0 : wall);
+                    const T vR = (c & 1u) ? xo[q + 1] : (i < g.nx ? p0 : wall);
+                    const T vB = (c & 8u) ? xo[q - W] : (j > 1 ? p0 : wall);
+                    const T vT = (c & 4u) ? xo[q + W] : (j < g.ny ? p0 : wall);
+                    const T vF = (c & 32u) ? pdn[e] : (k > 1 ? p0 : wall);
+                    const T vK = (c & 16u) ? pup[e] : (k < g.nz ? p0 : wall);
+                    a_[e] = sizeof(T) == 8
+                                ? diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2
+                                : ((p0 - vL) + (p0 - vR)) * idx2 + ((p0 - vB) + (p0 - vT)) * idy2 +
+                                      ((p0 - vF) + (p0 - vK)) * idz2;
+                    acc[0] += (double)p0 * (double)a_[e];
+                }
+            }
+            const int id = o.gid + k * g.sxy;
+            if (o.ina) { pnew[id] = pA1; ap[id] = a_[0]; }
+            if (o.inb) { pnew[id + g.sx] = pB1; ap[id + g.sx] = a_[1]; }
+        }
+        pA2 = pA1; pB2 = pB1;
+        pA1 = pA; pB1 = pB;
+        cA1 = cA; cB1 = cB;
+        bool okk = true;
+        if (tid == 0 && s + 1 <= R.plast) okk = R.wait(s + 1);
+        if (!step_barrier(okk, err)) return;
+        if (tid == 0) R.refill(M, s);
+    }
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
+        const double pap = tot[0];
+        cg->pap = pap;
+        if (!(pap == pap)) { cg->status = CG_NAN; cg->done = 1; }
+        else if (pap < cg->breakdown) { cg->status = CG_BREAKDOWN; cg->done = 1; }
+        else cg->alpha = cg->rz_old / pap;
+    }
+}
+
 #undef UAAMG_FUSED_SMEM
 
 }  // namespace
