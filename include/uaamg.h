@@ -151,6 +151,15 @@ UAAMG_API uaamg_status uaamg_set_dirichlet_walls(uaamg_handle* h, int on);
  * All give identical results in FP64; 1, 2, 4 and 5 exist to cross-check 0. */
 UAAMG_API uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps);
 
+/* Smoothing schedule of this handle's V-cycle: pre- and post-smoothing sweeps (1 to 4)
+ * on the finest level and on the coarse levels, i.e. V(nu, nu) cycles; 1, 1 (default)
+ * is the reference's V(1,1) (UAAMGPreconditioner3D::vCycle, uaamg_preconditioner_3d.cpp:
+ * 183-196; its CUDA path fixes NU = 1, cuda_uaamg_preconditioner_3d_opt_f.cu:444).  More
+ * sweeps make a different (still symmetric) preconditioner; the batch autotuner
+ * (uaamg_set_autotune) may choose them per problem class.  Takes effect at the next
+ * solve. */
+UAAMG_API uaamg_status uaamg_set_smoothing(uaamg_handle* h, int sweeps_fine, int sweeps_coarse);
+
 /* Solve lap(p) = rhs with HOST FP64 arrays (padded): the Solver::solve /
  * Solver3D::solve drop-in (include/solver/solver.h:18-34, solver_3d.h:7-12;
  * CudaPCGSolver::solve, cuda_pcg_solver.cu:21-63).  Host<->device copies are
@@ -287,6 +296,14 @@ UAAMG_API uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_pro
  * results are cached per level shape for the process.  0 (default): fixed rule.
  * No reference counterpart (the reference's kernels have fixed shapes). */
 UAAMG_API uaamg_status uaamg_set_autotune(uaamg_handle* h, int on);
+
+/* Process-wide file (JSON) that keeps the autotuner's choices -- z-chunk lengths per
+ * level shape, and for batches the smoothing schedule per problem class (GPU,
+ * precision, shape, solid fraction to 0.05) -- so later processes reuse them; NULL:
+ * memory only (the default).  An existing file is read at once and rewritten as
+ * choices are added.  No counterpart in the reference, whose CUDA kernels fix tile
+ * shapes and smoothing at compile time. */
+UAAMG_API uaamg_status uaamg_set_tune_cache(const char* path);
 
 /* ---- Serving (uaamg_server_{start,submit,poll,stop}) --------------------------
  * A device-resident request loop on one GPU.  Requests carry a simulation id; the

@@ -139,3 +139,61 @@ def test_autotuned_chunks_give_identical_results(prec):
         hd.close()
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp32", "fp64"])
+def test_smoothing_schedules_converge(prec):
+    """V(nu, nu) cycles (uaamg_set_smoothing): more sweeps on the coarse levels, or on
+    every level, still give a symmetric preconditioner -- PCG reaches the same
+    tolerance (the mixed form's FP64 true residual 1e-6; FP64 and plain FP32 their
+    recursive one) -- and needs no more iterations than the reference's V(1,1) (to
+    within two)."""
+    probs = _problems()[1:4]
+    hd = Handle(0)
+    for s, r, dx, dy, dz in probs:
+        hd.set_problem(s, dx, dy, dz)
+        its = {}
+        for nu in [(1, 1), (1, 2), (2, 2)]:
+            hd.set_smoothing(*nu)
+            p = np.zeros_like(r)
+            st = hd.solve(r, p, hd.options(prec, 1e-6, 400, "rel"))
+            assert st.status == 0, (prec, nu, st.status)
+            if prec == "mixed":
+                res, bn = O.true_residual(s, r, p, dx, dy, dz)
+                assert res / bn <= 1e-6, (nu, res / bn)
+            its[nu] = st.iterations
+        hd.set_smoothing(1, 1)
+        assert its[(2, 2)] <= its[(1, 1)] + 2 and its[(1, 2)] <= its[(1, 1)] + 2, its
+    hd.close()
+
+
+def test_batch_autotune_schedules_and_cache_file(tmp_path):
+    """With the autotuner on, a mixed batch picks a smoothing schedule and z-chunk
+    lengths per problem class, stores them in the cache file, and a second batch call
+    reuses them (identical results); every result meets the true residual 1e-6."""
+    import json
+    from uaamg_b200.solver import set_tune_cache
+    path = tmp_path / "tune.json"
+    set_tune_cache(str(path))
+    try:
+        probs = _problems()[:4]
+        hd = Handle(0)
+        hd.set_autotune(True)
+        opts = hd.options("mixed", 1e-6, 400, "rel")
+        runs = []
+        for rep in range(2):
+            ps = [np.zeros_like(r) for _, r, *_ in probs]
+            hd.solve_batch([(s, r, p, dx, dy, dz) for (s, r, dx, dy, dz), p in zip(probs, ps)], opts)
+            runs.append(ps)
+            for (s, r, dx, dy, dz), p in zip(probs, ps):
+                res, bn = O.true_residual(s, r, p, dx, dy, dz)
+                assert res / bn <= 1e-6
+        for a, b in zip(*runs):
+            assert np.array_equal(a, b)
+        entries = json.load(open(path))["entries"]
+        assert sum(k.startswith("nu|") for k in entries) == len(probs)
+        assert any(k.startswith("zc|") for k in entries)
+        assert all(v in ([1, 1], [1, 2], [2, 2]) for k, v in entries.items() if k.startswith("nu|"))
+        hd.close()
+    finally:
+        set_tune_cache(None)

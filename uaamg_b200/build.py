@@ -30,6 +30,7 @@ UNITS = [
     ("api.cpp", ["-x", "cu"]),
     ("runtime.cpp", ["-x", "cu"]),
     ("noalloc.cu", ["-fmad=false"]),
+    ("tunecache.cpp", ["-x", "cu"]),
     ("project.cu", ["-fmad=false"]),
 ]
 HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "fused.cuh", "flat2d.cuh", "tail.cuh", "vec.cuh", "tma.cuh",

@@ -100,6 +100,7 @@ uaamg_status engine_for(uaamg_handle* h, int p, uaamg::Engine** out) {
     }
     h->eng[p]->set_stream(h->stream);
     uaamg::api::apply_vcycle_mode(h->eng[p], h->sweeps);
+    h->eng[p]->set_smoothing(h->nu_fine, h->nu_coarse);
     h->eng[p]->set_autotune(h->autotune != 0);
     if (h->lap_on)
         h->eng[p]->set_operator(h->d_lap[0], h->d_lap[1], h->d_lap[2], h->nx + 2, h->lap_version);
@@ -252,6 +253,15 @@ uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps) {
     if (!h) return UAAMG_INVALID_ARG;
     if (sweeps < 0 || sweeps > 5) return fail(h, UAAMG_INVALID_ARG, "V-cycle kernels: 0 to 5");
     h->sweeps = sweeps;
+    return UAAMG_OK;
+}
+
+uaamg_status uaamg_set_smoothing(uaamg_handle* h, int sweeps_fine, int sweeps_coarse) {
+    if (!h) return UAAMG_INVALID_ARG;
+    if (sweeps_fine < 1 || sweeps_fine > 4 || sweeps_coarse < 1 || sweeps_coarse > 4)
+        return fail(h, UAAMG_INVALID_ARG, "smoothing sweeps: 1 to 4");
+    h->nu_fine = sweeps_fine;
+    h->nu_coarse = sweeps_coarse;
     return UAAMG_OK;
 }
 

@@ -261,6 +261,12 @@ public:
     void set_graphs(bool on) override { graphs_ = on; }
     void set_autotune(bool on) override { autotune_ = on; }
     void set_small_levels(bool on) override { tail_on_ = on; }
+    void set_smoothing(int fine, int coarse) override {
+        if (fine == nu_fine_ && coarse == nu_coarse_) return;
+        drop_graph();
+        nu_fine_ = fine;
+        nu_coarse_ = coarse;
+    }
     void set_flat2d(bool on) override {
         if (on == flat2d_) return;
         drop_graph();  // a captured step holds the other kernels
@@ -368,6 +374,7 @@ private:
     bool flat2d_ = false;    // 2D finest level as flat walks (flat2d.cuh) instead of marches
     bool fused_ = true;      // two fused marches a level (fused.cuh) instead of four
     bool pdl_ = true;        // programmatic dependent launch between the kernels
+    int nu_fine_ = 1, nu_coarse_ = 1;  // pre- and post-smoothing sweeps: finest / coarse levels
     int tail_lt_ = 0;        // first level of the small-level kernel
     int tail_nc_ = 0;        // 1: the hierarchy has a tail (0: it does not fit the kernel)
     size_t tail_smem_ = 0;   // its dynamic shared memory (x and b of every tail level)
@@ -773,15 +780,14 @@ private:
                           tail_smem_, a, done);
     }
 
-    // Autotuner: for every level with marches, time its four V-cycle marches
-    // (down and up, on the level's own buffers) for each z-chunk length in
-    // {2, 4, 8, 16, 32} and keep the fastest; the choice is cached per level shape
-    // and precision for the process.  Chunk length changes only the blocks' shape,
-    // not the arithmetic, so the results do not depend on it.
+    // Autotuner: for every level with marches, time its V-cycle marches (down and up,
+    // on the level's own buffers) for each z-chunk length in {2, 4, 8, 16, 32} and
+    // keep the fastest; the choice is cached per GPU, precision, level shape and
+    // march kind (tune_lookup / tune_store: for the process, and in the cache file
+    // when one is set).  Chunk length changes only the blocks' shape, not the
+    // arithmetic, so the results do not depend on it.
     template <int DIM>
     int tune() {
-        static std::mutex mu;
-        static std::map<std::tuple<int, int, int, int, int, int, int>, int> cache;
         cudaEvent_t a = nullptr, b = nullptr;
         if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return E_CUDA;
         const bool prof = prof_on_;
@@ -790,12 +796,13 @@ private:
         for (int l = 0; l + 1 < (int)lv_.size() && e == E_OK; ++l) {
             if (use_tail() && l >= tail_lt_) break;  // the small-level kernel runs those levels
             LevelBuf<T, CS>& L = lv_[l];
-            const auto key = std::make_tuple((int)sizeof(T), mixed_ ? 1 : 0, L.g.nx, L.g.ny, L.g.nz,
-                                             l == 0 ? 1 : 0, fused_ ? 1 : 0);
+            const std::string key = "zc|" + tune_gpu_id() + "|" + (sizeof(T) == 8 ? "f64" : mixed_ ? "mixed" : "f32") +
+                                    "|" + std::to_string(L.g.nx) + "x" + std::to_string(L.g.ny) + "x" +
+                                    std::to_string(L.g.nz) + "|" + (l == 0 ? "fine" : "coarse") + "|" +
+                                    (fused_ && level_nu(l) == 1 ? "fused" : "four") + (L.c32 ? "|c32" : "");
             {
-                std::lock_guard<std::mutex> lk(mu);
-                auto it = cache.find(key);
-                if (it != cache.end()) { L.zc = it->second; continue; }
+                std::vector<int> v;
+                if (tune_lookup(key, &v) && v.size() == 1 && v[0] >= 2 && v[0] <= 32) { L.zc = v[0]; continue; }
             }
             int best = L.zc;
             float best_ms = 1e30f;
@@ -817,8 +824,7 @@ private:
                 if (ms < best_ms) { best_ms = ms; best = zc; }
             }
             L.zc = best;
-            std::lock_guard<std::mutex> lk(mu);
-            cache[key] = best;
+            tune_store(key, {best});
         }
         prof_on_ = prof;
         cudaEventDestroy(a);
@@ -979,14 +985,17 @@ private:
         down_level_cs<DIM, FINE, CS>(l, done);
     }
 
+    int level_nu(int l) const { return l == 0 ? nu_fine_ : nu_coarse_; }
+
     template <int DIM, bool FINE, class CSL>
     void down_level_cs(int l, const int* done) {
+        const int nu = level_nu(l);
         const LevelBuf<T, CS>& L = lv_[l];
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
         if constexpr (std::is_same<CSL, CS>::value) {
-            if (DIM == 2 && flat2d_) {
+            if (DIM == 2 && flat2d_ && nu == 1) {
                 // b, code (coarse levels: couplings, diagonal) in; x out / b, x, code in;
                 // coarse b out
                 const F2Op<T, CS> op = flat_op(l);
@@ -1002,7 +1011,7 @@ private:
             }
         }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
-        if (fused_) {
+        if (fused_ && nu == 1) {
             // b, code (coarse levels: diagonal, couplings) in; coarse code in, coarse b out
             UAAMG_LAUNCH_SMEM((KTag{K_DOWN, l, c * (t + 1.0 + coef) + cc * (t + 1.0)}),
                               (k_level_fused<DIM, T, FINE, CSL, false, false>), grid, blk,
@@ -1014,6 +1023,11 @@ private:
         UAAMG_LAUNCH_SMEM((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_smooth<DIM, T, FINE, CSL>),
                           grid, blk, (FwdCfg<DIM, T, FINE, CSL>::BYTES), maps<DIM>(l, false, false),
                           mlevel(l), x, done, err_);
+        for (int q = 1; q < nu; ++q) {  // further forward sweeps (colour 1, then 0) on the stored x
+            const LevelView<T> v = view(l, r_, z_);
+            sweep<DIM>(v, 1, done, l);
+            sweep<DIM>(v, 0, done, l);
+        }
         UAAMG_LAUNCH_SMEM((KTag{K_RES, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
                           (k_restrict_res<DIM, T, FINE, CSL>), grid, blk, (ResCfg<DIM, T, FINE, CSL>::BYTES),
                           maps<DIM>(l, true, false), mlevel(l), Cl.code, Cl.b, done, err_);
@@ -1031,12 +1045,13 @@ private:
 
     template <int DIM, bool FINE, class CSL>
     void up_level_cs(int l, const int* done, bool zdot) {
+        const int nu = level_nu(l);
         const LevelBuf<T, CS>& L = lv_[l];
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
         if constexpr (std::is_same<CSL, CS>::value) {
-            if (DIM == 2 && flat2d_) {
+            if (DIM == 2 && flat2d_ && nu == 1) {
                 const dim3 fg = flat_grid((L.g.ny + 1) / 2, L.g.nx), fb(32, 8);
                 const F2Op<T, CS> op = flat_op(l);
                 T* b = l == 0 ? r_ : L.b;
@@ -1057,7 +1072,7 @@ private:
         }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
-        if (fused_) {
+        if (fused_ && nu == 1) {
             // b, code (coarse levels: diagonal, couplings), coarse x in; x out
             const KTag tag{K_UP, l, c * (2.0 * t + 1.0 + coef) + cc * t};
             if (FINE && zdot)
@@ -1073,6 +1088,20 @@ private:
         UAAMG_LAUNCH_SMEM((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
                           (k_up_even<DIM, T, FINE, CSL>), grid, blk, (UpeCfg<DIM, T, FINE, CSL>::BYTES),
                           maps<DIM>(l, false, true), mlevel(l), x, done, err_);
+        if (nu > 1) {  // first reverse sweep, further reverse sweeps (colour 0, then 1), z sums
+            UAAMG_LAUNCH_SMEM((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
+                              (k_up_odd<DIM, T, FINE, false, CSL>), grid, blk, (UpoCfg<DIM, T, FINE, CSL>::BYTES),
+                              maps<DIM>(l, true, false), mlevel(l), x, done, err_, partials_, cg_);
+            const LevelView<T> v = view(l, r_, z_);
+            for (int q = 1; q < nu; ++q) {
+                sweep<DIM>(v, 0, done, l);
+                sweep<DIM>(v, 1, done, l);
+            }
+            if (FINE && zdot)
+                UAAMG_LAUNCH((KTag{K_ZDOT, 0, c * (2.0 * t + 1.0)}), (k_zdot<DIM, T>), vec_grid(L.g),
+                             dim3(32, 8), L.g, L.solid, r_, z_, partials_, cg_);
+            return;
+        }
         if (zdot)
             UAAMG_LAUNCH_SMEM((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
                               (k_up_odd<DIM, T, FINE, true, CSL>), grid, blk, (UpoCfg<DIM, T, FINE, CSL>::BYTES),

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <string>
 #include <vector>
 
 namespace uaamg {
@@ -100,6 +101,10 @@ public:
     // and restriction; up = prolongation and reverse sweep) instead of four
     // (march.cuh).  Default on.
     virtual void set_fused(bool on) = 0;
+    // Pre- and post-smoothing sweeps on the finest level and on the coarse levels
+    // (V(nu, nu) cycles; the reference's V(1,1) is 1, 1, the default).  More than one
+    // sweep runs the four-march level with the extra sweeps as colour-sweep kernels.
+    virtual void set_smoothing(int fine, int coarse) = 0;
     // 2D variable-coefficient outer-CG operator (the lap_diag / lap_off_x / lap_off_y
     // branch of PCG::solve, pcg.cpp:35-46): device arrays in the caller's padded
     // layout with row stride sx, read in place by every solve until changed;
@@ -118,6 +123,13 @@ public:
     // Non-zero if a kernel of the last call gave up waiting for its TMA loads.
     virtual int timed_out() = 0;
 };
+
+// The autotuner's persistent choices (tunecache.cpp): an id of the current GPU, and
+// lookup / store of integer lists by key (in memory; also in the JSON file set by
+// uaamg_set_tune_cache).
+std::string tune_gpu_id();
+bool tune_lookup(const std::string& key, std::vector<int>* val);
+void tune_store(const std::string& key, const std::vector<int>& val);
 
 Engine* create_engine_f64();
 Engine* create_engine_f32(int mixed);

@@ -33,6 +33,7 @@ struct uaamg_handle {
                      // 3 as 0 with 2D march levels as flat walks, 4 four marches a level
                      // + small-level kernel, 5 four marches on every level
     int autotune = 0;
+    int nu_fine = 1, nu_coarse = 1;  // smoothing sweeps (uaamg_set_smoothing)
     std::string err;
     struct BatchPool* batch = nullptr;  // runtime.cpp: per-problem slots of uaamg_solve_batch
 };

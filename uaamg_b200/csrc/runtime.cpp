@@ -21,6 +21,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "common.cuh"
 #include "engine.h"
 #include "handle.h"
 
@@ -133,6 +134,51 @@ struct DevProblem {
     }
 };
 
+// Smoothing schedule of a batch problem chosen by the autotuner: the fastest of
+// V(1,1) (the reference's), V(1,1) on the finest level with V(2,2) below, and
+// V(2,2), timed as a full solve of the problem itself (the second of two, after the
+// graph capture), among those that converge; cached per GPU, precision, shape and
+// solid fraction (to 0.05).  The problem's right-hand side must be on the device.
+std::vector<int> tune_schedule(DevProblem& d, const uaamg_problem& p, const uaamg_options& o) {
+    size_t solid = 0, inner = 0;
+    for (int k = (p.dim == 3 ? 1 : 0); k <= (p.dim == 3 ? p.nz : 0); ++k)
+        for (int j = 1; j <= p.ny; ++j)
+            for (int i = 1; i <= p.nx; ++i) {
+                solid += p.solid[i + (size_t)(p.nx + 2) * (j + (size_t)(p.ny + 2) * k)] != 0;
+                ++inner;
+            }
+    const int bucket = (int)(20.0 * (double)solid / (double)(inner ? inner : 1) + 0.5);
+    const std::string key = "nu|" + tune_gpu_id() + "|" +
+                            (o.precision == PREC_MIXED ? "mixed" : "f32") + "|" + std::to_string(p.dim) +
+                            "|" + std::to_string(p.nx) + "x" + std::to_string(p.ny) + "x" +
+                            std::to_string(p.dim == 3 ? p.nz : 0) + "|s" + std::to_string(bucket);
+    std::vector<int> best;
+    if (tune_lookup(key, &best) && best.size() == 2) return best;
+    const int cand[3][2] = {{1, 1}, {1, 2}, {2, 2}};
+    double best_ms = 1e300;
+    best = {1, 1};
+    for (const auto& c : cand) {
+        d.eng->set_smoothing(c[0], c[1]);
+        double ms = 0.0;
+        bool ok = true;
+        for (int rep = 0; rep < 2 && ok; ++rep) {
+            cudaMemsetAsync(d.d_p, 0, d.n * sizeof(double), d.stream);
+            cudaStreamSynchronize(d.stream);
+            const auto t0 = Clock::now();
+            SolveResult r;
+            std::memset(&r, 0, sizeof(r));
+            ok = d.eng->solve(d.args(o), &r) == E_OK && r.status == CG_CONVERGED;
+            ms = ms_since(t0);
+        }
+        if (ok && ms < best_ms) {
+            best_ms = ms;
+            best = {c[0], c[1]};
+        }
+    }
+    tune_store(key, best);
+    return best;
+}
+
 }  // namespace
 }  // namespace uaamg
 
@@ -198,8 +244,14 @@ uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_problem* prob
             d.release();
             return s;
         }
-        // as uaamg_solve: the result is accumulated into the caller's p
         cudaMemcpyAsync(d.d_rhs, p.rhs, d.n * 8, cudaMemcpyHostToDevice, d.stream);
+        if (h->autotune && opts.precision != PREC_FP64) {
+            const std::vector<int> nu = tune_schedule(d, p, opts);
+            d.eng->set_smoothing(nu[0], nu[1]);
+        } else {
+            d.eng->set_smoothing(h->nu_fine, h->nu_coarse);
+        }
+        // as uaamg_solve: the result is accumulated into the caller's p
         cudaMemcpyAsync(d.d_p, p.p, d.n * 8, cudaMemcpyHostToDevice, d.stream);
         if ((e = d.eng->solve_begin(d.args(opts))) != E_OK)
             return api::map_engine(h, e, "batch: solve", d.eng);

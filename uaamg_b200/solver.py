@@ -95,6 +95,15 @@ class Grid3D:
 # Handle
 
 
+def set_tune_cache(path=None):
+    """Process-wide JSON file that keeps the autotuner's choices (uaamg_set_tune_cache);
+    None: memory only."""
+    lib = _capi.load()
+    st = lib.uaamg_set_tune_cache(None if path is None else str(path).encode())
+    if st != _capi.OK:
+        raise _capi.UaamgError(st, "set_tune_cache")
+
+
 class Handle:
     """Owns one ``uaamg_handle`` (one GPU, one problem at a time)."""
 
@@ -135,6 +144,12 @@ class Handle:
         4: four z marches a level + the small-level kernel; 5: four marches on every
         level."""
         self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(mode)), "vcycle")
+
+    def set_smoothing(self, sweeps_fine=1, sweeps_coarse=1):
+        """Pre- and post-smoothing sweeps on the finest and the coarse levels
+        (uaamg_set_smoothing; 1, 1 is the reference's V(1,1))."""
+        self._check(self.lib.uaamg_set_smoothing(self.h, int(sweeps_fine), int(sweeps_coarse)),
+                    "smoothing")
 
     def set_variable_laplacian(self, lap_diag=None, lap_off_x=None, lap_off_y=None):
         """The outer CG's variable-coefficient operator for the current 2D problem
