@@ -305,6 +305,13 @@ UAAMG_API uaamg_status uaamg_set_autotune(uaamg_handle* h, int on);
  * shapes and smoothing at compile time. */
 UAAMG_API uaamg_status uaamg_set_tune_cache(const char* path);
 
+/* uaamg_solve_batch: the problems of at most max_cells padded cells share ONE CUDA
+ * graph per step (two PCG iterations of each, on their own streams, forked and
+ * joined inside the graph) instead of one graph each; 0 (default): every problem
+ * runs its own graph.  Results are the same either way.  No counterpart in the
+ * reference. */
+UAAMG_API uaamg_status uaamg_set_batch_group(uaamg_handle* h, long long max_cells);
+
 /* ---- Serving (uaamg_server_{start,submit,poll,stop}) --------------------------
  * A device-resident request loop on one GPU.  Requests carry a simulation id; the
  * server keeps each id's hierarchy and FP64 pressure on the device and

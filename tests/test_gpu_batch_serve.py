@@ -197,3 +197,25 @@ def test_batch_autotune_schedules_and_cache_file(tmp_path):
         hd.close()
     finally:
         set_tune_cache(None)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_batch_group_graph_matches_per_problem_graphs(prec):
+    """uaamg_set_batch_group: the small problems of a batch replayed as one CUDA graph
+    per step give the same results, bit for bit, as one graph per problem (the same
+    kernels in the same order on each problem's stream)."""
+    probs = _problems()
+    hd = Handle(0)
+    opts = hd.options(prec, 1e-6, 400, "rel")
+    out = {}
+    for group in (0, 40000):
+        hd.set_batch_group(group)
+        ps = [np.zeros_like(r) for _, r, *_ in probs]
+        stats = hd.solve_batch([(s, r, p, dx, dy, dz) for (s, r, dx, dy, dz), p in zip(probs, ps)],
+                               opts)
+        out[group] = (ps, [st.iterations for st in stats])
+    hd.set_batch_group(0)
+    assert out[0][1] == out[40000][1]
+    for a, b in zip(out[0][0], out[40000][0]):
+        assert np.array_equal(a, b)
+    hd.close()

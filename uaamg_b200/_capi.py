@@ -38,6 +38,7 @@ EXPORTS = [
     "uaamg_server_submit", "uaamg_server_poll", "uaamg_server_drain", "uaamg_server_info",
     "uaamg_server_stop", "uaamg_project", "uaamg_project_device", "uaamg_static_pressure",
     "uaamg_static_pressure_device", "uaamg_set_smoothing", "uaamg_set_tune_cache",
+    "uaamg_set_batch_group",
 ]
 
 
@@ -152,6 +153,7 @@ def load(path: str | None = None):
     L.uaamg_set_vcycle_kernels.argtypes = [p, i]
     L.uaamg_set_smoothing.argtypes = [p, i, i]
     L.uaamg_set_tune_cache.argtypes = [C.c_char_p]
+    L.uaamg_set_batch_group.argtypes = [p, C.c_longlong]
     L.uaamg_residual_noalloc.argtypes = [i, i, i, i, d, d, d, p, p, p, p, p]
     L.uaamg_solve.argtypes = [p, p, p, C.POINTER(Options), C.POINTER(Stats)]
     L.uaamg_solve_device.argtypes = [p, p, p, C.POINTER(Options), C.POINTER(Stats)]

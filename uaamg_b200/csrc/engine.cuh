@@ -184,6 +184,22 @@ public:
 
     int solve_end_enqueue() override { return dim_ == 3 ? end_enqueue<3>() : end_enqueue<2>(); }
 
+    int enqueue_step(cudaStream_t s, int* flag_dst) override {
+        if (lv_.empty()) return E_NOPROB;
+        const cudaStream_t saved = st_;
+        st_ = s;
+        if (dim_ == 3) {
+            cg_iteration<3>(true);
+            cg_iteration<3>(false);
+        } else {
+            cg_iteration<2>(true);
+            cg_iteration<2>(false);
+        }
+        if (flag_dst) cudaMemcpyAsync(flag_dst, &cg_->done, sizeof(int), cudaMemcpyDeviceToHost, st_);
+        st_ = saved;
+        return E_OK;
+    }
+
     int solve_end_collect(SolveResult* res) override {
         int e = sync_check();
         if (e != E_OK) return e;

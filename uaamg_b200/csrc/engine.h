@@ -80,6 +80,11 @@ public:
     // stream; collect reads the result once that work has completed (e.g. after an
     // event recorded behind it reports done), and then does not wait.
     virtual int solve_end_enqueue() = 0;
+    // After solve_begin: queue one step (two PCG iterations) on stream s, without a
+    // graph, then copy the device 'done' flag into flag_dst (pinned host memory).
+    // For capturing the steps of many engines into one CUDA graph (batches); the
+    // engine's own step bookkeeping (solve_step / solve_poll) is not used then.
+    virtual int enqueue_step(cudaStream_t s, int* flag_dst) = 0;
     virtual int solve_end_collect(SolveResult* res) = 0;
     virtual int nlevels() const = 0;
     virtual void level_dims(int l, int* nx, int* ny, int* nz) const = 0;

@@ -34,6 +34,8 @@ struct uaamg_handle {
                      // + small-level kernel, 5 four marches on every level
     int autotune = 0;
     int nu_fine = 1, nu_coarse = 1;  // smoothing sweeps (uaamg_set_smoothing)
+    long long batch_group_cells = 0; // batch problems of at most this many padded cells
+                                     // share one CUDA graph per step (0: none)
     std::string err;
     struct BatchPool* batch = nullptr;  // runtime.cpp: per-problem slots of uaamg_solve_batch
 };

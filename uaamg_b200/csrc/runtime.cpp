@@ -179,6 +179,111 @@ std::vector<int> tune_schedule(DevProblem& d, const uaamg_problem& p, const uaam
     return best;
 }
 
+// The small problems of a batch replayed as ONE CUDA graph per step
+// (uaamg_set_batch_group): the graph forks to every member's stream, queues its two
+// PCG iterations and the copy of its 'done' flag, and joins; two such graphs (one
+// per flag buffer) keep two steps in flight.  Finished members' kernels return at
+// once, so the graph keeps issuing them until every member has stopped.
+struct GroupGraph {
+    std::vector<int> members;
+    cudaStream_t master = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins;
+    int* flags = nullptr;  // pinned, 2 x members
+    int launched = 0, seen = 0, max_steps = 0;
+    bool done = false;
+
+    void release() {
+        if (master) cudaStreamSynchronize(master);
+        for (auto& x : exec) if (x) { cudaGraphExecDestroy(x); x = nullptr; }
+        for (auto& e : ev) if (e) { cudaEventDestroy(e); e = nullptr; }
+        if (fork) { cudaEventDestroy(fork); fork = nullptr; }
+        for (auto& e : joins) if (e) cudaEventDestroy(e);
+        joins.clear();
+        if (flags) { cudaFreeHost(flags); flags = nullptr; }
+        if (master) { cudaStreamDestroy(master); master = nullptr; }
+        members.clear();
+    }
+
+    // After every member's solve_begin.  Returns false if the graph could not be
+    // made (the members then run on their own graphs).
+    bool build(std::vector<DevProblem>& slots, const std::vector<int>& m, int max_iter) {
+        members = m;
+        const int G = (int)m.size();
+        max_steps = (max_iter + 1) / 2 + 1;
+        if (cudaStreamCreateWithFlags(&master, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaHostAlloc(&flags, 2 * G * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+            cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        std::memset(flags, 0, 2 * G * sizeof(int));
+        joins.assign(G, nullptr);
+        for (auto& e : joins)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+        // the first launch follows every member's set-up work
+        for (int k = 0; k < G; ++k) {
+            cudaEventRecord(joins[k], slots[m[k]].stream);
+            cudaStreamWaitEvent(master, joins[k], 0);
+        }
+        for (int slot = 0; slot < 2; ++slot) {
+            cudaGraph_t g = nullptr;
+            if (cudaStreamBeginCapture(master, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+            cudaEventRecord(fork, master);
+            for (int k = 0; k < G; ++k) {
+                DevProblem& d = slots[m[k]];
+                cudaStreamWaitEvent(d.stream, fork, 0);
+                d.eng->enqueue_step(d.stream, &flags[slot * G + k]);
+                cudaEventRecord(joins[k], d.stream);
+                cudaStreamWaitEvent(master, joins[k], 0);
+            }
+            if (cudaStreamEndCapture(master, &g) != cudaSuccess || !g) {
+                cudaGetLastError();
+                return false;
+            }
+            const cudaError_t ce = cudaGraphInstantiate(&exec[slot], g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) {
+                cudaGetLastError();
+                exec[slot] = nullptr;
+                return false;
+            }
+        }
+        return true;
+    }
+
+    // Non-blocking: keeps two steps in flight and reads the flags of the oldest one.
+    int advance() {
+        const int G = (int)members.size();
+        while (!done && launched - seen < 2 && launched < max_steps) {
+            const int s = launched & 1;
+            if (cudaGraphLaunch(exec[s], master) != cudaSuccess) return E_CUDA;
+            cudaEventRecord(ev[s], master);
+            ++launched;
+        }
+        if (seen < launched) {
+            const cudaError_t q = cudaEventQuery(ev[seen & 1]);
+            if (q == cudaErrorNotReady) return E_OK;
+            if (q != cudaSuccess) return E_CUDA;
+            bool all = true;
+            for (int k = 0; k < G; ++k) all = all && flags[(seen & 1) * G + k] != 0;
+            ++seen;
+            if (all || seen >= max_steps) done = true;
+        }
+        return E_OK;
+    }
+
+    // Once done: every member's stream follows the last step launched.
+    void join(std::vector<DevProblem>& slots) {
+        cudaEventRecord(fork, master);
+        for (int i : members) cudaStreamWaitEvent(slots[i].stream, fork, 0);
+    }
+};
+
 }  // namespace
 }  // namespace uaamg
 
@@ -256,18 +361,49 @@ uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_problem* prob
         if ((e = d.eng->solve_begin(d.args(opts))) != E_OK)
             return api::map_engine(h, e, "batch: solve", d.eng);
     }
+    // optional: the problems of at most batch_group_cells padded cells share one graph
+    GroupGraph grp;
+    std::vector<char> grouped(n, 0);
+    if (h->batch_group_cells > 0) {
+        std::vector<int> m;
+        for (int i = 0; i < n; ++i)
+            if ((long long)slots[i].n <= h->batch_group_cells) m.push_back(i);
+        if (m.size() >= 2 && grp.build(slots, m, opts.max_iter)) {
+            for (int i : m) grouped[i] = 1;
+        } else {
+            grp.release();
+        }
+    }
     // advance every unfinished problem: keep two steps queued, collect finished ones
     std::vector<char> open(n, 1);
     int left = n;
     uaamg_status first_bad = UAAMG_OK;
+    bool group_joined = false;
     while (left > 0) {
         bool progressed = false;
+        if (!grp.members.empty() && !grp.done) {
+            const int seen = grp.seen;
+            if (grp.advance() != E_OK) {
+                grp.release();
+                return api::fail(h, UAAMG_CUDA_ERROR, "batch: grouped graph launch");
+            }
+            progressed = grp.seen != seen;
+        }
+        if (grp.done && !group_joined) {
+            grp.join(slots);
+            group_joined = true;
+        }
         for (int i = 0; i < n; ++i) {
             if (!open[i]) continue;
             DevProblem& d = slots[i];
             bool stopped = false;
-            int e = d.eng->solve_step();
-            if (e == E_OK) e = d.eng->solve_poll(false, &stopped);
+            int e = E_OK;
+            if (grouped[i]) {
+                stopped = group_joined;
+            } else {
+                e = d.eng->solve_step();
+                if (e == E_OK) e = d.eng->solve_poll(false, &stopped);
+            }
             if (e != E_OK) return api::map_engine(h, e, "batch: solve", d.eng);
             if (!stopped) continue;
             SolveResult r;
@@ -289,7 +425,14 @@ uaamg_status uaamg_solve_batch(uaamg_handle* h, int n, const uaamg_problem* prob
         }
         if (!progressed) std::this_thread::yield();
     }
+    grp.release();
     return first_bad;
+}
+
+uaamg_status uaamg_set_batch_group(uaamg_handle* h, long long max_cells) {
+    if (!h || max_cells < 0) return UAAMG_INVALID_ARG;
+    h->batch_group_cells = max_cells;
+    return UAAMG_OK;
 }
 
 uaamg_status uaamg_set_autotune(uaamg_handle* h, int on) {

@@ -145,6 +145,11 @@ class Handle:
         level."""
         self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(mode)), "vcycle")
 
+    def set_batch_group(self, max_cells=0):
+        """solve_batch: problems of at most max_cells padded cells share one CUDA graph
+        per step (uaamg_set_batch_group; 0: one graph each)."""
+        self._check(self.lib.uaamg_set_batch_group(self.h, int(max_cells)), "batch_group")
+
     def set_smoothing(self, sweeps_fine=1, sweeps_coarse=1):
         """Pre- and post-smoothing sweeps on the finest and the coarse levels
         (uaamg_set_smoothing; 1, 1 is the reference's V(1,1))."""
