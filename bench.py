@@ -604,7 +604,13 @@ def run_batch(args):
     probs_all = workloads.batch96()
     probs = shard.shard(probs_all, rank, ws)
     hd = Handle(device)
+    tune_file = None
     if args.autotune:
+        # the autotuner's choices (z chunks per level shape, smoothing schedule per
+        # problem class) go to a cache file, read back below to report them
+        from uaamg_b200.solver import set_tune_cache
+        tune_file = os.path.join(tempfile.mkdtemp(), "tune.json")
+        set_tune_cache(tune_file)
         hd.set_autotune(True)
     hd.set_vcycle_kernels(args.vcycle_kernels)
     opts = hd.options(args.precision, 1e-6, 500, "rel")
@@ -654,7 +660,21 @@ def run_batch(args):
         }
         print(json.dumps(line), flush=True)
         return 0
-    # beside: one problem at a time through uaamg_solve, and plain FP32 batched
+    # beside: the small problems sharing one graph per step, one problem at a time
+    # through uaamg_solve, and plain FP32 batched
+    group_cells = 1 << 17
+    hd.set_batch_group(group_cells)
+    step(opts)
+    tg = statistics.mean(step(opts)[0] for _ in range(max(1, args.steps // 2)))
+    hd.set_batch_group(0)
+    schedules = None
+    if tune_file and os.path.exists(tune_file):
+        ent = json.load(open(tune_file))["entries"]
+        schedules = {}
+        for k, v in ent.items():
+            if k.startswith("nu|"):
+                schedules[f"V({v[0]},{v[0]}) fine, V({v[1]},{v[1]}) coarse"] = \
+                    schedules.get(f"V({v[0]},{v[0]}) fine, V({v[1]},{v[1]}) coarse", 0) + 1
     seq = 0.0
     for (s, r, dx, dy, dz), p in zip(probs, ps):
         hd.set_problem(s, dx, dy, dz)
@@ -685,6 +705,10 @@ def run_batch(args):
                 "d2h_bytes_per_step": sum(s.size * 8 for s, *_ in probs)},
         "clocks": clocks,
         "beside": {"sequential_ms": round(seq, 3), "batched_speedup": round(seq / ms, 2),
+                   "grouped_graph_ms": round(tg, 3),
+                   "grouped_graph_note": f"problems of at most {group_cells} padded cells share "
+                                         "one CUDA graph per step (uaamg_set_batch_group)",
+                   "autotuned_schedules": schedules,
                    "fp32_batch_ms": round(t32, 3),
                    "fp32_worst_true_rel_residual": max(
                        a / b for a, b in (O.true_residual(s, r, p, dx, dy, dz)
