@@ -76,15 +76,16 @@ struct KTag {
 };
 
 // Kernel launch on the engine's stream.  Outside the per-kernel profiler every
-// launch carries the programmatic-stream-serialisation attribute (the kernels
-// begin with pdl_entry, common.cuh), so a kernel's launch and block scheduling
-// overlap the end of the one before it.
+// launch on a created stream (the CUDA-graph captures always use one) carries the
+// programmatic-stream-serialisation attribute (the kernels begin with pdl_entry,
+// common.cuh), so a kernel's launch and block scheduling overlap the end of the one
+// before it; launches on the legacy default stream are plain.
 #define UAAMG_LAUNCH_SMEM(tag, kern, grid, block, smem, ...)              \
     do {                                                                  \
         const KTag tg_ = (tag);                                           \
         cudaEvent_t e0_ = nullptr, e1_ = nullptr;                         \
         if (prof_on_) prof_begin(tg_, &e0_, &e1_);                        \
-        if (pdl_ && !prof_on_) {                                          \
+        if (pdl_ && !prof_on_ && st_ != nullptr) {                        \
             cudaLaunchConfig_t cf_ = {};                                  \
             cudaLaunchAttribute at_[1];                                   \
             at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization; \
