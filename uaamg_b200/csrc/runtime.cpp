@@ -595,6 +595,10 @@ void finish(uaamg_server* s, Ticket* t, int status) {
 bool start_request(uaamg_server* s, Ticket* t) {
     const uaamg_request& q = t->req;
     const uaamg_server_config& c = s->cfg;
+    int slot = -1;
+    for (int i = 0; i < (int)s->stage.size(); ++i)
+        if (!s->stage[i].used) { slot = i; break; }
+    if (slot < 0) return false;  // every staging slot busy: wait for a finishing request
     SimState* sim = nullptr;
     auto it = s->sims.find(q.sim_id);
     if (it != s->sims.end()) {
@@ -629,10 +633,7 @@ bool start_request(uaamg_server* s, Ticket* t) {
     } else {
         warm = c.warm_start && sim->has_p;
     }
-    int slot = -1;
-    for (int i = 0; i < (int)s->stage.size(); ++i)
-        if (!s->stage[i].used) { slot = i; break; }
-    if (slot < 0 || !s->stage[slot].ensure(sim->dp.n)) { finish(s, t, UAAMG_OOM); return true; }
+    if (!s->stage[slot].ensure(sim->dp.n)) { finish(s, t, UAAMG_OOM); return true; }
     StageBuf& b = s->stage[slot];
     b.used = true;
     t->slot = slot;
@@ -754,7 +755,8 @@ void worker_main(uaamg_server* s) {
                 });
                 continue;
             }
-            int room = s->cfg.max_active - (int)s->active.size();
+            // a result waiting for its host copy still holds its staging slot
+            int room = s->cfg.max_active - (int)s->active.size() - s->copying;
             std::vector<long long> blocked;
             for (auto it = s->pending.begin(); it != s->pending.end() && room > 0;) {
                 Ticket* t = *it;
