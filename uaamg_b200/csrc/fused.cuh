@@ -447,19 +447,21 @@ __global__ void __launch_bounds__(kThreads)
         const FCell q0 = r1Role0 ? cR1 : cR2, q1 = r1Role0 ? cR2 : cR1;
         FHist<T> ht[2] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
         T hr[2] = {T(0), T(0)};  // ring columns: last odd value
-        auto xp_of = [&](int p) -> T* { return xpl + (size_t)((p + 3) % 3) * (C::XB / sizeof(T)); };
+        // stages of planes s+1, s, s-1, s-2 and the shared x planes s+1, s, s-1,
+        // rotated once per step (planes below p0 are never read)
+        const unsigned char* ring_end = sm + C::OFF_RING + S * P::STAGE;
+        const unsigned char* sp1 = R.at(s0 + 1);
+        const unsigned char* s00 = R.at(s0);
+        const unsigned char* sm1 = R.at(s0 - 1);
+        const unsigned char* sm2 = R.at(s0 - 2);
+        T* xn = xpl + (size_t)((s0 + 4) % 3) * (C::XB / sizeof(T));
+        T* xc = xpl + (size_t)((s0 + 3) % 3) * (C::XB / sizeof(T));
+        T* xo = xpl + (size_t)((s0 + 5) % 3) * (C::XB / sizeof(T));
         // one step; R0: the role whose cell is even at plane s (compile-time)
         auto step = [&](int s, auto R0c) -> bool {
             constexpr int RC = decltype(R0c)::value, RO = 1 - RC;
             const FCell& tc = RC == 0 ? t0 : t1;
             const FCell& qc = RC == 0 ? q0 : q1;
-            const unsigned char* sp1 = R.at(s + 1);
-            const unsigned char* s00 = R.at(s);
-            const unsigned char* sm1 = R.at(s - 1);
-            const unsigned char* sm2 = R.at(s - 2);
-            T* xn = xp_of(s + 1);
-            T* xc = xp_of(s);
-            const T* xo = xp_of(s - 1);
             // 1. odd values of plane s+1
             const T on = oval(sp1, tc, s + 1);
             xn[tc.qt] = on;
@@ -489,6 +491,17 @@ __global__ void __launch_bounds__(kThreads)
             ht[RC].o1 = on;
             ht[RC].e1 = en;
             hr[RC] = onr;
+            sm2 = sm1;
+            sm1 = s00;
+            s00 = sp1;
+            sp1 += P::STAGE;
+            if (sp1 == ring_end) sp1 = sm + C::OFF_RING;
+            {
+                T* t = xo;
+                xo = xc;
+                xc = xn;
+                xn = t;
+            }
             bool okk = true;
             if (tid == 0 && s + 2 <= R.plast) okk = R.wait(s + 2);
             if (!step_barrier(okk, err)) return false;
@@ -569,9 +582,10 @@ __global__ void __launch_bounds__(kThreads)
     double acc[1] = {0.0};
     T pA1 = T(0), pB1 = T(0), pA2 = T(0), pB2 = T(0);  // own columns at planes s-1, s-2
     uint32_t cA1 = 0, cB1 = 0;                          // their codes at plane s-1
+    const unsigned char* stg = R.at(R.p0);                // stage of plane s, rotated
+    const unsigned char* ring_end = sm + Lay::OFF_RING + S * P::STAGE;
 #pragma unroll 1
     for (int s = R.p0; s <= ke; ++s) {
-        const unsigned char* stg = R.at(s);
         T* xs = xb + (size_t)(s & 1) * (C::XB / sizeof(T));
         const T* xo = xb + (size_t)((s + 1) & 1) * (C::XB / sizeof(T));
         const uint32_t cA = stg[P::OFF_CODE + o.ca], cB = stg[P::OFF_CODE + o.ca + WC];
@@ -614,6 +628,8 @@ __global__ void __launch_bounds__(kThreads)
         pA2 = pA1; pB2 = pB1;
         pA1 = pA; pB1 = pB;
         cA1 = cA; cB1 = cB;
+        stg += P::STAGE;
+        if (stg == ring_end) stg = sm + Lay::OFF_RING;
         bool okk = true;
         if (tid == 0 && s + 1 <= R.plast) okk = R.wait(s + 1);
         if (!step_barrier(okk, err)) return;
