@@ -927,9 +927,9 @@ def main():
     ap.add_argument("--autotune", dest="autotune", action="store_true", default=True,
                     help="time the marches' z-chunk lengths at set-up (default on; outside the timing)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
-    ap.add_argument("--vcycle-kernels", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
+    ap.add_argument("--vcycle-kernels", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="uaamg_set_vcycle_kernels mode (0 default: two fused marches a "
-                         "level; 3: 2D levels as flat walks; 4: four marches a level)")
+                         "level; 3: four marches a level)")
     ap.add_argument("--serve-ids", type=int, default=500)
     ap.add_argument("--served-ids", type=int, default=100,
                     help="simulation ids of the bounded serving run in the default line "

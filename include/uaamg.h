@@ -143,12 +143,10 @@ UAAMG_API uaamg_status uaamg_set_dirichlet_walls(uaamg_handle* h, int on);
  * 1 = one kernel per colour sweep, restriction and prolongation, step by step as
  * UAAMGPreconditioner3D::vCycle (uaamg_preconditioner_3d.cpp:183-196);
  * 2 = the two-march levels on every level and a separate coarsest-level kernel;
- * 3 = as 0, with every march level of a 2D problem as four flat walks over the level
- * instead of marches (a 2D level is one plane: nothing to pipeline);
- * 4 = as 0 with four marches per level (forward sweep; residual + restriction;
+ * 3 = as 0 with four marches per level (forward sweep; residual + restriction;
  * prolongation + even colour; odd colour);
- * 5 = four marches per level on every level and a separate coarsest-level kernel.
- * All give identical results in FP64; 1, 2, 4 and 5 exist to cross-check 0. */
+ * 4 = four marches per level on every level and a separate coarsest-level kernel.
+ * All give identical results in FP64; 1 to 4 exist to cross-check 0. */
 UAAMG_API uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps);
 
 /* Smoothing schedule of this handle's V-cycle: pre- and post-smoothing sweeps (1 to 4)

@@ -62,7 +62,6 @@ def lib():
         L.oh_level_solid.argtypes = [_p, _i, _p]
         L.oh_level_coeffs.argtypes = [_p, _i, _p, _p, _p, _p]
         L.oh_vcycle.argtypes = [_p, _p, _p]
-        L.oh_vcycle_stages.argtypes = [_p, _p, _i, _p, _p, _p, _p, _p]
         L.oracle_pcg.restype = _i
         L.oracle_pcg.argtypes = [_i, _i, _i, _i, _d, _d, _d, _p, _p, _p, _i, _d, _i, _i, _i,
                                  _i, _p, C.POINTER(_i)]
@@ -181,19 +180,6 @@ class Hierarchy:
         z = np.zeros_like(r)
         lib().oh_vcycle(self.h, _ptr(r), _ptr(z))
         return z
-
-    def vcycle_stages(self, r, level=0):
-        """Level `level`'s states in one V-cycle of r: (its b on entry, x after the
-        forward sweep, the next level's b after the restriction, the next level's x
-        before the prolongation, its x on exit)."""
-        if not 0 <= level < self.nlevels - 1:
-            raise ValueError("level must lie below the coarsest level")
-        r = _cd(r)
-        b_l, x_fwd, x_out = (np.zeros(self._shape(level)) for _ in range(3))
-        b1, x1 = np.zeros(self._shape(level + 1)), np.zeros(self._shape(level + 1))
-        lib().oh_vcycle_stages(self.h, _ptr(r), level, _ptr(b_l), _ptr(x_fwd), _ptr(b1), _ptr(x1),
-                               _ptr(x_out))
-        return b_l, x_fwd, b1, x1, x_out
 
 
 def pcg(solid, rhs, dx, dy, dz=1.0, max_iter=200, tol=1e-6, precond=True, tol_mode=1,

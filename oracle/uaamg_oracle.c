@@ -322,52 +322,6 @@ void oh_vcycle(oh_hier* h, const double* r, double* z) {
             }
 }
 
-/* vcycle (uaamg_preconditioner_3d.cpp:183-196) with level cl's states captured: its b
- * on entry, x after the forward sweep, the next level's b after the restriction and
- * x before the prolongation, and its x on exit. */
-static void vcycle_cap(oh_hier* h, int l, int cl, double* b_l, double* x_fwd, double* b1,
-                       double* x1, double* x_out) {
-    olevel* L = &h->L[l];
-    if (l == h->nl - 1) {
-        for (int s = 0; s < 10; s++) { smooth(L, 0); smooth(L, 1); }
-        return;
-    }
-    const size_t n = sizeof(double) * (size_t)L->n;
-    if (l == cl && b_l) memcpy(b_l, L->b, n);
-    smooth(L, 0);
-    if (l == cl && x_fwd) memcpy(x_fwd, L->p, n);
-    olevel* C = &h->L[l + 1];
-    restrict_residual(L, C);
-    if (l == cl && b1) memcpy(b1, C->b, sizeof(double) * (size_t)C->n);
-    memset(C->p, 0, sizeof(double) * (size_t)C->n);
-    vcycle_cap(h, l + 1, cl, b_l, x_fwd, b1, x1, x_out);
-    if (l == cl && x1) memcpy(x1, C->p, sizeof(double) * (size_t)C->n);
-    prolongate_add(C, L);
-    smooth(L, 1);
-    if (l == cl && x_out) memcpy(x_out, L->p, n);
-}
-
-/* oh_vcycle with level cl's intermediate states captured (for stage-by-stage checks
- * of an implementation of one level): level cl's b on entry and x after the forward
- * sweep, level cl+1's b after the restriction and x before the prolongation, and
- * level cl's x on exit.  Each pointer may be NULL; cl must be below the coarsest
- * level.  Coarse levels' b start at 0, so b of a solid coarse cell stays 0. */
-void oh_vcycle_stages(oh_hier* h, const double* r, int cl, double* b_l, double* x_fwd,
-                      double* b1, double* x1, double* x_out) {
-    olevel* L0 = &h->L[0];
-    for (int i = 1; i <= L0->nx; i++)
-        for (int j = 1; j <= L0->ny; j++)
-            for (int k = KLO(L0); k <= KHI(L0); k++) {
-                long id = cid(L0, i, j, k);
-                L0->b[id] = r[id];
-            }
-    for (int l = 0; l < h->nl; l++) {
-        memset(h->L[l].p, 0, sizeof(double) * (size_t)h->L[l].n);
-        if (l > 0) memset(h->L[l].b, 0, sizeof(double) * (size_t)h->L[l].n);
-    }
-    vcycle_cap(h, 0, cl, b_l, x_fwd, b1, x1, x_out);
-}
-
 /* ------------------------------------------------------------------------- */
 /* PCG (pcg_3d.cpp:18-125, pcg.cpp:18-126)                                    */
 

@@ -29,11 +29,6 @@ void     oh_level_coeffs(const oh_hier* h, int l, double* cx, double* cy, double
                          double* diag);
 /* z = M^{-1} r: one V(1,1) cycle (UAAMGPreconditioner[3D]::apply). */
 void     oh_vcycle(oh_hier* h, const double* r, double* z);
-/* The same cycle with level cl's stages captured (padded arrays, each may be NULL):
- * level cl's b on entry and x after the forward sweep, level cl+1's b after the
- * restriction and x before the prolongation, level cl's x on exit (cl < nlevels-1). */
-void     oh_vcycle_stages(oh_hier* h, const double* r, int cl, double* b_l, double* x_fwd,
-                          double* b1, double* x1, double* x_out);
 
 /* PCG with the reference's semantics (PCG::solve / PCG3D::solve).
  *   precond    1 = UAAMG V-cycle, 0 = identity (plain CG)

@@ -36,14 +36,13 @@ def rel_l2_meanfree(a, b, solid):
 # --- golden fixtures ---------------------------------------------------------
 
 
-@pytest.fixture(params=["fused", "sweeps", "fused_all", "flat2d", "march", "march_all"])
+@pytest.fixture(params=["fused", "sweeps", "fused_all", "march", "march_all"])
 def vkernels(request, handle):
     """Every V-cycle implementation: two fused z marches a level with the single-block
-    small-level kernel, per-colour sweeps, fused marches on every level, flat walks on
-    the 2D march levels (fused marches on a 3D problem), four z marches a level with
-    the small-level kernel, and four marches on every level."""
-    handle.set_vcycle_kernels({"fused": 0, "sweeps": 1, "fused_all": 2, "flat2d": 3, "march": 4,
-                               "march_all": 5}[request.param])
+    small-level kernel, per-colour sweeps, fused marches on every level, four z marches
+    a level with the small-level kernel, and four marches on every level."""
+    handle.set_vcycle_kernels({"fused": 0, "sweeps": 1, "fused_all": 2, "march": 3,
+                               "march_all": 4}[request.param])
     yield request.param
     handle.set_vcycle_kernels(0)
 

@@ -42,10 +42,10 @@ def lap_of(g):
     return g["lap_diag"], g["lap_off_x"], g["lap_off_y"]
 
 
-@pytest.fixture(params=["fused", "sweeps", "fused_all", "flat2d", "march", "march_all"])
+@pytest.fixture(params=["fused", "sweeps", "fused_all", "march", "march_all"])
 def vkernels(request, handle):
-    handle.set_vcycle_kernels({"fused": 0, "sweeps": 1, "fused_all": 2, "flat2d": 3, "march": 4,
-                               "march_all": 5}[request.param])
+    handle.set_vcycle_kernels({"fused": 0, "sweeps": 1, "fused_all": 2, "march": 3,
+                               "march_all": 4}[request.param])
     yield request.param
     handle.set_vcycle_kernels(0)
 

@@ -33,7 +33,7 @@ UNITS = [
     ("tunecache.cpp", ["-x", "cu"]),
     ("project.cu", ["-fmad=false"]),
 ]
-HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "fused.cuh", "flat2d.cuh", "tail.cuh", "vec.cuh", "tma.cuh",
+HEADERS = ["common.cuh", "kernels.cuh", "march.cuh", "fused.cuh", "tail.cuh", "vec.cuh", "tma.cuh",
            "engine.cuh", "engine.h", "handle.h"]
 
 

@@ -251,7 +251,7 @@ uaamg_status uaamg_set_stream(uaamg_handle* h, void* stream) {
 
 uaamg_status uaamg_set_vcycle_kernels(uaamg_handle* h, int sweeps) {
     if (!h) return UAAMG_INVALID_ARG;
-    if (sweeps < 0 || sweeps > 5) return fail(h, UAAMG_INVALID_ARG, "V-cycle kernels: 0 to 5");
+    if (sweeps < 0 || sweeps > 4) return fail(h, UAAMG_INVALID_ARG, "V-cycle kernels: 0 to 4");
     h->sweeps = sweeps;
     return UAAMG_OK;
 }

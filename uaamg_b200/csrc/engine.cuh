@@ -24,7 +24,6 @@
 #include <vector>
 
 #include "engine.h"
-#include "flat2d.cuh"
 #include "fused.cuh"
 #include "kernels.cuh"
 #include "tail.cuh"
@@ -284,11 +283,6 @@ public:
         nu_fine_ = fine;
         nu_coarse_ = coarse;
     }
-    void set_flat2d(bool on) override {
-        if (on == flat2d_) return;
-        drop_graph();  // a captured step holds the other kernels
-        flat2d_ = on;
-    }
     void set_fused(bool on) override {
         if (on == fused_) return;
         drop_graph();
@@ -388,7 +382,6 @@ private:
     bool graphs_ = true;   // replay the PCG step as a CUDA graph
     bool autotune_ = false;  // time the marches' z-chunk lengths at set-up
     bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
-    bool flat2d_ = false;    // 2D finest level as flat walks (flat2d.cuh) instead of marches
     bool fused_ = true;      // two fused marches a level (fused.cuh) instead of four
     bool pdl_ = true;        // programmatic dependent launch between the kernels
     int nu_fine_ = 1, nu_coarse_ = 1;  // pre- and post-smoothing sweeps: finest / coarse levels
@@ -957,24 +950,6 @@ private:
         return m;
     }
 
-    // The coarse operator of level l as the flat 2D walks read it (flat2d.cuh).
-    F2Op<T, CS> flat_op(int l) const {
-        F2Op<T, CS> op;
-        op.dg = l > 0 ? lv_[l].dg : nullptr;
-        op.cx = l > 0 ? lv_[l].hcx : nullptr;
-        op.cy = l > 0 ? lv_[l].hcy : nullptr;
-        return op;
-    }
-
-    // grid of a flat 2D walk (flat2d.cuh) over rows of `rows` items of 32 columns:
-    // eight rows a block, up to 8 blocks per SM (within the partials' capacity)
-    dim3 flat_grid(long long rows, int cols) const {
-        const long long items = rows * ((cols + 31) / 32);
-        long long nb = std::min<long long>((items + 7) / 8, 8LL * num_sms_);
-        nb = std::min<long long>(nb, reduce_blocks_);
-        return dim3((unsigned)(nb < 1 ? 1 : nb));
-    }
-
     // Tensor maps of a fused march over level l (boxes with a 2-cell ring); up: with
     // the next-coarser level's x as parent boxes.
     FMaps fmaps(int l, bool up) const {
@@ -1011,22 +986,6 @@ private:
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
-        if constexpr (std::is_same<CSL, CS>::value) {
-            if (DIM == 2 && flat2d_ && nu == 1) {
-                // b, code (coarse levels: couplings, diagonal) in; x out / b, x, code in;
-                // coarse b out
-                const F2Op<T, CS> op = flat_op(l);
-                T* b = l == 0 ? r_ : L.b;
-                T* x = l == 0 ? z_ : L.x;
-                UAAMG_LAUNCH((KTag{K_FWD, l, c * (2.0 * t + 1.0 + coef)}), (k_fwd_flat2d<T, CS, FINE>),
-                             flat_grid((L.g.ny + 1) / 2, L.g.nx), dim3(32, 8), mlevel(l), op, L.code, b,
-                             x, done);
-                UAAMG_LAUNCH((KTag{K_RES, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
-                             (k_res_flat2d<T, CS, FINE>), flat_grid(Cl.g.ny, Cl.g.nx), dim3(32, 8),
-                             mlevel(l), op, L.code, b, x, Cl.code, Cl.b, done);
-                return;
-            }
-        }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         if (fused_ && nu == 1) {
             // b, code (coarse levels: diagonal, couplings) in; coarse code in, coarse b out
@@ -1067,26 +1026,6 @@ private:
         const LevelBuf<T, CS>& Cl = lv_[l + 1];
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
-        if constexpr (std::is_same<CSL, CS>::value) {
-            if (DIM == 2 && flat2d_ && nu == 1) {
-                const dim3 fg = flat_grid((L.g.ny + 1) / 2, L.g.nx), fb(32, 8);
-                const F2Op<T, CS> op = flat_op(l);
-                T* b = l == 0 ? r_ : L.b;
-                T* x = l == 0 ? z_ : L.x;
-                // b, code, coarse x in; x out / b, x, code in; odd x out
-                UAAMG_LAUNCH((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),
-                             (k_upe_flat2d<T, CS, FINE>), fg, fb, mlevel(l), op, L.code, b, Cl.x, x, done);
-                if (FINE && zdot)
-                    UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
-                                 (k_upo_flat2d<T, CS, FINE, true>), fg, fb, mlevel(l), op, L.code, b, x,
-                                 done, partials_, cg_);
-                else
-                    UAAMG_LAUNCH((KTag{K_UPO, l, c * (2.5 * t + 1.0 + coef)}),
-                                 (k_upo_flat2d<T, CS, FINE, false>), fg, fb, mlevel(l), op, L.code, b, x,
-                                 done, partials_, cg_);
-                return;
-            }
-        }
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
         if (fused_ && nu == 1) {

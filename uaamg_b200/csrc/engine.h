@@ -99,9 +99,6 @@ public:
     // Marches: run the small levels and the coarsest solve as one single-block
     // kernel (default on; off: marches on every level).
     virtual void set_small_levels(bool on) = 0;
-    // 2D problems: the four V-cycle steps of every march level as flat walks over the
-    // level (flat2d.cuh) instead of z marches (default off).
-    virtual void set_flat2d(bool on) = 0;
     // Marches: two fused marches per level (fused.cuh: down = forward sweep, residual
     // and restriction; up = prolongation and reverse sweep) instead of four
     // (march.cuh).  Default on.

@@ -30,8 +30,8 @@ struct uaamg_handle {
     bool ready[3] = {false, false, false};
     int sweeps = 0;  // V-cycle kernels (uaamg_set_vcycle_kernels): 0 fused marches +
                      // small-level kernel, 1 sweeps, 2 fused marches on every level,
-                     // 3 as 0 with 2D march levels as flat walks, 4 four marches a level
-                     // + small-level kernel, 5 four marches on every level
+                     // 3 four marches a level + small-level kernel, 4 four marches on
+                     // every level
     int autotune = 0;
     int nu_fine = 1, nu_coarse = 1;  // smoothing sweeps (uaamg_set_smoothing)
     long long batch_group_cells = 0; // batch problems of at most this many padded cells
@@ -55,9 +55,8 @@ void free_batch(uaamg_handle* h);
 // The engine flags of a V-cycle kernel mode (uaamg_set_vcycle_kernels).
 inline void apply_vcycle_mode(uaamg::Engine* e, int mode) {
     e->set_vcycle_sweeps(mode == 1);
-    e->set_small_levels(mode == 0 || mode == 3 || mode == 4);
-    e->set_flat2d(mode == 3);
-    e->set_fused(mode == 0 || mode == 2 || mode == 3);
+    e->set_small_levels(mode == 0 || mode == 3);
+    e->set_fused(mode == 0 || mode == 2);
 }
 
 }  // namespace api

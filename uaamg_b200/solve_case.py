@@ -35,7 +35,7 @@ def main(argv=None):
     ap.add_argument("--workload", default="spheres",
                     choices=["spheres", "obstacle_2d", "layered_2d"])
     ap.add_argument("--project", action="store_true")
-    ap.add_argument("--vcycle-kernels", type=int, default=0, choices=[0, 1, 2, 3, 4, 5])
+    ap.add_argument("--vcycle-kernels", type=int, default=0, choices=[0, 1, 2, 3, 4])
     a = ap.parse_args(argv)
     if a.workload in ("obstacle_2d", "layered_2d"):
         solid, u0, v0, rhs, dx, dy, dt = workloads.obstacle_2d()

@@ -140,9 +140,8 @@ class Handle:
     def set_vcycle_kernels(self, mode):
         """0 / False: two fused z marches a level + the single-block small-level
         kernel (default); 1 / True: per-colour sweep kernels; 2: fused marches on every
-        level; 3: as 0 with every march level of a 2D problem as four flat walks;
-        4: four z marches a level + the small-level kernel; 5: four marches on every
-        level."""
+        level; 3: four z marches a level + the small-level kernel; 4: four marches on
+        every level."""
         self._check(self.lib.uaamg_set_vcycle_kernels(self.h, int(mode)), "vcycle")
 
     def set_batch_group(self, max_cells=0):
