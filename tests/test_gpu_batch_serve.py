@@ -125,20 +125,27 @@ def test_small_budget_evicts_idle_simulations():
 
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
 def test_autotuned_chunks_give_identical_results(prec):
-    # the z-chunk length changes only the blocks' shape, never the arithmetic
+    """The z-chunk length changes only the blocks' shape: the preconditioner (every
+    per-cell value) is bit-identical with autotuned chunks.  The solve's FP64 dot
+    products are summed per block, so a different chunk length sums them in another
+    order: the PCG iterates agree to rounding (FP64 1e-10, mixed 1e-6 relative) and
+    the iteration counts to one."""
     s, r = workloads.spheres_3d(80, 64, 72, 12, 3.0, 9.0, seed=11)
     h = 1.0 / 80
-    out = []
+    out, z = [], []
     for tune in (False, True):
         hd = Handle(0)
         hd.set_autotune(tune)
         hd.set_problem(s, h, h, h)
+        z.append(hd.precond_apply(r, prec))
         p = np.zeros_like(r)
         st = hd.solve(r, p, hd.options(prec, 1e-6, 300, "rel"), strict=True)
         out.append((p, st.iterations))
         hd.close()
-    assert out[0][1] == out[1][1]
-    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(z[0], z[1])
+    assert abs(out[0][1] - out[1][1]) <= 1
+    d = np.abs(out[0][0] - out[1][0]).max() / np.abs(out[0][0]).max()
+    assert d <= (1e-10 if prec == "fp64" else 1e-6), d
 
 
 @pytest.mark.parametrize("prec", ["mixed", "fp32", "fp64"])

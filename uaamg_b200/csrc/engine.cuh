@@ -625,7 +625,6 @@ private:
         // dynamic shared memory of the marches
         if ((e = march_attrs<DIM, true, CS>()) || (e = march_attrs<DIM, false, CS>()) ||
             (e = smem_attr(k_pmatvec<DIM, T>, PmvCfg<DIM, T>::BYTES)) ||
-            (e = smem_attr(k_pmatvec_col<T>, PmcCfg<T>::BYTES)) ||
             (e = fused_attrs<DIM, true, CS>()) || (e = fused_attrs<DIM, false, CS>()))
             return e;
         if constexpr (kHalf) {  // levels with FP32 couplings
@@ -794,8 +793,9 @@ private:
     // on the level's own buffers) for each z-chunk length in {2, 4, 8, 16, 32} and
     // keep the fastest; the choice is cached per GPU, precision, level shape and
     // march kind (tune_lookup / tune_store: for the process, and in the cache file
-    // when one is set).  Chunk length changes only the blocks' shape, not the
-    // arithmetic, so the results do not depend on it.
+    // when one is set).  Chunk length changes only the blocks' shape, not a per-cell
+    // value; the FP64 dot products are summed per block, so their rounding (and so
+    // the last bits of the iterates) may differ.
     template <int DIM>
     int tune() {
         cudaEvent_t a = nullptr, b = nullptr;
@@ -987,7 +987,9 @@ private:
         const double c = cells(L.g), cc = cells(Cl.g), t = sizeof(T);
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
-        if (fused_ && nu == 1) {
+        // a finest level with Dirichlet walls takes the four-march path (the fused
+        // finest level's branch-free cell table holds no wall terms)
+        if (fused_ && nu == 1 && !(FINE && dirichlet_)) {
             // b, code (coarse levels: diagonal, couplings) in; coarse code in, coarse b out
             UAAMG_LAUNCH_SMEM((KTag{K_DOWN, l, c * (t + 1.0 + coef) + cc * (t + 1.0)}),
                               (k_level_fused<DIM, T, FINE, CSL, false, false>), grid, blk,
@@ -1028,7 +1030,7 @@ private:
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
-        if (fused_ && nu == 1) {
+        if (fused_ && nu == 1 && !(FINE && dirichlet_)) {
             // b, code (coarse levels: diagonal, couplings), coarse x in; x out
             const KTag tag{K_UP, l, c * (2.0 * t + 1.0 + coef) + cc * t};
             if (FINE && zdot)
@@ -1170,15 +1172,10 @@ private:
             MarchMaps pm = maps<DIM>(0, true, false);  // z and the current search direction
             pm.v[0] = lv_[0].mx;
             pm.v[1] = from_p ? map_p_ : map_p2_;
-            const KTag tag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)};
-            if (fused_ && DIM == 3)  // column march (fused.cuh)
-                UAAMG_LAUNCH_SMEM(tag, (k_pmatvec_col<T>), march_grid<DIM>(g, lv_[0].zc), dim3(kThreads),
-                                  (PmcCfg<T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st, partials_, cg_,
-                                  err_);
-            else
-                UAAMG_LAUNCH_SMEM(tag, (k_pmatvec<DIM, T>), march_grid<DIM>(g, lv_[0].zc), dim3(kThreads),
-                                  (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st, partials_,
-                                  cg_, err_);
+            UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
+                              (k_pmatvec<DIM, T>), march_grid<DIM>(g, lv_[0].zc), dim3(kThreads),
+                              (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st, partials_, cg_,
+                              err_);
         }
         const long long nvec = (long long)g.n / Vec16<T>::N;
         // x_lo, r, p, Ap in; x_lo, r out (a fold after a replacement adds x_hi in and out)

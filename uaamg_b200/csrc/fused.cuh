@@ -85,13 +85,19 @@ template <int DIM, class T, class CS, bool FINE, bool UP>
 struct FCfg {
     using P = FPlan<DIM, T, CS, FINE, UP>;
     static constexpr int LAG = FINE ? 1 : 2;
-    static constexpr int S = DIM == 2 ? 1 : LAG + 3 + (FINE ? 3 : 1);
+    static constexpr int S = DIM == 2 ? 1 : LAG + 3 + (FINE ? (UP ? 2 : 3) : 1);
     static constexpr int NXP = DIM == 2 ? 1 : 3;  // shared x planes
     static constexpr size_t OFF_LUT = 128;          // after the stage barriers
-    static constexpr size_t OFF_RING = OFF_LUT + align128(64 * sizeof(T));
+    // finest level in FP32: the per-code table of the branch-free cell updates
+    static constexpr bool LEAN = FINE && sizeof(T) == 4;
+    static constexpr size_t OFF_TAB = OFF_LUT + align128(64 * sizeof(T));
+    static constexpr size_t OFF_RING = OFF_TAB + (LEAN ? 128 * sizeof(float4) : 0);
     static constexpr size_t OFF_X = OFF_RING + S * P::STAGE;
     static constexpr size_t XB = align128(RBox<T>::BYTES);
     static constexpr size_t BYTES = OFF_X + NXP * XB;
+    // resident blocks per SM the finest FP32 level is compiled for (registers);
+    // its shared memory fits five
+    static constexpr int MINB = LEAN && DIM == 3 ? 5 : 1;
     static_assert(S <= 16, "stage barriers: 128 bytes");
 };
 
@@ -193,7 +199,7 @@ struct FHist {
     }
 
 template <int DIM, class T, bool FINE, class CS, bool UP, bool ZDOT>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
     k_level_fused(const __grid_constant__ FMaps M, MLevel<T> L, const uint8_t* __restrict__ ccode,
                   T* __restrict__ out, const int* __restrict__ done, int* err, double* partials,
                   CGState* cg) {
@@ -209,6 +215,29 @@ __global__ void __launch_bounds__(kThreads)
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int i0 = 1 + kMX * (int)blockIdx.x, j0 = 1 + kMY * (int)blockIdx.y;
     if (FINE) build_lut<DIM, T>(lut, L.idx2, L.idy2, L.idz2);
+    // Finest level in FP32 (no Dirichlet walls: those problems take the four-march
+    // level): every cell update is a multiply-add driven by the table entry of its
+    // code's low 7 bits (neighbour bits, interior-fluid bit):
+    //   x = 1/d (0 unless an interior fluid cell the smoother relaxes, d >= 1e-30),
+    //   y = 1 for a relaxed cell, z = 1 for an interior fluid cell the smoother skips,
+    //   w = 1 for any interior fluid cell.
+    constexpr bool LEAN = C::LEAN;
+    const float4* tab = reinterpret_cast<const float4*>(sm + C::OFF_TAB);
+    if constexpr (LEAN) {
+        if (tid < 128) {
+            const uint32_t c = (uint32_t)tid;
+            float d = ((c & 1u) ? (float)L.idx2 : 0.f) + ((c & 2u) ? (float)L.idx2 : 0.f) +
+                      ((c & 4u) ? (float)L.idy2 : 0.f) + ((c & 8u) ? (float)L.idy2 : 0.f);
+            if (DIM == 3) d = d + ((c & 16u) ? (float)L.idz2 : 0.f) + ((c & 32u) ? (float)L.idz2 : 0.f);
+            const bool act = (c & kActive) != 0, skip = act && d < 1e-30f;
+            float4 e;
+            e.x = act && !skip ? mdiv<float, CS>(1.0f, d) : 0.f;
+            e.y = act && !skip ? 1.f : 0.f;
+            e.z = skip ? 1.f : 0.f;
+            e.w = act ? 1.f : 0.f;
+            reinterpret_cast<float4*>(sm + C::OFF_TAB)[tid] = e;
+        }
+    }
 
     // --- per-cell arithmetic --------------------------------------------------
     auto code_at = [&](const unsigned char* st, const FCell& c) -> uint32_t {
@@ -259,6 +288,11 @@ __global__ void __launch_bounds__(kThreads)
     // odd-colour value at plane k: pre-smoothed (b + 0)/d, plus the prolongation on
     // the way up; 0 on cells that are not interior fluid
     auto oval = [&](const unsigned char* st, const FCell& c, int k) -> T {
+        if constexpr (LEAN) {
+            const float4 t = tab[code_at(st, c) & 127u];
+            if constexpr (UP) return b_at(st, c) * t.x + t.w * prolong(st, c);
+            else return b_at(st, c) * t.x;
+        }
         const uint32_t code = code_at(st, c);
         if (!(code & kActive)) return T(0);
         const T d = diag_of(st, c, code, k);
@@ -271,6 +305,14 @@ __global__ void __launch_bounds__(kThreads)
     // 0 + the prolongation)
     auto evalc = [&](const unsigned char* st, const unsigned char* stm, const T* xv, const FCell& c,
                      int k, T op, T om) -> T {
+        if constexpr (LEAN) {
+            const float4 t = tab[code_at(st, c) & 127u];
+            const int q = c.qt;
+            T nb = L.idx2 * (xv[q + 1] + xv[q - 1]) + L.idy2 * (xv[q + WT] + xv[q - WT]);
+            if (DIM == 3) nb = nb + L.idz2 * (op + om);
+            if constexpr (UP) return (b_at(st, c) + nb) * t.x + t.z * prolong(st, c);
+            else return (b_at(st, c) + nb) * t.x;
+        }
         const uint32_t code = code_at(st, c);
         if (!(code & kActive)) return T(0);
         const T d = diag_of(st, c, code, k);
@@ -312,7 +354,18 @@ __global__ void __launch_bounds__(kThreads)
                           T zpE, T zmE, T (&rlo)[2]) {
         const uint32_t kO = code_at(st, cO), kE = code_at(st, cE);
         T resO = UP ? vO : T(0), resE = UP ? vE : T(0);
-        if (kO & kActive) {  // odd cell: reverse-sweep update / residual
+        if constexpr (LEAN) {
+            const float4 tO = tab[kO & 127u], tE = tab[kE & 127u];
+            const int q = cO.qt;
+            T nb = L.idx2 * (xv[q + 1] + xv[q - 1]) + L.idy2 * (xv[q + WT] + xv[q - WT]);
+            if (DIM == 3) nb = nb + L.idz2 * (zpO + zmO);
+            if constexpr (UP) {
+                resO = (b_at(st, cO) + nb) * tO.x + tO.z * vO;  // a skipped cell keeps vO
+            } else {
+                resO = tO.y * nb + tO.z * b_at(st, cO);
+                resE = tE.z * b_at(st, cE);
+            }
+        } else if (kO & kActive) {  // odd cell: reverse-sweep update / residual
             const T d = diag_of(st, cO, kO, k);
             if constexpr (UP) {
                 if (!(d < T(1e-30))) {
@@ -337,7 +390,7 @@ __global__ void __launch_bounds__(kThreads)
                 }
             }
         }
-        if constexpr (!UP) {
+        if constexpr (!UP && !LEAN) {
             if (kE & kActive) {  // even cell: residual (0 after its relaxation in FP32)
                 const T d = diag_of(st, cE, kE, k);
                 if constexpr (kFull) {
@@ -358,17 +411,30 @@ __global__ void __launch_bounds__(kThreads)
             if (inO) out[cO.gid + base] = resO;
             if (inE) out[cE.gid + base] = resE;
             if (ZDOT) {
-                if ((kO & kActive) && inO) {
-                    const double zv = (double)resO, rv = (double)b_at(st, cO);
-                    acc[0] += zv;
-                    acc[1] += rv * zv;
-                    acc[2] += rv;
-                }
-                if ((kE & kActive) && inE) {
-                    const double zv = (double)resE, rv = (double)b_at(st, cE);
-                    acc[0] += zv;
-                    acc[1] += rv * zv;
-                    acc[2] += rv;
+                if constexpr (LEAN) {
+                    // z and b are 0 on every cell that is not interior fluid (ghosts,
+                    // padding and cells past the level included)
+                    const double zo = (double)resO, ro = (double)b_at(st, cO);
+                    const double ze = (double)resE, re = (double)b_at(st, cE);
+                    acc[0] += zo;
+                    acc[1] += ro * zo;
+                    acc[2] += ro;
+                    acc[0] += ze;
+                    acc[1] += re * ze;
+                    acc[2] += re;
+                } else {
+                    if ((kO & kActive) && inO) {
+                        const double zv = (double)resO, rv = (double)b_at(st, cO);
+                        acc[0] += zv;
+                        acc[1] += rv * zv;
+                        acc[2] += rv;
+                    }
+                    if ((kE & kActive) && inE) {
+                        const double zv = (double)resE, rv = (double)b_at(st, cE);
+                        acc[0] += zv;
+                        acc[1] += rv * zv;
+                        acc[2] += rv;
+                    }
                 }
             }
         } else {
@@ -517,131 +583,6 @@ __global__ void __launch_bounds__(kThreads)
     if constexpr (UP && ZDOT) {
         double tot[3];
         if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
-    }
-}
-
-// CG search direction fused with the operator, as a column march (3D): step s forms
-// p = (z - m) + beta p_old of plane s once per cell (tile and 1-cell ring) into a
-// shared plane and keeps each thread's own two columns in registers, then computes
-// A p of plane s-1 on the tile from the shared plane s-1 (in-plane neighbours) and
-// the registers (planes s and s-2), so each p is formed once and one block barrier
-// per plane suffices.  Same expressions and the same per-thread accumulation order
-// of p.Ap as k_pmatvec (march.cuh): a solid or out-of-domain neighbour reads p_C
-// (Neumann) or -p_C at a Dirichlet wall (pcg_3d.cpp:38-55); the last block sets
-// alpha = rz_old / p.Ap or stops on breakdown (pcg_3d.cpp:94-99).
-template <class T>
-struct PmcCfg {
-    using P = MPlan<3, T, true, false, false>;  // slots: z (b slot), p_old (x slot), codes
-    static constexpr int S = 4;
-    using Lay = MLayout<T, S, P>;
-    static constexpr size_t XB = align128(PBox<T>::BYTES);
-    static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * XB;
-};
-
-template <class T>
-__global__ void __launch_bounds__(kThreads)
-    k_pmatvec_col(const __grid_constant__ MarchMaps M, Geom g, int zc, T* __restrict__ pnew,
-                  T* __restrict__ ap, Stencil st, double* partials, CGState* cg, int* err) {
-    pdl_entry();
-    if (cg->done) return;
-    using C = PmcCfg<T>;
-    using P = typename C::P;
-    using Lay = typename C::Lay;
-    constexpr int S = C::S, W = PBox<T>::W, WC = PBox<uint8_t>::W;
-    UAAMG_FUSED_SMEM(sm, err)
-    const int tid = threadIdx.x;
-    const Pair o = own_pair<T>(g);
-    const T m = (T)cg->mean_z, beta = (T)cg->beta;
-    const T idx2 = (T)st.idx2, idy2 = (T)st.idy2, idz2 = (T)st.idz2, diag = (T)st.diag;
-    const bool dw = st.dirichlet != 0;
-    // ring cells of the 1-cell ring (box columns 0 and 33, rows 0 and 17): two per
-    // thread for the first 50 threads
-    const bool ring = tid < 50;
-    int ra0 = 0, rr0 = 0, ra1 = 0, rr1 = 0;
-    if (tid < 17) { ra0 = 2 * tid; ra1 = ra0 + 1; rr0 = rr1 = 0; }
-    else if (tid < 34) { ra0 = 2 * (tid - 17); ra1 = ra0 + 1; rr0 = rr1 = kMY + 1; }
-    else if (tid < 42) { ra0 = ra1 = 0; rr0 = 1 + 2 * (tid - 34); rr1 = rr0 + 1; }
-    else if (tid < 50) { ra0 = ra1 = kMX + 1; rr0 = 1 + 2 * (tid - 42); rr1 = rr0 + 1; }
-    const int rq0 = rr0 * W + ra0, rq1 = rr1 * W + ra1;
-    const int rc0 = rr0 * WC + ra0, rc1 = rr1 * WC + ra1;
-    int kb, ke;
-    zrange<3>(g, zc, kb, ke);
-    MRing<3, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING, kb - 1, ke};
-    bool ok = true;
-    if (tid == 0) {
-        R.start(M);
-        ok = R.wait(R.p0);
-    }
-    if (!step_barrier(ok, err)) return;
-    T* xb = reinterpret_cast<T*>(sm + Lay::OFF_EXTRA);
-    auto pv = [&](const unsigned char* stg, int q, int qc) -> T {
-        return (stg[P::OFF_CODE + qc] & kActive)
-                   ? (boxv<T>(stg, P::QB * P::VB, q) - m) + beta * boxv<T>(stg, P::QX * P::VB, q)
-                   : T(0);
-    };
-    double acc[1] = {0.0};
-    T pA1 = T(0), pB1 = T(0), pA2 = T(0), pB2 = T(0);  // own columns at planes s-1, s-2
-    uint32_t cA1 = 0, cB1 = 0;                          // their codes at plane s-1
-    const unsigned char* stg = R.at(R.p0);                // stage of plane s, rotated
-    const unsigned char* ring_end = sm + Lay::OFF_RING + S * P::STAGE;
-#pragma unroll 1
-    for (int s = R.p0; s <= ke; ++s) {
-        T* xs = xb + (size_t)(s & 1) * (C::XB / sizeof(T));
-        const T* xo = xb + (size_t)((s + 1) & 1) * (C::XB / sizeof(T));
-        const uint32_t cA = stg[P::OFF_CODE + o.ca], cB = stg[P::OFF_CODE + o.ca + WC];
-        const T pA = pv(stg, o.qa, o.ca), pB = pv(stg, o.qa + W, o.ca + WC);
-        xs[o.qa] = pA;
-        xs[o.qa + W] = pB;
-        if (ring) {
-            xs[rq0] = pv(stg, rq0, rc0);
-            xs[rq1] = pv(stg, rq1, rc1);
-        }
-        if (s >= kb + 1) {  // A p of plane k = s - 1
-            const int k = s - 1;
-            const uint32_t cc[2] = {cA1, cB1};
-            const T p0s[2] = {pA1, pB1}, pup[2] = {pA, pB}, pdn[2] = {pA2, pB2};
-            T a_[2] = {T(0), T(0)};
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const uint32_t c = cc[e];
-                if (c & kActive) {
-                    const int q = o.qa + e * W, i = o.i, j = o.j + e;
-                    const T p0 = p0s[e];
-                    const T wall = dw ? -p0 : p0;
-                    const T vL = (c & 2u) ? xo[q - 1] : (i > 1 ? p0 : wall);
-                    const T vR = (c & 1u) ? xo[q + 1] : (i < g.nx ? p0 : wall);
-                    const T vB = (c & 8u) ? xo[q - W] : (j > 1 ? p0 : wall);
-                    const T vT = (c & 4u) ? xo[q + W] : (j < g.ny ? p0 : wall);
-                    const T vF = (c & 32u) ? pdn[e] : (k > 1 ? p0 : wall);
-                    const T vK = (c & 16u) ? pup[e] : (k < g.nz ? p0 : wall);
-                    a_[e] = sizeof(T) == 8
-                                ? diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2
-                                : ((p0 - vL) + (p0 - vR)) * idx2 + ((p0 - vB) + (p0 - vT)) * idy2 +
-                                      ((p0 - vF) + (p0 - vK)) * idz2;
-                    acc[0] += (double)p0 * (double)a_[e];
-                }
-            }
-            const int id = o.gid + k * g.sxy;
-            if (o.ina) { pnew[id] = pA1; ap[id] = a_[0]; }
-            if (o.inb) { pnew[id + g.sx] = pB1; ap[id + g.sx] = a_[1]; }
-        }
-        pA2 = pA1; pB2 = pB1;
-        pA1 = pA; pB1 = pB;
-        cA1 = cA; cB1 = cB;
-        stg += P::STAGE;
-        if (stg == ring_end) stg = sm + Lay::OFF_RING;
-        bool okk = true;
-        if (tid == 0 && s + 1 <= R.plast) okk = R.wait(s + 1);
-        if (!step_barrier(okk, err)) return;
-        if (tid == 0) R.refill(M, s);
-    }
-    double tot[1];
-    if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
-        const double pap = tot[0];
-        cg->pap = pap;
-        if (!(pap == pap)) { cg->status = CG_NAN; cg->done = 1; }
-        else if (pap < cg->breakdown) { cg->status = CG_BREAKDOWN; cg->done = 1; }
-        else cg->alpha = cg->rz_old / pap;
     }
 }
 
