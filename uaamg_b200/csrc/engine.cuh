@@ -990,11 +990,11 @@ private:
         // a finest level with Dirichlet walls takes the four-march path (the fused
         // finest level's branch-free cell table holds no wall terms)
         if (fused_ && nu == 1 && !(FINE && dirichlet_)) {
-            // b, code (coarse levels: diagonal, couplings) in; coarse code in, coarse b out
-            UAAMG_LAUNCH_SMEM((KTag{K_DOWN, l, c * (t + 1.0 + coef) + cc * (t + 1.0)}),
+            // b, code (coarse levels: diagonal, couplings) in; coarse b out
+            UAAMG_LAUNCH_SMEM((KTag{K_DOWN, l, c * (t + 1.0 + coef) + cc * t}),
                               (k_level_fused<DIM, T, FINE, CSL, false, false>), grid, blk,
                               (FCfg<DIM, T, CSL, FINE, false>::BYTES), fmaps(l, false), mlevel(l),
-                              Cl.code, Cl.b, done, err_, partials_, cg_);
+                              Cl.b, done, err_, partials_, cg_);
             return;
         }
         T* x = l == 0 ? z_ : L.x;
@@ -1035,12 +1035,12 @@ private:
             const KTag tag{K_UP, l, c * (2.0 * t + 1.0 + coef) + cc * t};
             if (FINE && zdot)
                 UAAMG_LAUNCH_SMEM(tag, (k_level_fused<DIM, T, FINE, CSL, true, true>), grid, blk,
-                                  (FCfg<DIM, T, CSL, FINE, true>::BYTES), fmaps(l, true), mlevel(l),
-                                  (const uint8_t*)nullptr, x, done, err_, partials_, cg_);
+                                  (FCfg<DIM, T, CSL, FINE, true>::BYTES), fmaps(l, true), mlevel(l), x,
+                                  done, err_, partials_, cg_);
             else
                 UAAMG_LAUNCH_SMEM(tag, (k_level_fused<DIM, T, FINE, CSL, true, false>), grid, blk,
-                                  (FCfg<DIM, T, CSL, FINE, true>::BYTES), fmaps(l, true), mlevel(l),
-                                  (const uint8_t*)nullptr, x, done, err_, partials_, cg_);
+                                  (FCfg<DIM, T, CSL, FINE, true>::BYTES), fmaps(l, true), mlevel(l), x,
+                                  done, err_, partials_, cg_);
             return;
         }
         UAAMG_LAUNCH_SMEM((KTag{K_UPE, l, c * (2.0 * t + 1.0 + coef) + cc * t}),

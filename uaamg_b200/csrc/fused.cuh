@@ -91,7 +91,7 @@ struct FCfg {
     // finest level in FP32: the per-code table of the branch-free cell updates
     static constexpr bool LEAN = FINE && sizeof(T) == 4;
     static constexpr size_t OFF_TAB = OFF_LUT + align128(64 * sizeof(T));
-    static constexpr size_t OFF_RING = OFF_TAB + (LEAN ? 128 * sizeof(float4) : 0);
+    static constexpr size_t OFF_RING = OFF_TAB + (LEAN ? 128 * sizeof(float2) : 0);
     static constexpr size_t OFF_X = OFF_RING + S * P::STAGE;
     static constexpr size_t XB = align128(RBox<T>::BYTES);
     static constexpr size_t BYTES = OFF_X + NXP * XB;
@@ -102,11 +102,13 @@ struct FCfg {
 };
 
 // A cell of a task: box positions in the T, code and coupling boxes, the parent
-// box position, its indices and its global offset in a level plane.
+// box position, its global offset in a level plane, whether it lies in the level,
+// and its colour on plane 0 ((i + j) & 1).
 struct FCell {
     int qt, qc, qs, qq;
-    int i, j;
     int gid;
+    bool in;
+    int par;
 };
 
 template <class T, class CS>
@@ -116,9 +118,10 @@ __device__ __forceinline__ FCell fcell(const Geom& g, int i0, int j0, int di, in
     c.qc = RBox<uint8_t>::pos(di, dj);
     c.qs = RBox<CS>::pos(di, dj);
     c.qq = ((dj + 2) >> 1) * QBox<T>::W + ((di + 2) >> 1);
-    c.i = i0 + di;
-    c.j = j0 + dj;
-    c.gid = c.i + c.j * g.sx;
+    const int i = i0 + di, j = j0 + dj;
+    c.gid = i + j * g.sx;
+    c.in = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny;
+    c.par = (i + j) & 1;
     return c;
 }
 
@@ -200,9 +203,8 @@ struct FHist {
 
 template <int DIM, class T, bool FINE, class CS, bool UP, bool ZDOT>
 __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
-    k_level_fused(const __grid_constant__ FMaps M, MLevel<T> L, const uint8_t* __restrict__ ccode,
-                  T* __restrict__ out, const int* __restrict__ done, int* err, double* partials,
-                  CGState* cg) {
+    k_level_fused(const __grid_constant__ FMaps M, MLevel<T> L, T* __restrict__ out,
+                  const int* __restrict__ done, int* err, double* partials, CGState* cg) {
     pdl_entry();
     if (done && *done) return;
     using C = FCfg<DIM, T, CS, FINE, UP>;
@@ -217,12 +219,11 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
     if (FINE) build_lut<DIM, T>(lut, L.idx2, L.idy2, L.idz2);
     // Finest level in FP32 (no Dirichlet walls: those problems take the four-march
     // level): every cell update is a multiply-add driven by the table entry of its
-    // code's low 7 bits (neighbour bits, interior-fluid bit):
-    //   x = 1/d (0 unless an interior fluid cell the smoother relaxes, d >= 1e-30),
-    //   y = 1 for a relaxed cell, z = 1 for an interior fluid cell the smoother skips,
-    //   w = 1 for any interior fluid cell.
+    // code's low 7 bits (neighbour bits, interior-fluid bit): x = 1/d for an interior
+    // fluid cell the smoother relaxes (d >= 1e-30), else 0; y = 1 for an interior
+    // fluid cell it skips (d < 1e-30), else 0.
     constexpr bool LEAN = C::LEAN;
-    const float4* tab = reinterpret_cast<const float4*>(sm + C::OFF_TAB);
+    const float2* tab = reinterpret_cast<const float2*>(sm + C::OFF_TAB);
     if constexpr (LEAN) {
         if (tid < 128) {
             const uint32_t c = (uint32_t)tid;
@@ -230,12 +231,10 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
                       ((c & 4u) ? (float)L.idy2 : 0.f) + ((c & 8u) ? (float)L.idy2 : 0.f);
             if (DIM == 3) d = d + ((c & 16u) ? (float)L.idz2 : 0.f) + ((c & 32u) ? (float)L.idz2 : 0.f);
             const bool act = (c & kActive) != 0, skip = act && d < 1e-30f;
-            float4 e;
+            float2 e;
             e.x = act && !skip ? mdiv<float, CS>(1.0f, d) : 0.f;
-            e.y = act && !skip ? 1.f : 0.f;
-            e.z = skip ? 1.f : 0.f;
-            e.w = act ? 1.f : 0.f;
-            reinterpret_cast<float4*>(sm + C::OFF_TAB)[tid] = e;
+            e.y = skip ? 1.f : 0.f;
+            reinterpret_cast<float2*>(sm + C::OFF_TAB)[tid] = e;
         }
     }
 
@@ -246,11 +245,10 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
     auto b_at = [&](const unsigned char* st, const FCell& c) -> T {
         return reinterpret_cast<const T*>(st + P::OFF_B)[c.qt];
     };
+    // (a finest level with Dirichlet walls never runs here: no wall diagonal)
     auto diag_of = [&](const unsigned char* st, const FCell& c, uint32_t code, int k) -> T {
         if constexpr (FINE) {
-            T d = lut[code & 63u];
-            if (L.dirichlet) d = d + wall_diag_at<DIM, T>(L, c.i, c.j, k);
-            return d;
+            return lut[code & 63u];
         } else {
             return reinterpret_cast<const T*>(st + P::OFF_DG)[c.qt];
         }
@@ -289,8 +287,9 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
     // the way up; 0 on cells that are not interior fluid
     auto oval = [&](const unsigned char* st, const FCell& c, int k) -> T {
         if constexpr (LEAN) {
-            const float4 t = tab[code_at(st, c) & 127u];
-            if constexpr (UP) return b_at(st, c) * t.x + t.w * prolong(st, c);
+            const uint32_t code = code_at(st, c);
+            const float2 t = tab[code & 127u];
+            if constexpr (UP) return b_at(st, c) * t.x + ((code & kActive) ? prolong(st, c) : T(0));
             else return b_at(st, c) * t.x;
         }
         const uint32_t code = code_at(st, c);
@@ -306,11 +305,11 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
     auto evalc = [&](const unsigned char* st, const unsigned char* stm, const T* xv, const FCell& c,
                      int k, T op, T om) -> T {
         if constexpr (LEAN) {
-            const float4 t = tab[code_at(st, c) & 127u];
+            const float2 t = tab[code_at(st, c) & 127u];
             const int q = c.qt;
             T nb = L.idx2 * (xv[q + 1] + xv[q - 1]) + L.idy2 * (xv[q + WT] + xv[q - WT]);
             if (DIM == 3) nb = nb + L.idz2 * (op + om);
-            if constexpr (UP) return (b_at(st, c) + nb) * t.x + t.z * prolong(st, c);
+            if constexpr (UP) return (b_at(st, c) + nb) * t.x + t.y * prolong(st, c);
             else return (b_at(st, c) + nb) * t.x;
         }
         const uint32_t code = code_at(st, c);
@@ -349,21 +348,23 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
     // odd and even cells there, vO / vE their x values, zp* / zm* their columns'
     // values at k+1 and k-1; aOdd: A is the odd cell.  rlo: the way down's dk = 0
     // residuals, kept from the odd plane below.
-    auto final_pair = [&](const unsigned char* st, const unsigned char* stm, const T* xv, int k,
-                          const FCell& cO, const FCell& cE, bool aOdd, T vO, T vE, T zpO, T zmO,
-                          T zpE, T zmE, T (&rlo)[2]) {
+    auto final_pair = [&](auto kodd, const unsigned char* st, const unsigned char* stm, const T* xv,
+                          int k, const FCell& cO, const FCell& cE, bool aOdd, T vO, T vE, T zpO,
+                          T zmO, T zpE, T zmE, T (&rlo)[2]) {
+        constexpr bool KODD = decltype(kodd)::value;  // plane k is odd (3D)
         const uint32_t kO = code_at(st, cO), kE = code_at(st, cE);
         T resO = UP ? vO : T(0), resE = UP ? vE : T(0);
         if constexpr (LEAN) {
-            const float4 tO = tab[kO & 127u], tE = tab[kE & 127u];
+            const float2 tO = tab[kO & 127u];
             const int q = cO.qt;
             T nb = L.idx2 * (xv[q + 1] + xv[q - 1]) + L.idy2 * (xv[q + WT] + xv[q - WT]);
             if (DIM == 3) nb = nb + L.idz2 * (zpO + zmO);
             if constexpr (UP) {
-                resO = (b_at(st, cO) + nb) * tO.x + tO.z * vO;  // a skipped cell keeps vO
+                resO = (b_at(st, cO) + nb) * tO.x + tO.y * vO;  // a skipped cell keeps vO
             } else {
-                resO = tO.y * nb + tO.z * b_at(st, cO);
-                resE = tE.z * b_at(st, cE);
+                const float2 tE = tab[kE & 127u];
+                resO = (tO.x != 0.f ? nb : T(0)) + tO.y * b_at(st, cO);
+                resE = tE.y * b_at(st, cE);
             }
         } else if (kO & kActive) {  // odd cell: reverse-sweep update / residual
             const T d = diag_of(st, cO, kO, k);
@@ -407,7 +408,7 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
         }
         if constexpr (UP) {
             const int base = k * g.sxy;
-            const bool inO = cO.i <= g.nx && cO.j <= g.ny, inE = cE.i <= g.nx && cE.j <= g.ny;
+            const bool inO = cO.in, inE = cE.in;
             if (inO) out[cO.gid + base] = resO;
             if (inE) out[cE.gid + base] = resE;
             if (ZDOT) {
@@ -441,7 +442,7 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
             const T res[2] = {aOdd ? resO : resE, aOdd ? resE : resO};  // [dj]
             // restriction: children dk = 0 on odd planes; the set is complete on the
             // even plane that follows (2D: one plane)
-            if (DIM == 3 && (k & 1)) {
+            if (DIM == 3 && KODD) {
                 rlo[0] = res[0];
                 rlo[1] = res[1];
             } else {
@@ -462,7 +463,8 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
                         sum += res[0]; sum += res[1];
                         sum += pr[0][1]; sum += pr[1][1];
                     }
-                    out[cid] = (ccode[cid] & kActive) ? sum : T(0);
+                    // also written on solid coarse cells, where no kernel reads b
+                    out[cid] = sum;
                 }
             }
         }
@@ -481,9 +483,9 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
         }
         if (!step_barrier(ok, err)) return;
         // A is odd when i + j is odd; ring pairs likewise
-        const bool oddA = ((cA.i + cA.j) & 1) != 0;
+        const bool oddA = cA.par != 0;
         const FCell tO = oddA ? cA : cB, tE = oddA ? cB : cA;
-        const bool odd1 = ((cR1.i + cR1.j) & 1) != 0;
+        const bool odd1 = cR1.par != 0;
         const FCell rO = odd1 ? cR1 : cR2, rE = odd1 ? cR2 : cR1;
         const T ot = oval(st, tO, 0);
         xpl[tO.qt] = ot;
@@ -493,7 +495,8 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
         xpl[tE.qt] = et;
         if (ring1) xpl[rE.qt] = evalc(st, st, xpl, rE, 0, T(0), T(0));
         __syncthreads();
-        final_pair(st, st, xpl, 0, tO, tE, oddA, ot, et, T(0), T(0), T(0), T(0), rlo);
+        final_pair(std::false_type(), st, st, xpl, 0, tO, tE, oddA, ot, et, T(0), T(0), T(0), T(0),
+                   rlo);
     } else {
         // steps s = kb-3 .. ke: odd values of planes kb-2 .. ke+1, even values of
         // kb-1 .. ke, final results of kb .. ke-1
@@ -507,9 +510,9 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
         }
         if (!step_barrier(ok, err)) return;
         // role 0 is the cell that is even on planes s0, s0+2, ... (odd on s0+1, ...)
-        const bool aRole0 = ((cA.i + cA.j + s0) & 1) == 0;
+        const bool aRole0 = ((cA.par + s0) & 1) == 0;
         const FCell t0 = aRole0 ? cA : cB, t1 = aRole0 ? cB : cA;
-        const bool r1Role0 = ((cR1.i + cR1.j + s0) & 1) == 0;
+        const bool r1Role0 = ((cR1.par + s0) & 1) == 0;
         const FCell q0 = r1Role0 ? cR1 : cR2, q1 = r1Role0 ? cR2 : cR1;
         FHist<T> ht[2] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
         T hr[2] = {T(0), T(0)};  // ring columns: last odd value
@@ -523,9 +526,13 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
         T* xn = xpl + (size_t)((s0 + 4) % 3) * (C::XB / sizeof(T));
         T* xc = xpl + (size_t)((s0 + 3) % 3) * (C::XB / sizeof(T));
         T* xo = xpl + (size_t)((s0 + 5) % 3) * (C::XB / sizeof(T));
-        // one step; R0: the role whose cell is even at plane s (compile-time)
-        auto step = [&](int s, auto R0c) -> bool {
-            constexpr int RC = decltype(R0c)::value, RO = 1 - RC;
+        // one step; R0c: the role whose cell is even at plane s; PHc: the phases it runs
+        // (2: odd and even values, 3: all three; 0: decided at run time from s) --
+        // compile-time
+        auto step = [&](int s, auto R0c, auto PHc) -> bool {
+            constexpr int RC = decltype(R0c)::value, RO = 1 - RC, PH = decltype(PHc)::value;
+            const bool run_even = PH == 0 ? s >= kb - 1 : PH >= 2;
+            const bool run_final = PH == 0 ? s >= kb + 1 : PH == 3;
             const FCell& tc = RC == 0 ? t0 : t1;
             const FCell& qc = RC == 0 ? q0 : q1;
             // 1. odd values of plane s+1
@@ -538,20 +545,21 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
             }
             // 2. even values of plane s
             T en = T(0);
-            if (s >= kb - 1) {
+            if (run_even) {
                 en = evalc(s00, sm1, xc, tc, s, on, ht[RC].o1);
                 xc[tc.qt] = en;
                 if (ring1) xc[qc.qt] = evalc(s00, sm1, xc, qc, s, onr, hr[RC]);
             }
-            // 3. final results of plane s-1: the role-RC cell is odd there
-            if (s >= kb + 1) {
+            // 3. final results of plane s-1: the role-RC cell is odd there (plane s-1 is
+            // odd for role 0: s0 = kb - 3 is even)
+            if (run_final) {
                 const int p = s - 1;
                 const T vR = ht[RC].o1, vO = ht[RO].e1;   // x at p
                 const T zpR = en, zmR = ht[RC].e1;         // role RC: even values at p+1, p-1
                 const T zpO = ht[RO].o1, zmO = ht[RO].o2;  // role RO: odd values at p+1, p-1
                 const FCell& to = RC == 0 ? t1 : t0;
-                final_pair(sm1, sm2, xo, p, tc, to, aRole0 == (RC == 0), vR, vO, zpR, zmR, zpO, zmO,
-                           rlo);
+                final_pair(std::integral_constant<bool, RC == 0>(), sm1, sm2, xo, p, tc, to,
+                           aRole0 == (RC == 0), vR, vO, zpR, zmR, zpO, zmO, rlo);
             }
             ht[RC].o2 = ht[RC].o1;
             ht[RC].o1 = on;
@@ -574,10 +582,29 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
             if (tid == 0) R.refill(M, s - C::LAG);
             return true;
         };
+        using R0 = std::integral_constant<int, 0>;
+        using R1 = std::integral_constant<int, 1>;
+        if constexpr (UP) {
+            // one loop, phases by s (fewer registers than two loops here)
 #pragma unroll 1
-        for (int s = s0; s <= ke; s += 2) {
-            if (!step(s, std::integral_constant<int, 0>())) return;
-            if (s + 1 <= ke && !step(s + 1, std::integral_constant<int, 1>())) return;
+            for (int s = s0; s <= ke; s += 2) {
+                if (!step(s, R0(), std::integral_constant<int, 0>())) return;
+                if (s + 1 <= ke && !step(s + 1, R1(), std::integral_constant<int, 0>())) return;
+            }
+        } else {
+            // steps kb-3 .. kb fill the pipeline: odd and even values only (the even
+            // values of planes kb-3, kb-2 are not needed; their shared positions are
+            // written again before any read); then ke >= kb + 1 steps run all three
+#pragma unroll 1
+            for (int s = s0; s <= kb; s += 2) {
+                if (!step(s, R0(), std::integral_constant<int, 2>())) return;
+                if (!step(s + 1, R1(), std::integral_constant<int, 2>())) return;
+            }
+#pragma unroll 1
+            for (int s = kb + 1; s <= ke; s += 2) {
+                if (!step(s, R0(), std::integral_constant<int, 3>())) return;
+                if (s + 1 <= ke && !step(s + 1, R1(), std::integral_constant<int, 3>())) return;
+            }
         }
     }
     if constexpr (UP && ZDOT) {
