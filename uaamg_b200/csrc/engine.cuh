@@ -624,7 +624,8 @@ private:
             if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return E_CUDA;
         // dynamic shared memory of the marches
         if ((e = march_attrs<DIM, true, CS>()) || (e = march_attrs<DIM, false, CS>()) ||
-            (e = smem_attr(k_pmatvec<DIM, T>, PmvCfg<DIM, T>::BYTES)) ||
+            (e = smem_attr(k_pmatvec<DIM, T, true>, PmvCfg<DIM, T>::BYTES)) ||
+            (e = smem_attr(k_pmatvec<DIM, T, false>, PmvCfg<DIM, T>::BYTES)) ||
             (e = fused_attrs<DIM, true, CS>()) || (e = fused_attrs<DIM, false, CS>()))
             return e;
         if constexpr (kHalf) {  // levels with FP32 couplings
@@ -1172,10 +1173,15 @@ private:
             MarchMaps pm = maps<DIM>(0, true, false);  // z and the current search direction
             pm.v[0] = lv_[0].mx;
             pm.v[1] = from_p ? map_p_ : map_p2_;
-            UAAMG_LAUNCH_SMEM((KTag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)}),
-                              (k_pmatvec<DIM, T>), march_grid<DIM>(g, lv_[0].zc), dim3(kThreads),
-                              (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st, partials_, cg_,
-                              err_);
+            const KTag tag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)};
+            if (dirichlet_)
+                UAAMG_LAUNCH_SMEM(tag, (k_pmatvec<DIM, T, true>), march_grid<DIM>(g, lv_[0].zc),
+                                  dim3(kThreads), (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st,
+                                  partials_, cg_, err_);
+            else
+                UAAMG_LAUNCH_SMEM(tag, (k_pmatvec<DIM, T, false>), march_grid<DIM>(g, lv_[0].zc),
+                                  dim3(kThreads), (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st,
+                                  partials_, cg_, err_);
         }
         const long long nvec = (long long)g.n / Vec16<T>::N;
         // x_lo, r, p, Ap in; x_lo, r out (a fold after a replacement adds x_hi in and out)

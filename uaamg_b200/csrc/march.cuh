@@ -834,8 +834,10 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
 // the fly from the staged z and p_old (a solid or out-of-domain neighbour reads
 // p_C -- Neumann -- or -p_C at a Dirichlet wall; pcg_3d.cpp:38-55); p.Ap is
 // reduced and the last block sets alpha = rz_old / p.Ap or stops on breakdown
-// (pcg_3d.cpp:94-99).  p_old and p_new are distinct buffers.
-template <int DIM, class T>
+// (pcg_3d.cpp:94-99).  p_old and p_new are distinct buffers.  DIRW: the problem has
+// Dirichlet walls (with Neumann walls a missing neighbour always reads p_C, so the
+// wall tests drop out; the selected values are the same).
+template <int DIM, class T, bool DIRW = true>
 __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ MarchMaps M, Geom g,
                                                       int zc, T* __restrict__ pnew,
                                                       T* __restrict__ ap, Stencil st,
@@ -878,15 +880,15 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
             if (c & kActive) {
                 const int q = o.qa + e * W, i = o.i, j = o.j + e;
                 const T p0 = pc[e];
-                const T wall = st.dirichlet ? -p0 : p0;
-                const T vL = (c & 2u) ? pv(sg.c, q - 1) : (i > 1 ? p0 : wall);
-                const T vR = (c & 1u) ? pv(sg.c, q + 1) : (i < g.nx ? p0 : wall);
+                const T wall = DIRW && st.dirichlet ? -p0 : p0;
+                const T vL = (c & 2u) ? pv(sg.c, q - 1) : (!DIRW || i > 1 ? p0 : wall);
+                const T vR = (c & 1u) ? pv(sg.c, q + 1) : (!DIRW || i < g.nx ? p0 : wall);
                 // the pair's other cell is the +y (A) or -y (B) neighbour
-                const T vB = (c & 8u) ? (e ? pc[0] : pv(sg.c, q - W)) : (j > 1 ? p0 : wall);
-                const T vT = (c & 4u) ? (e ? pv(sg.c, q + W) : pc[1]) : (j < g.ny ? p0 : wall);
+                const T vB = (c & 8u) ? (e ? pc[0] : pv(sg.c, q - W)) : (!DIRW || j > 1 ? p0 : wall);
+                const T vT = (c & 4u) ? (e ? pv(sg.c, q + W) : pc[1]) : (!DIRW || j < g.ny ? p0 : wall);
                 if (DIM == 3) {
-                    const T vF = (c & 32u) ? pv(sg.m, q) : (k > 1 ? p0 : wall);
-                    const T vK = (c & 16u) ? pv(sg.n, q) : (k < g.nz ? p0 : wall);
+                    const T vF = (c & 32u) ? pv(sg.m, q) : (!DIRW || k > 1 ? p0 : wall);
+                    const T vK = (c & 16u) ? pv(sg.n, q) : (!DIRW || k < g.nz ? p0 : wall);
                     a_[e] = sizeof(T) == 8
                                 ? diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2
                                 : ((p0 - vL) + (p0 - vR)) * idx2 + ((p0 - vB) + (p0 - vT)) * idy2 +
