@@ -719,16 +719,46 @@ def run_batch(args):
     return 0
 
 
-def _serve_pass(srv, reqs, make, rate=None, max_outstanding=256, check=()):
+class _PinnedPool:
+    """Page-locked float64 arrays by shape, reused across requests (the serving
+    requests lend their right-hand sides and outputs to the server)."""
+
+    def __init__(self):
+        import threading
+        self.free, self.lock, self.keep = {}, threading.Lock(), {}
+
+    def get(self, shape):
+        import torch
+        with self.lock:
+            lst = self.free.get(shape)
+            if lst:
+                return lst.pop()
+        t = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+        a = t.numpy()
+        with self.lock:
+            self.keep[a.ctypes.data] = t  # the tensor owns the pinned memory
+        return a
+
+    def put(self, a):
+        if a is None:
+            return
+        with self.lock:
+            self.free.setdefault(a.shape, []).append(a)
+
+
+def _serve_pass(srv, reqs, make, rate=None, max_outstanding=64, check=(), pool=None):
     """Submits reqs [(sim_id, step)] to the server: as fast as the producers build
     them (closed loop, at most max_outstanding in the server), or at Poisson
-    arrivals of `rate` per second (open loop).  Returns (results, wall seconds,
-    {index: (p, solid, rhs, h)} for the indices in `check`)."""
+    arrivals of `rate` per second (open loop).  Each request's right-hand side is
+    built into a pinned buffer lent to the server (UAAMG_REQUEST_BORROW), so no host
+    copy of it is made.  Returns (results, wall seconds, {index: (p, solid, rhs, h)}
+    for the indices in `check`)."""
     import queue
     import threading
 
     import numpy as np
 
+    pool = pool or _PinnedPool()
     n = len(reqs)
     arrivals = None
     if rate:
@@ -747,14 +777,19 @@ def _serve_pass(srv, reqs, make, rate=None, max_outstanding=256, check=()):
                 return
             i, t_arr = item
             sid, step = reqs[i]
-            solid, rhs, h = make(sid, step)
-            p = np.zeros_like(rhs) if i in check else None
+            solid, h, fill = make(sid, step)
+            rhs = pool.get(solid.shape)
+            fill(rhs)
+            p = pool.get(solid.shape) if i in check else None
+            if p is not None:
+                p[...] = 0.0
             t_sub = time.perf_counter()
-            tk = srv.submit(sid, solid, rhs, h, h, h if solid.ndim == 3 else 1.0, p_out=p)
+            tk = srv.submit(sid, solid, rhs, h, h, h if solid.ndim == 3 else 1.0, p_out=p,
+                            borrow=True)
             with lock:
-                outstanding[tk] = (i, t_arr, t_sub)
+                outstanding[tk] = (i, t_arr, t_sub, rhs, p)
                 if p is not None:
-                    kept[i] = (p, solid, rhs, h)
+                    kept[i] = (p, solid, rhs.copy(), h)
 
     def poller():
         while True:
@@ -762,7 +797,7 @@ def _serve_pass(srv, reqs, make, rate=None, max_outstanding=256, check=()):
                 items = list(outstanding.items())
             if not items and done_submitting.is_set():
                 return
-            for tk, (i, t_arr, t_sub) in items:
+            for tk, (i, t_arr, t_sub, rhs, p) in items:
                 r = srv.poll(tk)
                 if r is None:
                     continue
@@ -771,6 +806,10 @@ def _serve_pass(srv, reqs, make, rate=None, max_outstanding=256, check=()):
                 results[i] = r
                 with lock:
                     del outstanding[tk]
+                pool.put(rhs)
+                if p is not None:
+                    kept[i] = (p.copy(), kept[i][1], kept[i][2], kept[i][3])
+                    pool.put(p)
                 slots.release()
             time.sleep(0.0002)
 
@@ -819,8 +858,13 @@ def serve_forms(args, device, rank, ws, n_ids, steps, precs):
         fields = dict(zip(mine, ex.map(lambda sid: workloads.serve_fields(*plan[sid][1:4]), mine)))
 
     def make(sid, t):
+        """(solid, h, fill): fill(out) writes step t's right-hand side r0 + (t/steps) r1."""
         solid, r0, r1 = fields[sid]
-        return solid, r0 + (t / steps) * r1, 1.0 / plan[sid][2]
+
+        def fill(out):
+            np.multiply(r1, t / steps, out=out)
+            out += r0
+        return solid, 1.0 / plan[sid][2], fill
 
     reqs = [(sid, t) for t in range(steps) for sid in mine]
     rng = np.random.Generator(np.random.MT19937(7 + rank))
@@ -838,20 +882,22 @@ def serve_forms(args, device, rank, ws, n_ids, steps, precs):
                 "all_ok": all(r["status"] == 0 for r in res)}
 
     out = {}
+    pool = _PinnedPool()
     for prec in precs:
         srv = Server(device, prec, 1e-6, 500, max_active=args.serve_active)
         # warm-up: every id's hierarchy and graph, not timed
-        _serve_pass(srv, [(sid, 0) for sid in mine], make)
-        closed, wall_c, kept_c = _serve_pass(srv, reqs, make, check=check)
+        _serve_pass(srv, [(sid, 0) for sid in mine], make, pool=pool)
+        closed, wall_c, kept_c = _serve_pass(srv, reqs, make, check=check, pool=pool)
         cap = len(reqs) / wall_c  # this rank's capacity
         entry = {"closed_loop": summary(shard.gather(closed), shard.reduce_sum(cap))}
         kept = kept_c
         if prec == precs[0]:
             srv.stop()
             srv = Server(device, prec, 1e-6, 500, max_active=args.serve_active)
-            _serve_pass(srv, [(sid, 0) for sid in mine], make)
+            _serve_pass(srv, [(sid, 0) for sid in mine], make, pool=pool)
             with ClockSampler(device) as clk:
-                opened, wall_o, kept = _serve_pass(srv, reqs, make, rate=0.8 * cap, check=check)
+                opened, wall_o, kept = _serve_pass(srv, reqs, make, rate=0.8 * cap, check=check,
+                                                   pool=pool)
             entry["open_loop"] = summary(shard.gather(opened), shard.reduce_sum(len(reqs) / wall_o))
             entry["open_loop"]["arrival_rate_per_s"] = round(shard.reduce_sum(0.8 * cap), 1)
             entry["clocks"] = clk.summary()

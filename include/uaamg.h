@@ -337,10 +337,18 @@ typedef struct uaamg_request {
     int dim, nx, ny, nz;
     double dx, dy, dz;
     const uint8_t* solid;     /* host, copied by submit */
-    const double* rhs;        /* host, copied by submit */
+    const double* rhs;        /* host, copied by submit (see flags) */
     double* p_out;            /* host, may be NULL: receives the padded pressure (reference
                                  layout) when the solve finishes; must stay valid until then */
+    int flags;                /* UAAMG_REQUEST_* bits, 0 by default */
 } uaamg_request;
+
+/* uaamg_request.flags: rhs (and p_out, when given) are lent to the server instead of
+ * copied -- the right-hand side is copied to the device straight from rhs and the
+ * pressure straight into p_out; the caller keeps both valid, and rhs unmodified, until
+ * the ticket is polled done.  Page-locked (pinned) buffers make both copies
+ * asynchronous; no host copy of either array is made. */
+#define UAAMG_REQUEST_BORROW 1
 
 typedef struct uaamg_result {
     long long ticket;

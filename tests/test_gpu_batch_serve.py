@@ -226,3 +226,35 @@ def test_batch_group_graph_matches_per_problem_graphs(prec):
     for a, b in zip(out[0][0], out[40000][0]):
         assert np.array_equal(a, b)
     hd.close()
+
+
+def test_borrowed_request_buffers_match_copies():
+    """UAAMG_REQUEST_BORROW: a request that lends its right-hand side and output
+    (no host copies; pinned here, so the device copies are asynchronous) gives the
+    same pressure, bit for bit, as the copying submit."""
+    import torch
+    sims = _sims()
+    out = {}
+    for borrow in (False, True):
+        srv = Server(0, "mixed", 1e-6, 500, max_active=4)
+        tickets = []
+        for sid, dx, dy, dz, gen in sims:
+            s, r = gen(0)
+            if borrow:
+                rb = torch.empty(r.shape, dtype=torch.float64, pin_memory=True)
+                pb = torch.zeros(r.shape, dtype=torch.float64, pin_memory=True)
+                rb.numpy()[...] = r
+                tk = srv.submit(sid, s, rb.numpy(), dx, dy, dz, p_out=pb.numpy(), borrow=True)
+                tickets.append((tk, sid, pb, rb))
+            else:
+                p = np.zeros_like(r)
+                tk = srv.submit(sid, s, r, dx, dy, dz, p_out=p)
+                tickets.append((tk, sid, p, None))
+        srv.drain()
+        for tk, sid, p, _ in tickets:
+            res = srv.poll(tk)
+            assert res is not None and res["status"] == 0, res
+            out[(borrow, sid)] = np.array(p.numpy() if borrow else p)
+        srv.stop()
+    for sid, *_ in sims:
+        assert np.array_equal(out[(False, sid)], out[(True, sid)]), sid

@@ -106,7 +106,11 @@ class Request(C.Structure):
         ("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
         ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
         ("solid", C.c_void_p), ("rhs", C.c_void_p), ("p_out", C.c_void_p),
+        ("flags", C.c_int),
     ]
+
+
+REQUEST_BORROW = 1
 
 
 class Result(C.Structure):

@@ -475,6 +475,8 @@ struct Ticket {
     SimState* sim = nullptr;
     bool ending = false;     // exit work queued; waiting for the slot's event
     int status = UAAMG_OK;   // result status once collected (the pressure copy may follow)
+    const double* rhs_ptr = nullptr;  // the right-hand side: rhs.data(), or the caller's
+    bool borrow = false;              // UAAMG_REQUEST_BORROW: rhs and p_out are the caller's
 };
 
 // Pinned host staging of one concurrent solve, and the event recorded behind its
@@ -640,8 +642,12 @@ bool start_request(uaamg_server* s, Ticket* t) {
     t->sim = sim;
     sim->busy = true;
     DevProblem& d = sim->dp;
-    std::memcpy(b.h, t->rhs.data(), d.n * sizeof(double));
-    cudaMemcpyAsync(d.d_rhs, b.h, d.n * sizeof(double), cudaMemcpyHostToDevice, d.stream);
+    if (t->borrow) {  // straight from the caller's buffer
+        cudaMemcpyAsync(d.d_rhs, t->rhs_ptr, d.n * sizeof(double), cudaMemcpyHostToDevice, d.stream);
+    } else {
+        std::memcpy(b.h, t->rhs_ptr, d.n * sizeof(double));
+        cudaMemcpyAsync(d.d_rhs, b.h, d.n * sizeof(double), cudaMemcpyHostToDevice, d.stream);
+    }
     if (!warm) cudaMemsetAsync(d.d_p, 0, d.n * sizeof(double), d.stream);
     uaamg_options o;
     uaamg_default_options(&o);
@@ -679,7 +685,8 @@ bool advance(uaamg_server* s, Ticket* t) {
         if (e == E_OK) e = d.eng->solve_end_enqueue();
         cudaError_t ce = cudaSuccess;
         if (e == E_OK && t->req.p_out)
-            ce = cudaMemcpyAsync(b.h, d.d_p, d.n * sizeof(double), cudaMemcpyDeviceToHost, d.stream);
+            ce = cudaMemcpyAsync(t->borrow ? t->req.p_out : b.h, d.d_p, d.n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, d.stream);
         if (e == E_OK && ce == cudaSuccess) ce = cudaEventRecord(b.ev, d.stream);
         if (e != E_OK || ce != cudaSuccess) {
             t->sim->has_p = false;
@@ -704,7 +711,7 @@ bool advance(uaamg_server* s, Ticket* t) {
     t->res.iterations = st.iterations;
     t->res.rel_residual = st.rel_residual;
     t->sim->has_p = true;
-    if (!t->req.p_out) {
+    if (!t->req.p_out || t->borrow) {  // nothing to copy on the host
         finish(s, t, t->status);
         return true;
     }
@@ -850,7 +857,13 @@ uaamg_status uaamg_server_submit(uaamg_server* s, const uaamg_request* q, long l
     t->req = *q;
     if (q->dim == 2) { t->req.nz = 0; t->req.dz = 1.0; }
     t->solid.assign(q->solid, q->solid + n);
-    t->rhs.assign(q->rhs, q->rhs + n);
+    t->borrow = (q->flags & UAAMG_REQUEST_BORROW) != 0;
+    if (t->borrow) {
+        t->rhs_ptr = q->rhs;
+    } else {
+        t->rhs.assign(q->rhs, q->rhs + n);
+        t->rhs_ptr = t->rhs.data();
+    }
     t->req.solid = nullptr;
     t->req.rhs = nullptr;
     t->t_submit = uaamg::Clock::now();

@@ -390,8 +390,11 @@ class Server:
             raise _capi.UaamgError(st, "server_start")
         self._keep = {}
 
-    def submit(self, sim_id, solid, rhs, dx, dy, dz=1.0, p_out=None) -> int:
-        """Queues one solve; p_out (padded float64, optional) receives the pressure."""
+    def submit(self, sim_id, solid, rhs, dx, dy, dz=1.0, p_out=None, borrow=False) -> int:
+        """Queues one solve; p_out (padded float64, optional) receives the pressure.
+        borrow: rhs and p_out are lent to the server (UAAMG_REQUEST_BORROW) -- keep them
+        alive and rhs unchanged until the ticket is polled done; pinned arrays make the
+        device copies asynchronous."""
         solid = np.ascontiguousarray(solid, dtype=np.uint8)
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         q = _capi.Request()
@@ -406,11 +409,13 @@ class Server:
             if p_out.dtype != np.float64 or not p_out.flags.c_contiguous or p_out.shape != solid.shape:
                 raise ValueError("p_out must be a C-contiguous float64 array of the padded shape")
             q.p_out = p_out.ctypes.data
+        q.flags = _capi.REQUEST_BORROW if borrow else 0
         t = C.c_longlong()
         st = self.lib.uaamg_server_submit(self.s, C.byref(q), C.byref(t))
         if st != _capi.OK:
             raise _capi.UaamgError(st, "server_submit")
-        self._keep[t.value] = p_out  # the output buffer must outlive the solve
+        # the output buffer (and a lent right-hand side) must outlive the solve
+        self._keep[t.value] = (p_out, rhs if borrow else None)
         return t.value
 
     def poll(self, ticket):
