@@ -84,7 +84,7 @@ struct KTag {
         const KTag tg_ = (tag);                                           \
         cudaEvent_t e0_ = nullptr, e1_ = nullptr;                         \
         if (prof_on_) prof_begin(tg_, &e0_, &e1_);                        \
-        if (pdl_ && !prof_on_ && st_ != nullptr) {                        \
+        if (pdl_ && !nopdl_next_ && !prof_on_ && st_ != nullptr) {        \
             cudaLaunchConfig_t cf_ = {};                                  \
             cudaLaunchAttribute at_[1];                                   \
             at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization; \
@@ -100,6 +100,7 @@ struct KTag {
             kern<<<(grid), (block), (smem), st_>>>(__VA_ARGS__);          \
         }                                                                 \
         if (prof_on_) cudaEventRecord(e1_, st_);                          \
+        nopdl_next_ = false;                                              \
         ++launches_;                                                      \
     } while (0)
 #define UAAMG_LAUNCH(tag, kern, grid, block, ...) \
@@ -384,6 +385,8 @@ private:
     bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
     bool fused_ = true;      // two fused marches a level (fused.cuh) instead of four
     bool pdl_ = true;        // programmatic dependent launch between the kernels
+    bool nopdl_next_ = false;  // the next launch is plain (a kernel that usually exits at
+                               // once: its blocks should not wait resident for their turn)
     int nu_fine_ = 1, nu_coarse_ = 1;  // pre- and post-smoothing sweeps: finest / coarse levels
     int tail_lt_ = 0;        // first level of the small-level kernel
     int tail_nc_ = 0;        // 1: the hierarchy has a tail (0: it does not fit the kernel)
@@ -1189,7 +1192,9 @@ private:
                      max_reduce_blocks(), 256, nvec, xlo_, r_, pnew, ap_, mixed_ ? xd_ : nullptr,
                      partials_, cg_, cur_.hist);
         if (mixed_) {
-            // residual replacement (when due): b, x_hi, x_lo, codes in; r out
+            // residual replacement (when due, one iteration in replace_every; the others
+            // return at once): b, x_hi, x_lo, codes in; r out
+            nopdl_next_ = true;
             UAAMG_LAUNCH((KTag{K_REPLACE, 0, cells(g) * (17.0 + 2.0 * sizeof(T))}),
                          (k_resid_x64<DIM, T>), resid_grid(g), dim3(32, 8), g, lv_[0].code, b64_, xd_,
                          xlo_, r_, st, kResidZc, partials_, cg_, 5, 1, cur_.tol, cur_.tol_mode);
