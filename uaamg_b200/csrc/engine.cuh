@@ -53,7 +53,14 @@ struct LevelBuf {
     // boxes with a 2-cell ring for the fused marches (fused.cuh): b, codes, diagonal,
     // couplings
     CUtensorMap fb, fcode, fdg, fcx, fcy, fcz;
+    // small 3D levels: whole-tile boxes (fused.cuh k_level_box) and this level's x as
+    // their parent box
+    bool box = false;
+    CUtensorMap bb, bcode, bdg, bcx, bcy, bcz, bxq;
 };
+
+// 3D levels of at most this many cells run the fused steps as whole-tile boxes
+constexpr double kBoxCells = 64.0 * 64.0 * 64.0;
 
 // Kernel classes for the in-situ per-kernel timing (uaamg_profile_solve).
 enum KClass : int {
@@ -513,6 +520,12 @@ private:
                     DIM == 3 ? (unsigned)((g.nz + zc - 1) / zc) : 1u);
     }
 
+    // Blocks of the whole-tile box kernels over level g: 8^3 tiles.
+    static dim3 box_grid(const Geom& g) {
+        return dim3((unsigned)((g.nx + kBT - 1) / kBT), (unsigned)((g.ny + kBT - 1) / kBT),
+                    (unsigned)((g.nz + kBT - 1) / kBT));
+    }
+
     // Largest even chunk <= 16 planes that still gives every SM several blocks.
     int pick_zc(const Geom& g) const {
         const long long tiles = (long long)((g.nx + kMX - 1) / kMX) * ((g.ny + kMY - 1) / kMY);
@@ -537,6 +550,16 @@ private:
             (e = smem_attr(k_up_even<DIM, T, FINE, CSL>, UpeCfg<DIM, T, FINE, CSL>::BYTES)) ||
             (e = smem_attr(k_up_odd<DIM, T, FINE, false, CSL>, UpoCfg<DIM, T, FINE, CSL>::BYTES)) ||
             (e = smem_attr(k_up_odd<DIM, T, FINE, true, CSL>, UpoCfg<DIM, T, FINE, CSL>::BYTES)))
+            return e;
+        return E_OK;
+    }
+
+    template <bool FINE, class CSL>
+    int box_attrs() {
+        int e;
+        if ((e = smem_attr(k_level_box<T, FINE, CSL, false, false>, BPlan<T, CSL, FINE, false>::BYTES)) ||
+            (e = smem_attr(k_level_box<T, FINE, CSL, true, false>, BPlan<T, CSL, FINE, true>::BYTES)) ||
+            (e = smem_attr(k_level_box<T, FINE, CSL, true, true>, BPlan<T, CSL, FINE, true>::BYTES)))
             return e;
         return E_OK;
     }
@@ -582,6 +605,7 @@ private:
             L.zc = DIM == 3 ? pick_zc(L.g) : 2;
             // largest face count of a level-l coupling: 4^l (3D), 2^l (2D)
             L.c32 = kHalf && l > 0 && (DIM == 3 ? 2 * l : l) > 11;
+            L.box = DIM == 3 && cells(L.g) <= kBoxCells;
             const size_t n = (size_t)L.g.n;
             if ((e = alloc(L.solid, n))) return e;
             if ((e = alloc(L.code, n))) return e;
@@ -616,6 +640,8 @@ private:
             reduce_blocks_ = (long long)mg.x * mg.y * mg.z;
             const dim3 rg = resid_grid(g0);
             reduce_blocks_ = std::max(reduce_blocks_, (long long)rg.x * rg.y * rg.z);
+            const dim3 bg = box_grid(g0);  // a small finest level runs as boxes
+            if (lv_[0].box) reduce_blocks_ = std::max(reduce_blocks_, (long long)bg.x * bg.y * bg.z);
             if (reduce_blocks_ < max_reduce_blocks()) reduce_blocks_ = max_reduce_blocks();
         }
         if ((e = alloc(partials_, (size_t)reduce_blocks_ * 4))) return e;
@@ -633,6 +659,12 @@ private:
             return e;
         if constexpr (kHalf) {  // levels with FP32 couplings
             if ((e = march_attrs<DIM, false, T>()) || (e = fused_attrs<DIM, false, T>())) return e;
+        }
+        if (DIM == 3) {
+            if ((e = box_attrs<true, CS>()) || (e = box_attrs<false, CS>())) return e;
+            if constexpr (kHalf) {
+                if ((e = box_attrs<false, T>())) return e;
+            }
         }
         // plane-box tensor maps
         constexpr int BW = PBox<T>::W, BH = PBox<T>::H;
@@ -669,6 +701,28 @@ private:
                 ok = encode_level_map<T>(&L.fb, b, L.g, DIM, RBox<T>::W, RBox<T>::H, 1) &&
                      encode_level_map<uint8_t>(&L.fcode, L.code, L.g, DIM, RBox<uint8_t>::W,
                                                RBox<uint8_t>::H, 1);
+            if (ok && DIM == 3) {
+                // whole-tile boxes (small levels) and this level's x as the parent box of
+                // the next-finer level's box kernels
+                if (l > 0)
+                    ok = encode_level_map<T>(&L.bxq, L.x, L.g, DIM, BQBox<T>::W, 6, 6);
+                if (ok && L.box) {
+                    ok = encode_level_map<T>(&L.bb, b, L.g, DIM, BBox<T>::W, kBB, kBB) &&
+                         encode_level_map<uint8_t>(&L.bcode, L.code, L.g, DIM, BBox<uint8_t>::W, kBB,
+                                                   kBB);
+                    if (ok && l > 0) {
+                        ok = encode_level_map<T>(&L.bdg, L.dg, L.g, DIM, BBox<T>::W, kBB, kBB);
+                        if (ok && !L.c32)
+                            ok = encode_level_map<CS>(&L.bcx, L.hcx, L.g, DIM, BBox<CS>::W, kBB, kBB) &&
+                                 encode_level_map<CS>(&L.bcy, L.hcy, L.g, DIM, BBox<CS>::W, kBB, kBB) &&
+                                 encode_level_map<CS>(&L.bcz, L.hcz, L.g, DIM, BBox<CS>::W, kBB, kBB);
+                        if (ok && L.c32)
+                            ok = encode_level_map<T>(&L.bcx, L.cx, L.g, DIM, BBox<T>::W, kBB, kBB) &&
+                                 encode_level_map<T>(&L.bcy, L.cy, L.g, DIM, BBox<T>::W, kBB, kBB) &&
+                                 encode_level_map<T>(&L.bcz, L.cz, L.g, DIM, BBox<T>::W, kBB, kBB);
+                    }
+                }
+            }
             if (!ok) return E_CUDA;
         }
         if (!encode_level_map<T>(&map_p_, p_, g0, DIM, BW, BH, 1) ||
@@ -810,6 +864,7 @@ private:
         for (int l = 0; l + 1 < (int)lv_.size() && e == E_OK; ++l) {
             if (use_tail() && l >= tail_lt_) break;  // the small-level kernel runs those levels
             LevelBuf<T, CS>& L = lv_[l];
+            if (L.box && fused_ && level_nu(l) == 1) continue;  // whole-tile boxes: no chunks
             const std::string key = "zc|" + tune_gpu_id() + "|" + (sizeof(T) == 8 ? "f64" : mixed_ ? "mixed" : "f32") +
                                     "|" + std::to_string(L.g.nx) + "x" + std::to_string(L.g.ny) + "x" +
                                     std::to_string(L.g.nz) + "|" + (l == 0 ? "fine" : "coarse") + "|" +
@@ -971,6 +1026,23 @@ private:
         return m;
     }
 
+    // Tensor maps of a whole-tile box kernel over level l; up: with the next-coarser
+    // level's x as parent boxes.
+    BMaps bmaps(int l, bool up) const {
+        const LevelBuf<T, CS>& L = lv_[l];
+        BMaps m{};
+        m.b = L.bb;
+        m.code = L.bcode;
+        if (l > 0) {
+            m.dg = L.bdg;
+            m.cx = L.bcx;
+            m.cy = L.bcy;
+            m.cz = L.bcz;
+        }
+        if (up) m.xc = lv_[l + 1].bxq;
+        return m;
+    }
+
     // The way down through level l: b (and on coarse levels the couplings) in,
     // coarse b out.  CSL: the coupling storage of this level.
     template <int DIM, bool FINE>
@@ -993,6 +1065,14 @@ private:
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         // a finest level with Dirichlet walls takes the four-march path (the fused
         // finest level's branch-free cell table holds no wall terms)
+        if (DIM == 3 && L.box && fused_ && nu == 1 && !(FINE && dirichlet_)) {
+            // whole-tile boxes: b, code (coarse levels: diagonal, couplings) in; coarse b out
+            UAAMG_LAUNCH_SMEM((KTag{K_DOWN, l, c * (t + 1.0 + coef) + cc * t}),
+                              (k_level_box<T, FINE, CSL, false, false>), box_grid(L.g), blk,
+                              (BPlan<T, CSL, FINE, false>::BYTES), bmaps(l, false), mlevel(l), Cl.b,
+                              done, err_, partials_, cg_);
+            return;
+        }
         if (fused_ && nu == 1 && !(FINE && dirichlet_)) {
             // b, code (coarse levels: diagonal, couplings) in; coarse b out
             UAAMG_LAUNCH_SMEM((KTag{K_DOWN, l, c * (t + 1.0 + coef) + cc * t}),
@@ -1034,6 +1114,20 @@ private:
         const double coef = FINE ? 0.0 : DIM * (double)sizeof(CSL) + t;  // couplings + diagonal
         const dim3 grid = march_grid<DIM>(L.g, L.zc), blk(kThreads);
         T* x = l == 0 ? z_ : L.x;
+        if (DIM == 3 && L.box && fused_ && nu == 1 && !(FINE && dirichlet_)) {
+            // whole-tile boxes: b, code (coarse levels: diagonal, couplings), coarse x in;
+            // x out
+            const KTag tag{K_UP, l, c * (2.0 * t + 1.0 + coef) + cc * t};
+            if (FINE && zdot)
+                UAAMG_LAUNCH_SMEM(tag, (k_level_box<T, FINE, CSL, true, true>), box_grid(L.g), blk,
+                                  (BPlan<T, CSL, FINE, true>::BYTES), bmaps(l, true), mlevel(l), x, done,
+                                  err_, partials_, cg_);
+            else
+                UAAMG_LAUNCH_SMEM(tag, (k_level_box<T, FINE, CSL, true, false>), box_grid(L.g), blk,
+                                  (BPlan<T, CSL, FINE, true>::BYTES), bmaps(l, true), mlevel(l), x, done,
+                                  err_, partials_, cg_);
+            return;
+        }
         if (fused_ && nu == 1 && !(FINE && dirichlet_)) {
             // b, code (coarse levels: diagonal, couplings), coarse x in; x out
             const KTag tag{K_UP, l, c * (2.0 * t + 1.0 + coef) + cc * t};

@@ -613,6 +613,259 @@ __global__ void __launch_bounds__(kThreads, (FCfg<DIM, T, CS, FINE, UP>::MINB))
     }
 }
 
+// ---------------------------------------------------------------------------
+// Small 3D levels (a few 8^3 tiles): the same two steps per level as whole-tile
+// boxes instead of z marches, whose pipeline never fills on a handful of planes.  A
+// block owns an 8 x 8 x 8 tile; one TMA load per array brings the tile and a 2-cell
+// ring (12^3 cells) into shared memory; then (1) the odd-colour values on the whole
+// box, (2) the even-colour values on the tile and the inner ring, (3) the final
+// results on the tile (way down: residual and restriction; way up: odd colour of
+// the reverse sweep, the store, and on the finest level the z sums), with one block
+// barrier between the phases.  Per-cell expressions are those of k_level_fused.
+constexpr int kBT = 8;               // tile edge
+constexpr int kBB = kBT + 4;         // box edge (2-cell ring)
+
+// Box of element type E: cells i in [i0-2, i0+9] (i0 = 1 + 8 bx), the start column
+// 8 bx - A rounded to 16 bytes; rows and planes 12.
+template <class E>
+struct BBox {
+    static constexpr int A = 16 / (int)sizeof(E);
+    static constexpr int W = (A + kBB - 1 + A - 1) / A * A;
+    static constexpr uint32_t BYTES = (uint32_t)(W * kBB * kBB * sizeof(E));
+    __host__ __device__ static constexpr int pos(int di, int dj, int dk) {
+        return ((dk + 2) * kBB + (dj + 2)) * W + A + 1 + di;
+    }
+};
+// Parent box (coarse x under the box): coarse cells [4 bx, 4 bx + 5] per axis.
+template <class T>
+struct BQBox {
+    static constexpr int W = (6 * (int)sizeof(T) + 15) / 16 * 16 / (int)sizeof(T);
+    static constexpr uint32_t BYTES = (uint32_t)(W * 6 * 6 * sizeof(T));
+};
+
+template <class T, class CS, bool FINE, bool UP>
+struct BPlan {
+    static constexpr size_t OFF_B = 0;
+    static constexpr size_t OFF_CODE = align128(BBox<T>::BYTES);
+    static constexpr size_t OFF_DG = OFF_CODE + align128(BBox<uint8_t>::BYTES);
+    static constexpr size_t CB = align128(BBox<CS>::BYTES);
+    static constexpr size_t OFF_CX = OFF_DG + (FINE ? 0 : align128(BBox<T>::BYTES));
+    static constexpr size_t OFF_CY = OFF_CX + CB, OFF_CZ = OFF_CY + CB;
+    static constexpr size_t OFF_XC = OFF_CX + (FINE ? 0 : 3 * CB);
+    static constexpr size_t OFF_X = OFF_XC + (UP ? align128(BQBox<T>::BYTES) : 0);
+    static constexpr size_t OFF_BAR = OFF_X + align128(BBox<T>::BYTES);
+    static constexpr size_t OFF_LUT = OFF_BAR + 128;
+    static constexpr size_t BYTES = OFF_LUT + align128(64 * sizeof(T));
+    static constexpr uint32_t TX = BBox<T>::BYTES + BBox<uint8_t>::BYTES +
+                                   (FINE ? 0u : BBox<T>::BYTES + 3 * BBox<CS>::BYTES) +
+                                   (UP ? BQBox<T>::BYTES : 0u);
+};
+
+// Tensor maps of a box kernel: b, codes, diagonal, couplings (BBox geometry), and the
+// parent level's x (BQBox geometry).
+struct BMaps {
+    CUtensorMap b, code, dg, cx, cy, cz, xc;
+};
+
+template <class T, bool FINE, class CS, bool UP, bool ZDOT>
+__global__ void __launch_bounds__(kThreads)
+    k_level_box(const __grid_constant__ BMaps M, MLevel<T> L, T* __restrict__ out,
+                const int* __restrict__ done, int* err, double* partials, CGState* cg) {
+    pdl_entry();
+    if (done && *done) return;
+    using P = BPlan<T, CS, FINE, UP>;
+    constexpr int WT = BBox<T>::W, WC = BBox<uint8_t>::W, WS = BBox<CS>::W;
+    constexpr int PT = WT * kBB, PC = WC * kBB, PS = WS * kBB;  // plane strides
+    constexpr bool kFull = sizeof(T) == 8;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* sm = smem_raw;
+    if (smem_u32(sm) & 127u) {
+        if (threadIdx.x == 0) atomicExch(err, 2);
+        return;
+    }
+    const Geom& g = L.g;
+    const int tid = threadIdx.x;
+    const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+    const int i0 = 1 + kBT * bx, j0 = 1 + kBT * by, k0 = 1 + kBT * bz;
+    T* lut = reinterpret_cast<T*>(sm + P::OFF_LUT);
+    T* xs = reinterpret_cast<T*>(sm + P::OFF_X);
+    const T* bs = reinterpret_cast<const T*>(sm + P::OFF_B);
+    const unsigned char* cs = sm + P::OFF_CODE;
+    const T* dgs = reinterpret_cast<const T*>(sm + P::OFF_DG);
+    const CS* cxs = reinterpret_cast<const CS*>(sm + P::OFF_CX);
+    const CS* cys = reinterpret_cast<const CS*>(sm + P::OFF_CY);
+    const CS* czs = reinterpret_cast<const CS*>(sm + P::OFF_CZ);
+    const T* xcs = reinterpret_cast<const T*>(sm + P::OFF_XC);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + P::OFF_BAR);
+    if (FINE) build_lut<3, T>(lut, L.idx2, L.idy2, L.idz2);
+    bool ok = true;
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        const int x0 = kBT * bx, y0 = kBT * by - 1, z0 = kBT * bz - 1;
+        fence_proxy_async();
+        mbar_expect_tx(bar, P::TX);
+        tma_load<3>(sm + P::OFF_B, &M.b, x0 - BBox<T>::A, y0, z0, bar);
+        tma_load<3>(sm + P::OFF_CODE, &M.code, x0 - BBox<uint8_t>::A, y0, z0, bar);
+        if constexpr (!FINE) {
+            tma_load<3>(sm + P::OFF_DG, &M.dg, x0 - BBox<T>::A, y0, z0, bar);
+            tma_load<3>(sm + P::OFF_CX, &M.cx, x0 - BBox<CS>::A, y0, z0, bar);
+            tma_load<3>(sm + P::OFF_CY, &M.cy, x0 - BBox<CS>::A, y0, z0, bar);
+            tma_load<3>(sm + P::OFF_CZ, &M.cz, x0 - BBox<CS>::A, y0, z0, bar);
+        }
+        if constexpr (UP) tma_load<3>(sm + P::OFF_XC, &M.xc, x0 / 2, (y0 + 1) / 2, (z0 + 1) / 2, bar);
+        ok = mbar_wait(bar, 0u, kTmaWaitLimit);
+    }
+    if (!step_barrier(ok, err)) return;
+
+    // per-cell helpers on box offsets (di, dj, dk) in [-2, 9]
+    auto qT = [](int di, int dj, int dk) { return BBox<T>::pos(di, dj, dk); };
+    auto qC = [](int di, int dj, int dk) { return BBox<uint8_t>::pos(di, dj, dk); };
+    auto qS = [](int di, int dj, int dk) { return BBox<CS>::pos(di, dj, dk); };
+    auto diag = [&](uint32_t code, int q) -> T {
+        if constexpr (FINE) return lut[code & 63u];
+        else return dgs[q];
+    };
+    auto coup = [&](int qs, T (&cc)[6]) {
+        if constexpr (FINE) {
+            cc[0] = cc[1] = L.idx2;
+            cc[2] = cc[3] = L.idy2;
+            cc[4] = cc[5] = L.idz2;
+        } else {
+            cc[0] = coupling<T, CS>(cxs[qs], L.csx);
+            cc[1] = coupling<T, CS>(cxs[qs - 1], L.csx);
+            cc[2] = coupling<T, CS>(cys[qs], L.csy);
+            cc[3] = coupling<T, CS>(cys[qs - WS], L.csy);
+            cc[4] = coupling<T, CS>(czs[qs], L.csz);
+            cc[5] = coupling<T, CS>(czs[qs - PS], L.csz);
+        }
+    };
+    auto nbsum = [&](const T (&cc)[6], int q) -> T {
+        return cc[0] * xs[q + 1] + cc[1] * xs[q - 1] + cc[2] * xs[q + WT] + cc[3] * xs[q - WT] +
+               cc[4] * xs[q + PT] + cc[5] * xs[q - PT];
+    };
+    auto prolong = [&](int di, int dj, int dk) -> T {
+        return T(2) * xcs[(((dk + 2) >> 1) * 6 + ((dj + 2) >> 1)) * BQBox<T>::W + ((di + 2) >> 1)];
+    };
+    // colour of a box cell: (i + j + k) & 1 with i0 + j0 + k0 odd
+    const int par0 = (i0 + j0 + k0) & 1;
+
+    // 1. odd values on the whole box
+    for (int c = tid; c < kBB * kBB * kBB; c += kThreads) {
+        const int di = c % kBB - 2, dj = (c / kBB) % kBB - 2, dk = c / (kBB * kBB) - 2;
+        if (((di + dj + dk + par0) & 1) == 0) continue;
+        const int q = qT(di, dj, dk);
+        const uint32_t code = cs[qC(di, dj, dk)];
+        T v = T(0);
+        if (code & kActive) {
+            const T d = diag(code, q);
+            v = d < T(1e-30) ? T(0) : mdiv<T, CS>(bs[q] + T(0), d);
+            if constexpr (UP) v = v + prolong(di, dj, dk);
+        }
+        xs[q] = v;
+    }
+    __syncthreads();
+    // 2. even values on the tile and the inner ring
+    for (int c = tid; c < (kBT + 2) * (kBT + 2) * (kBT + 2); c += kThreads) {
+        const int di = c % (kBT + 2) - 1, dj = (c / (kBT + 2)) % (kBT + 2) - 1,
+                  dk = c / ((kBT + 2) * (kBT + 2)) - 1;
+        if (((di + dj + dk + par0) & 1) != 0) continue;
+        const int q = qT(di, dj, dk);
+        const uint32_t code = cs[qC(di, dj, dk)];
+        T v = T(0);
+        if (code & kActive) {
+            const T d = diag(code, q);
+            if (d < T(1e-30)) {
+                if constexpr (UP) v = T(0) + prolong(di, dj, dk);
+            } else {
+                T cc[6];
+                coup(qS(di, dj, dk), cc);
+                v = mdiv<T, CS>(bs[q] + nbsum(cc, q), d);
+            }
+        }
+        xs[q] = v;
+    }
+    __syncthreads();
+    // 3. final results on the tile
+    double acc[3] = {0.0, 0.0, 0.0};
+    T* rs = reinterpret_cast<T*>(sm + P::OFF_B);  // way down: residuals replace b (tile only)
+    T res[2];
+    int resq[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const int c = tid + u * kThreads;  // 512 tile cells, two a thread
+        const int di = c % kBT, dj = (c / kBT) % kBT, dk = c / (kBT * kBT);
+        const bool odd = ((di + dj + dk + par0) & 1) != 0;
+        const int q = qT(di, dj, dk);
+        const uint32_t code = cs[qC(di, dj, dk)];
+        const T x0 = xs[q];
+        T v = UP ? x0 : T(0);
+        if (code & kActive) {
+            const T d = diag(code, q);
+            if constexpr (UP) {
+                if (odd && !(d < T(1e-30))) {
+                    T cc[6];
+                    coup(qS(di, dj, dk), cc);
+                    v = mdiv<T, CS>(bs[q] + nbsum(cc, q), d);
+                }
+            } else if constexpr (kFull) {
+                T cc[6];
+                coup(qS(di, dj, dk), cc);
+                const T ax = d * x0 - cc[0] * xs[q + 1] - cc[1] * xs[q - 1] - cc[2] * xs[q + WT] -
+                             cc[3] * xs[q - WT] - cc[4] * xs[q + PT] - cc[5] * xs[q - PT];
+                v = bs[q] - ax;
+            } else {
+                if (d < T(1e-30)) {
+                    v = bs[q];
+                } else if (odd) {
+                    T cc[6];
+                    coup(qS(di, dj, dk), cc);
+                    v = nbsum(cc, q);
+                }
+            }
+        }
+        res[u] = v;
+        resq[u] = q;
+        if constexpr (UP) {
+            const int i = i0 + di, j = j0 + dj, k = k0 + dk;
+            if (i <= g.nx && j <= g.ny && k <= g.nz) {
+                out[cidx(g, i, j, k)] = v;
+                if (ZDOT && (code & kActive)) {
+                    const double zv = (double)v, rv = (double)bs[q];
+                    acc[0] += zv;
+                    acc[1] += rv * zv;
+                    acc[2] += rv;
+                }
+            }
+        }
+    }
+    if constexpr (!UP) {
+        __syncthreads();  // every b of the tile has been read
+#pragma unroll
+        for (int u = 0; u < 2; ++u) rs[resq[u]] = res[u];
+        __syncthreads();
+        // restriction: 4^3 coarse cells, the 2x2x2 children in (di, dj, dk) order
+        if (tid < (kBT / 2) * (kBT / 2) * (kBT / 2)) {
+            const int ci = tid % 4, cj = (tid / 4) % 4, ck = tid / 16;
+            const int ic = kBT / 2 * bx + 1 + ci, jc = kBT / 2 * by + 1 + cj, kc = kBT / 2 * bz + 1 + ck;
+            if (ic <= L.cg.nx && jc <= L.cg.ny && kc <= L.cg.nz) {
+                T sum = T(0);
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) sum += rs[qT(2 * ci + a, 2 * cj + b2, 2 * ck + e)];
+                // also written on solid coarse cells, where no kernel reads b
+                out[cidx(L.cg, ic, jc, kc)] = sum;
+            }
+        }
+    }
+    if constexpr (UP && ZDOT) {
+        double tot[3];
+        if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
+    }
+}
+
 #undef UAAMG_FUSED_SMEM
 
 }  // namespace
