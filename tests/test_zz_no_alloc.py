@@ -5,8 +5,8 @@ stream capture, host callbacks, or applications that own every allocation --
 use uaamg_residual_noalloc to measure ||b - A p|| and ||b|| with no handle and no
 cudaMalloc.  This test checks it, through the C-ABI, against the same two numbers
 from the regular entry point (uaamg_solve_device with max_iter = 0 and a warm
-start, whose exit statistics are the FP64 true residual of the given p), on two
-calls in a row: the second call reuses the shared scratch the first one left.
+start, whose exit statistics are the FP64 true residual of the given p) and against
+the oracle's FP64 residual of the same p, on two calls in a row: the second call reuses the shared scratch the first one left.
 
 This file is named to be collected last; it creates its own handle and buffers,
 so it also passes alone in a fresh process.
@@ -14,6 +14,7 @@ so it also passes alone in a fresh process.
 import ctypes as C
 
 import numpy as np
+import oracle as O
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -75,6 +76,9 @@ def test_residual_noalloc_matches_solver(dim):
             torch.cuda.synchronize()
             got = d_out.cpu().numpy()
             assert np.all(np.abs(got - ref) <= REL_TOL * np.abs(ref)), (got, ref)
+        # and directly against the oracle's FP64 residual of the same p
+        orc = np.array(O.true_residual(solid, rhs, p, *sp))
+        assert np.all(np.abs(got - orc) <= REL_TOL * np.abs(orc)), (got, orc)
     finally:
         h.close()
 

@@ -60,6 +60,7 @@ struct LevelBuf {
 };
 
 // 3D levels of at most this many cells run the fused steps as whole-tile boxes
+// (UAAMG_BOX_MAX_CELLS overrides it, for comparisons)
 constexpr double kBoxCells = 64.0 * 64.0 * 64.0;
 
 // Kernel classes for the in-situ per-kernel timing (uaamg_profile_solve).
@@ -125,6 +126,8 @@ public:
         // attribute (fully serialised on the stream), for comparisons
         const char* v = std::getenv("UAAMG_NO_PDL");
         pdl_ = !(v && v[0] == '1');
+        const char* bc = std::getenv("UAAMG_BOX_MAX_CELLS");
+        if (bc && bc[0]) box_cells_ = std::atof(bc);
     }
     ~EngineT() override {
         release();
@@ -391,6 +394,7 @@ private:
     bool autotune_ = false;  // time the marches' z-chunk lengths at set-up
     bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
     bool fused_ = true;      // two fused marches a level (fused.cuh) instead of four
+    double box_cells_ = kBoxCells;
     bool pdl_ = true;        // programmatic dependent launch between the kernels
     bool nopdl_next_ = false;  // the next launch is plain (a kernel that usually exits at
                                // once: its blocks should not wait resident for their turn)
@@ -605,7 +609,7 @@ private:
             L.zc = DIM == 3 ? pick_zc(L.g) : 2;
             // largest face count of a level-l coupling: 4^l (3D), 2^l (2D)
             L.c32 = kHalf && l > 0 && (DIM == 3 ? 2 * l : l) > 11;
-            L.box = DIM == 3 && cells(L.g) <= kBoxCells;
+            L.box = DIM == 3 && cells(L.g) <= box_cells_;
             const size_t n = (size_t)L.g.n;
             if ((e = alloc(L.solid, n))) return e;
             if ((e = alloc(L.code, n))) return e;

@@ -674,8 +674,8 @@ __global__ void __launch_bounds__(kThreads)
     pdl_entry();
     if (done && *done) return;
     using P = BPlan<T, CS, FINE, UP>;
-    constexpr int WT = BBox<T>::W, WC = BBox<uint8_t>::W, WS = BBox<CS>::W;
-    constexpr int PT = WT * kBB, PC = WC * kBB, PS = WS * kBB;  // plane strides
+    constexpr int WT = BBox<T>::W, WS = BBox<CS>::W;
+    constexpr int PT = WT * kBB, PS = WS * kBB;  // plane strides
     constexpr bool kFull = sizeof(T) == 8;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* sm = smem_raw;
@@ -698,6 +698,11 @@ __global__ void __launch_bounds__(kThreads)
     const T* xcs = reinterpret_cast<const T*>(sm + P::OFF_XC);
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + P::OFF_BAR);
     if (FINE) build_lut<3, T>(lut, L.idx2, L.idy2, L.idz2);
+    // The code box starts at the 16-byte boundary at or below its first column (x0 - 1
+    // in the padded array): x0 - 16 when bx is even, x0 - 8 when it is odd.  Every other
+    // box starts at x0 - A, a 16-byte boundary for its element size.
+    const int aC = kBT * bx - 16 * ((kBT * bx - 1) >> 4);
+    static_assert(16 + kBT + 2 < BBox<uint8_t>::W, "code box: tile and ring at the widest offset");
     bool ok = true;
     if (tid == 0) {
         mbar_init(bar, 1);
@@ -705,7 +710,7 @@ __global__ void __launch_bounds__(kThreads)
         fence_proxy_async();
         mbar_expect_tx(bar, P::TX);
         tma_load<3>(sm + P::OFF_B, &M.b, x0 - BBox<T>::A, y0, z0, bar);
-        tma_load<3>(sm + P::OFF_CODE, &M.code, x0 - BBox<uint8_t>::A, y0, z0, bar);
+        tma_load<3>(sm + P::OFF_CODE, &M.code, x0 - aC, y0, z0, bar);
         if constexpr (!FINE) {
             tma_load<3>(sm + P::OFF_DG, &M.dg, x0 - BBox<T>::A, y0, z0, bar);
             tma_load<3>(sm + P::OFF_CX, &M.cx, x0 - BBox<CS>::A, y0, z0, bar);
@@ -719,7 +724,9 @@ __global__ void __launch_bounds__(kThreads)
 
     // per-cell helpers on box offsets (di, dj, dk) in [-2, 9]
     auto qT = [](int di, int dj, int dk) { return BBox<T>::pos(di, dj, dk); };
-    auto qC = [](int di, int dj, int dk) { return BBox<uint8_t>::pos(di, dj, dk); };
+    auto qC = [aC](int di, int dj, int dk) {
+        return BBox<uint8_t>::pos(di, dj, dk) - BBox<uint8_t>::A + aC;
+    };
     auto qS = [](int di, int dj, int dk) { return BBox<CS>::pos(di, dj, dk); };
     auto diag = [&](uint32_t code, int q) -> T {
         if constexpr (FINE) return lut[code & 63u];
