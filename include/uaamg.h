@@ -220,6 +220,15 @@ UAAMG_API uaamg_status uaamg_num_levels(uaamg_handle* h, int* nlevels);
 UAAMG_API uaamg_status uaamg_level_dims(uaamg_handle* h, int l, int* nx, int* ny, int* nz);
 UAAMG_API uaamg_status uaamg_copy_level(uaamg_handle* h, int precision, int l, uint8_t* solid,
                               double* cx, double* cy, double* cz);
+/* Trimming of level l (3D levels of at most 64^3 cells, run as whole 8^3-tile boxes):
+ * *boxes = the level's boxes (0 on other levels), *trimmed = those whose tile and
+ * 2-cell ring are interior fluid with one diagonal and one coupling per axis, which
+ * the box kernels run without loading diagonals, couplings or codes (the reference's
+ * tile trimming, cuda_uaamg_preconditioner_3d.cu:81-99 and :357-375; results are
+ * identical either way).  UAAMG_NO_TRIM=1 in the environment turns trimming off for
+ * engines created afterwards. */
+UAAMG_API uaamg_status uaamg_level_trim(uaamg_handle* h, int precision, int l, int* boxes,
+                                        int* trimmed);
 
 /* In-situ kernel timing: runs uaamg_solve_device with a CUDA event pair around
  * every kernel launch and returns, per (kernel class, level), the launch count,

@@ -32,6 +32,7 @@ EXPORTS = [
     "uaamg_set_dirichlet_walls", "uaamg_set_variable_laplacian", "uaamg_solve",
     "uaamg_solve_device", "uaamg_precond_apply",
     "uaamg_residual_history", "uaamg_num_levels", "uaamg_level_dims", "uaamg_copy_level",
+    "uaamg_level_trim",
     "uaamg_device_bytes", "uaamg_last_error", "uaamg_status_string", "uaamg_profile_solve",
     "uaamg_set_vcycle_kernels", "uaamg_residual_noalloc", "uaamg_solve_batch",
     "uaamg_set_autotune", "uaamg_server_default_config", "uaamg_server_start",
@@ -170,6 +171,7 @@ def load(path: str | None = None):
     L.uaamg_num_levels.argtypes = [p, C.POINTER(i)]
     L.uaamg_level_dims.argtypes = [p, i, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
     L.uaamg_copy_level.argtypes = [p, i, i, p, p, p, p]
+    L.uaamg_level_trim.argtypes = [p, i, i, C.POINTER(i), C.POINTER(i)]
     L.uaamg_device_bytes.argtypes = [p, C.POINTER(C.c_size_t)]
     L.uaamg_profile_solve.argtypes = [p, p, p, C.POINTER(Options), C.POINTER(Stats),
                                       C.POINTER(KernelTime), i, C.POINTER(i)]

@@ -427,6 +427,16 @@ uaamg_status uaamg_level_dims(uaamg_handle* h, int l, int* nx, int* ny, int* nz)
     return UAAMG_OK;
 }
 
+uaamg_status uaamg_level_trim(uaamg_handle* h, int precision, int l, int* boxes, int* trimmed) {
+    if (!h || !boxes || !trimmed) return UAAMG_INVALID_ARG;
+    cudaSetDevice(h->device);
+    uaamg::Engine* eng = nullptr;
+    uaamg_status s = engine_for(h, precision, &eng);
+    if (s != UAAMG_OK) return s;
+    if (l < 0 || l >= eng->nlevels()) return fail(h, UAAMG_INVALID_ARG, "level out of range");
+    return map_engine(h, eng->level_trim(l, boxes, trimmed), "level_trim");
+}
+
 uaamg_status uaamg_copy_level(uaamg_handle* h, int precision, int l, uint8_t* solid, double* cx,
                               double* cy, double* cz) {
     if (!h) return UAAMG_INVALID_ARG;

@@ -57,6 +57,7 @@ struct LevelBuf {
     // their parent box
     bool box = false;
     CUtensorMap bb, bcode, bdg, bcx, bcy, bcz, bxq;
+    T* trim = nullptr;  // coarse box levels: per box {d, c_x, c_y, c_z} or d = 0 (k_box_trim)
 };
 
 // 3D levels of at most this many cells run the fused steps as whole-tile boxes
@@ -128,6 +129,9 @@ public:
         pdl_ = !(v && v[0] == '1');
         const char* bc = std::getenv("UAAMG_BOX_MAX_CELLS");
         if (bc && bc[0]) box_cells_ = std::atof(bc);
+        // UAAMG_NO_TRIM=1: coarse boxes always load their diagonals and couplings
+        const char* nt = std::getenv("UAAMG_NO_TRIM");
+        trim_ = !(nt && nt[0] == '1');
     }
     ~EngineT() override {
         release();
@@ -244,6 +248,22 @@ public:
 
     void level_dims(int l, int* nx, int* ny, int* nz) const override {
         *nx = lv_[l].g.nx; *ny = lv_[l].g.ny; *nz = lv_[l].g.nz;
+    }
+
+    int level_trim(int l, int* boxes, int* trimmed) override {
+        if (l < 0 || l >= (int)lv_.size()) return E_ARG;
+        const LevelBuf<T, CS>& L = lv_[l];
+        *boxes = *trimmed = 0;
+        if (!L.box) return E_OK;
+        const dim3 bg = box_grid(L.g);
+        *boxes = (int)(bg.x * bg.y * bg.z);
+        if (!L.trim || !trim_) return E_OK;
+        std::vector<T> rec((size_t)4 * *boxes);
+        if (cudaMemcpy(rec.data(), L.trim, rec.size() * sizeof(T), cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+            return E_CUDA;
+        for (int b = 0; b < *boxes; ++b) *trimmed += rec[(size_t)4 * b] != T(0);
+        return E_OK;
     }
 
     // Host copies in the reference layout of level l (row pitch nx_l + 2).
@@ -395,6 +415,7 @@ private:
     bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
     bool fused_ = true;      // two fused marches a level (fused.cuh) instead of four
     double box_cells_ = kBoxCells;
+    bool trim_ = true;       // trimmed coarse boxes (fused.cuh k_box_trim)
     bool pdl_ = true;        // programmatic dependent launch between the kernels
     bool nopdl_next_ = false;  // the next launch is plain (a kernel that usually exits at
                                // once: its blocks should not wait resident for their turn)
@@ -621,6 +642,10 @@ private:
                 if ((e = alloc(L.x, n))) return e;
                 if ((e = alloc(L.b, n))) return e;
                 if ((e = alloc(L.dg, n))) return e;
+                if (L.box) {
+                    const dim3 bg = box_grid(L.g);
+                    if ((e = alloc(L.trim, (size_t)4 * bg.x * bg.y * bg.z))) return e;
+                }
                 if constexpr (kHalf) {
                     if (!L.c32) {
                         if ((e = alloc(L.hcx, n)) || (e = alloc(L.hcy, n))) return e;
@@ -778,6 +803,21 @@ private:
         for (int l = 0; l < nl; ++l)
             UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), k_codes<DIM>, vec_grid(lv_[l].g), dim3(32, 8),
                          lv_[l].g, lv_[l].solid, lv_[l].code, l == 0 ? 1 : 0);
+        if constexpr (DIM == 3) {  // trimmed boxes of the coarse box levels
+            for (int l = 1; l < nl; ++l) {
+                const LevelBuf<T, CS>& Cl = lv_[l];
+                if (!Cl.box) continue;
+                const MLevel<T> m = mlevel(l);
+                if (kHalf && !Cl.c32)
+                    UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_box_trim<T, CS>), box_grid(Cl.g), 256,
+                                 Cl.g, Cl.code, Cl.dg, Cl.hcx, Cl.hcy, Cl.hcz, m.csx, m.csy, m.csz,
+                                 Cl.trim);
+                else
+                    UAAMG_LAUNCH((KTag{K_SETUP, l, 0.0}), (k_box_trim<T, T>), box_grid(Cl.g), 256,
+                                 Cl.g, Cl.code, Cl.dg, Cl.cx, Cl.cy, Cl.cz, m.csx, m.csy, m.csz,
+                                 Cl.trim);
+            }
+        }
         if ((e = sync_check()) != E_OK) return e;
         if ((e = tail_setup<DIM>()) != E_OK) return e;
         if (DIM == 3 && autotune_) return tune<DIM>();
@@ -1042,6 +1082,7 @@ private:
             m.cx = L.bcx;
             m.cy = L.bcy;
             m.cz = L.bcz;
+            m.trim = trim_ ? L.trim : nullptr;
         }
         if (up) m.xc = lv_[l + 1].bxq;
         return m;

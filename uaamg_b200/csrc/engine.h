@@ -90,6 +90,8 @@ public:
     virtual void level_dims(int l, int* nx, int* ny, int* nz) const = 0;
     // Host copies of level l: mask and FP64 views of cx, cy, cz (nullable).
     virtual int copy_level(int l, uint8_t* solid, double* cx, double* cy, double* cz) = 0;
+    // boxes of level l run by the whole-tile box kernels, and how many are trimmed
+    virtual int level_trim(int l, int* boxes, int* trimmed) = 0;
     virtual void set_stream(cudaStream_t s) = 0;
     virtual size_t device_bytes() const = 0;
     // Number of kernel launches issued by the last solve() (for launch accounting).

@@ -665,7 +665,62 @@ struct BPlan {
 // parent level's x (BQBox geometry).
 struct BMaps {
     CUtensorMap b, code, dg, cx, cy, cz, xc;
+    // coarse levels: per box the default stencil {d, c_x, c_y, c_z} (as T) when every
+    // cell of the box and its 2-cell ring is interior fluid with that diagonal and
+    // those couplings (a trimmed box), else d = 0 (k_box_trim); null: no trimming
+    const void* trim;
 };
+
+// Trimming of a coarse box level (the reference's tile trimming,
+// cuda_uaamg_preconditioner_3d.cu:81-99 and :357-375, on this kernel's 8^3 tiles): a
+// box whose 12^3 cells (tile and 2-cell ring) are all interior fluid and share one
+// diagonal and one coupling per axis needs none of its diagonal, coupling or code
+// boxes: the box kernel loads b (and the parent x) only and uses the four values.
+// The values are the stored ones, so results are identical with and without
+// trimming.  One block of 256 threads per box; rec[4 box + 0] = d or 0.
+template <class E>
+__device__ __forceinline__ bool same_bits(E a, E b) {
+    if constexpr (sizeof(E) == 2) return __half_as_ushort(a) == __half_as_ushort(b);
+    else if constexpr (sizeof(E) == 4) return __float_as_uint(a) == __float_as_uint(b);
+    else return __double_as_longlong(a) == __double_as_longlong(b);
+}
+
+template <class T, class CS>
+__global__ void __launch_bounds__(256) k_box_trim(Geom g, const uint8_t* __restrict__ code,
+                                                  const T* __restrict__ dg, const CS* __restrict__ cx,
+                                                  const CS* __restrict__ cy, const CS* __restrict__ cz,
+                                                  T csx, T csy, T csz, T* rec) {
+    pdl_entry();
+    const int i0 = 1 + kBT * (int)blockIdx.x, j0 = 1 + kBT * (int)blockIdx.y,
+              k0 = 1 + kBT * (int)blockIdx.z;
+    const bool inside = i0 - 2 >= 1 && j0 - 2 >= 1 && k0 - 2 >= 1 && i0 + kBT + 1 <= g.nx &&
+                        j0 + kBT + 1 <= g.ny && k0 + kBT + 1 <= g.nz;
+    bool ok = inside;
+    T d0 = T(0);
+    CS x0{}, y0{}, z0{};
+    if (inside) {
+        const int id0 = cidx(g, i0, j0, k0);
+        d0 = dg[id0];
+        x0 = cx[id0];
+        y0 = cy[id0];
+        z0 = cz[id0];
+        ok = !(d0 < T(1e-30));
+        for (int c = threadIdx.x; ok && c < kBB * kBB * kBB; c += blockDim.x) {
+            const int i = i0 - 2 + c % kBB, j = j0 - 2 + (c / kBB) % kBB, k = k0 - 2 + c / (kBB * kBB);
+            const int id = cidx(g, i, j, k);
+            ok = (code[id] & kActive) && same_bits(dg[id], d0) && same_bits(cx[id], x0) &&
+                 same_bits(cy[id], y0) && same_bits(cz[id], z0);
+        }
+    }
+    ok = __syncthreads_and(ok) != 0;
+    if (threadIdx.x == 0) {
+        const size_t r = 4 * (((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+        rec[r] = ok ? d0 : T(0);
+        rec[r + 1] = ok ? coupling<T, CS>(x0, csx) : T(0);
+        rec[r + 2] = ok ? coupling<T, CS>(y0, csy) : T(0);
+        rec[r + 3] = ok ? coupling<T, CS>(z0, csz) : T(0);
+    }
+}
 
 template <class T, bool FINE, class CS, bool UP, bool ZDOT>
 __global__ void __launch_bounds__(kThreads)
@@ -698,6 +753,16 @@ __global__ void __launch_bounds__(kThreads)
     const T* xcs = reinterpret_cast<const T*>(sm + P::OFF_XC);
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + P::OFF_BAR);
     if (FINE) build_lut<3, T>(lut, L.idx2, L.idy2, L.idz2);
+    // a trimmed coarse box: its default stencil (d > 0), read before any load
+    T trim[4] = {T(0), T(0), T(0), T(0)};
+    if constexpr (!FINE) {
+        if (M.trim) {
+            const T* r = reinterpret_cast<const T*>(M.trim) + 4 * ((bz * gridDim.y + by) * gridDim.x + bx);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) trim[q] = r[q];
+        }
+    }
+    const bool tr = !FINE && trim[0] != T(0);
     // The code box starts at the 16-byte boundary at or below its first column (x0 - 1
     // in the padded array): x0 - 16 when bx is even, x0 - 8 when it is odd.  Every other
     // box starts at x0 - A, a 16-byte boundary for its element size.
@@ -708,14 +773,17 @@ __global__ void __launch_bounds__(kThreads)
         mbar_init(bar, 1);
         const int x0 = kBT * bx, y0 = kBT * by - 1, z0 = kBT * bz - 1;
         fence_proxy_async();
-        mbar_expect_tx(bar, P::TX);
+        constexpr uint32_t kTrimTX = BBox<T>::BYTES + (UP ? BQBox<T>::BYTES : 0u);
+        mbar_expect_tx(bar, tr ? kTrimTX : P::TX);
         tma_load<3>(sm + P::OFF_B, &M.b, x0 - BBox<T>::A, y0, z0, bar);
-        tma_load<3>(sm + P::OFF_CODE, &M.code, x0 - aC, y0, z0, bar);
-        if constexpr (!FINE) {
-            tma_load<3>(sm + P::OFF_DG, &M.dg, x0 - BBox<T>::A, y0, z0, bar);
-            tma_load<3>(sm + P::OFF_CX, &M.cx, x0 - BBox<CS>::A, y0, z0, bar);
-            tma_load<3>(sm + P::OFF_CY, &M.cy, x0 - BBox<CS>::A, y0, z0, bar);
-            tma_load<3>(sm + P::OFF_CZ, &M.cz, x0 - BBox<CS>::A, y0, z0, bar);
+        if (!tr) {
+            tma_load<3>(sm + P::OFF_CODE, &M.code, x0 - aC, y0, z0, bar);
+            if constexpr (!FINE) {
+                tma_load<3>(sm + P::OFF_DG, &M.dg, x0 - BBox<T>::A, y0, z0, bar);
+                tma_load<3>(sm + P::OFF_CX, &M.cx, x0 - BBox<CS>::A, y0, z0, bar);
+                tma_load<3>(sm + P::OFF_CY, &M.cy, x0 - BBox<CS>::A, y0, z0, bar);
+                tma_load<3>(sm + P::OFF_CZ, &M.cz, x0 - BBox<CS>::A, y0, z0, bar);
+            }
         }
         if constexpr (UP) tma_load<3>(sm + P::OFF_XC, &M.xc, x0 / 2, (y0 + 1) / 2, (z0 + 1) / 2, bar);
         ok = mbar_wait(bar, 0u, kTmaWaitLimit);
@@ -728,24 +796,6 @@ __global__ void __launch_bounds__(kThreads)
         return BBox<uint8_t>::pos(di, dj, dk) - BBox<uint8_t>::A + aC;
     };
     auto qS = [](int di, int dj, int dk) { return BBox<CS>::pos(di, dj, dk); };
-    auto diag = [&](uint32_t code, int q) -> T {
-        if constexpr (FINE) return lut[code & 63u];
-        else return dgs[q];
-    };
-    auto coup = [&](int qs, T (&cc)[6]) {
-        if constexpr (FINE) {
-            cc[0] = cc[1] = L.idx2;
-            cc[2] = cc[3] = L.idy2;
-            cc[4] = cc[5] = L.idz2;
-        } else {
-            cc[0] = coupling<T, CS>(cxs[qs], L.csx);
-            cc[1] = coupling<T, CS>(cxs[qs - 1], L.csx);
-            cc[2] = coupling<T, CS>(cys[qs], L.csy);
-            cc[3] = coupling<T, CS>(cys[qs - WS], L.csy);
-            cc[4] = coupling<T, CS>(czs[qs], L.csz);
-            cc[5] = coupling<T, CS>(czs[qs - PS], L.csz);
-        }
-    };
     auto nbsum = [&](const T (&cc)[6], int q) -> T {
         return cc[0] * xs[q + 1] + cc[1] * xs[q - 1] + cc[2] * xs[q + WT] + cc[3] * xs[q - WT] +
                cc[4] * xs[q + PT] + cc[5] * xs[q - PT];
@@ -756,120 +806,160 @@ __global__ void __launch_bounds__(kThreads)
     // colour of a box cell: (i + j + k) & 1 with i0 + j0 + k0 odd
     const int par0 = (i0 + j0 + k0) & 1;
 
-    // 1. odd values on the whole box
-    for (int c = tid; c < kBB * kBB * kBB; c += kThreads) {
-        const int di = c % kBB - 2, dj = (c / kBB) % kBB - 2, dk = c / (kBB * kBB) - 2;
-        if (((di + dj + dk + par0) & 1) == 0) continue;
-        const int q = qT(di, dj, dk);
-        const uint32_t code = cs[qC(di, dj, dk)];
-        T v = T(0);
-        if (code & kActive) {
-            const T d = diag(code, q);
-            v = d < T(1e-30) ? T(0) : mdiv<T, CS>(bs[q] + T(0), d);
-            if constexpr (UP) v = v + prolong(di, dj, dk);
-        }
-        xs[q] = v;
-    }
-    __syncthreads();
-    // 2. even values on the tile and the inner ring
-    for (int c = tid; c < (kBT + 2) * (kBT + 2) * (kBT + 2); c += kThreads) {
-        const int di = c % (kBT + 2) - 1, dj = (c / (kBT + 2)) % (kBT + 2) - 1,
-                  dk = c / ((kBT + 2) * (kBT + 2)) - 1;
-        if (((di + dj + dk + par0) & 1) != 0) continue;
-        const int q = qT(di, dj, dk);
-        const uint32_t code = cs[qC(di, dj, dk)];
-        T v = T(0);
-        if (code & kActive) {
-            const T d = diag(code, q);
-            if (d < T(1e-30)) {
-                if constexpr (UP) v = T(0) + prolong(di, dj, dk);
+    // The three steps; TR: a trimmed box (every cell interior fluid, the stencil in
+    // trim[]), whose codes, diagonals and couplings were not loaded.
+    auto run = [&](auto trimc) {
+        constexpr bool TR = decltype(trimc)::value;
+        auto code_at = [&](int di, int dj, int dk) -> uint32_t {
+            if constexpr (TR) return kActive;
+            else return cs[qC(di, dj, dk)];
+        };
+        auto diag = [&](uint32_t code, int q) -> T {
+            if constexpr (TR) return trim[0];
+            else if constexpr (FINE) return lut[code & 63u];
+            else return dgs[q];
+        };
+        auto coup = [&](int qs, T (&cc)[6]) {
+            if constexpr (TR) {
+                cc[0] = cc[1] = trim[1];
+                cc[2] = cc[3] = trim[2];
+                cc[4] = cc[5] = trim[3];
+            } else if constexpr (FINE) {
+                cc[0] = cc[1] = L.idx2;
+                cc[2] = cc[3] = L.idy2;
+                cc[4] = cc[5] = L.idz2;
             } else {
-                T cc[6];
-                coup(qS(di, dj, dk), cc);
-                v = mdiv<T, CS>(bs[q] + nbsum(cc, q), d);
+                cc[0] = coupling<T, CS>(cxs[qs], L.csx);
+                cc[1] = coupling<T, CS>(cxs[qs - 1], L.csx);
+                cc[2] = coupling<T, CS>(cys[qs], L.csy);
+                cc[3] = coupling<T, CS>(cys[qs - WS], L.csy);
+                cc[4] = coupling<T, CS>(czs[qs], L.csz);
+                cc[5] = coupling<T, CS>(czs[qs - PS], L.csz);
             }
+        };
+
+        // 1. odd values on the whole box
+        for (int c = tid; c < kBB * kBB * kBB; c += kThreads) {
+            const int di = c % kBB - 2, dj = (c / kBB) % kBB - 2, dk = c / (kBB * kBB) - 2;
+            if (((di + dj + dk + par0) & 1) == 0) continue;
+            const int q = qT(di, dj, dk);
+            const uint32_t code = code_at(di, dj, dk);
+            T v = T(0);
+            if (code & kActive) {
+                const T d = diag(code, q);
+                v = d < T(1e-30) ? T(0) : mdiv<T, CS>(bs[q] + T(0), d);
+                if constexpr (UP) v = v + prolong(di, dj, dk);
+            }
+            xs[q] = v;
         }
-        xs[q] = v;
-    }
-    __syncthreads();
-    // 3. final results on the tile
-    double acc[3] = {0.0, 0.0, 0.0};
-    T* rs = reinterpret_cast<T*>(sm + P::OFF_B);  // way down: residuals replace b (tile only)
-    T res[2];
-    int resq[2];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-        const int c = tid + u * kThreads;  // 512 tile cells, two a thread
-        const int di = c % kBT, dj = (c / kBT) % kBT, dk = c / (kBT * kBT);
-        const bool odd = ((di + dj + dk + par0) & 1) != 0;
-        const int q = qT(di, dj, dk);
-        const uint32_t code = cs[qC(di, dj, dk)];
-        const T x0 = xs[q];
-        T v = UP ? x0 : T(0);
-        if (code & kActive) {
-            const T d = diag(code, q);
-            if constexpr (UP) {
-                if (odd && !(d < T(1e-30))) {
+        __syncthreads();
+        // 2. even values on the tile and the inner ring
+        for (int c = tid; c < (kBT + 2) * (kBT + 2) * (kBT + 2); c += kThreads) {
+            const int di = c % (kBT + 2) - 1, dj = (c / (kBT + 2)) % (kBT + 2) - 1,
+                      dk = c / ((kBT + 2) * (kBT + 2)) - 1;
+            if (((di + dj + dk + par0) & 1) != 0) continue;
+            const int q = qT(di, dj, dk);
+            const uint32_t code = code_at(di, dj, dk);
+            T v = T(0);
+            if (code & kActive) {
+                const T d = diag(code, q);
+                if (d < T(1e-30)) {
+                    if constexpr (UP) v = T(0) + prolong(di, dj, dk);
+                } else {
                     T cc[6];
                     coup(qS(di, dj, dk), cc);
                     v = mdiv<T, CS>(bs[q] + nbsum(cc, q), d);
                 }
-            } else if constexpr (kFull) {
-                T cc[6];
-                coup(qS(di, dj, dk), cc);
-                const T ax = d * x0 - cc[0] * xs[q + 1] - cc[1] * xs[q - 1] - cc[2] * xs[q + WT] -
-                             cc[3] * xs[q - WT] - cc[4] * xs[q + PT] - cc[5] * xs[q - PT];
-                v = bs[q] - ax;
-            } else {
-                if (d < T(1e-30)) {
-                    v = bs[q];
-                } else if (odd) {
+            }
+            xs[q] = v;
+        }
+        __syncthreads();
+        // 3. final results on the tile
+        double acc[3] = {0.0, 0.0, 0.0};
+        T* rs = reinterpret_cast<T*>(sm + P::OFF_B);  // way down: residuals replace b (tile only)
+        T res[2];
+        int resq[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int c = tid + u * kThreads;  // 512 tile cells, two a thread
+            const int di = c % kBT, dj = (c / kBT) % kBT, dk = c / (kBT * kBT);
+            const bool odd = ((di + dj + dk + par0) & 1) != 0;
+            const int q = qT(di, dj, dk);
+            const uint32_t code = code_at(di, dj, dk);
+            const T x0 = xs[q];
+            T v = UP ? x0 : T(0);
+            if (code & kActive) {
+                const T d = diag(code, q);
+                if constexpr (UP) {
+                    if (odd && !(d < T(1e-30))) {
+                        T cc[6];
+                        coup(qS(di, dj, dk), cc);
+                        v = mdiv<T, CS>(bs[q] + nbsum(cc, q), d);
+                    }
+                } else if constexpr (kFull) {
                     T cc[6];
                     coup(qS(di, dj, dk), cc);
-                    v = nbsum(cc, q);
+                    const T ax = d * x0 - cc[0] * xs[q + 1] - cc[1] * xs[q - 1] - cc[2] * xs[q + WT] -
+                                 cc[3] * xs[q - WT] - cc[4] * xs[q + PT] - cc[5] * xs[q - PT];
+                    v = bs[q] - ax;
+                } else {
+                    if (d < T(1e-30)) {
+                        v = bs[q];
+                    } else if (odd) {
+                        T cc[6];
+                        coup(qS(di, dj, dk), cc);
+                        v = nbsum(cc, q);
+                    }
+                }
+            }
+            res[u] = v;
+            resq[u] = q;
+            if constexpr (UP) {
+                const int i = i0 + di, j = j0 + dj, k = k0 + dk;
+                if (i <= g.nx && j <= g.ny && k <= g.nz) {
+                    out[cidx(g, i, j, k)] = v;
+                    if (ZDOT && (code & kActive)) {
+                        const double zv = (double)v, rv = (double)bs[q];
+                        acc[0] += zv;
+                        acc[1] += rv * zv;
+                        acc[2] += rv;
+                    }
                 }
             }
         }
-        res[u] = v;
-        resq[u] = q;
-        if constexpr (UP) {
-            const int i = i0 + di, j = j0 + dj, k = k0 + dk;
-            if (i <= g.nx && j <= g.ny && k <= g.nz) {
-                out[cidx(g, i, j, k)] = v;
-                if (ZDOT && (code & kActive)) {
-                    const double zv = (double)v, rv = (double)bs[q];
-                    acc[0] += zv;
-                    acc[1] += rv * zv;
-                    acc[2] += rv;
+        if constexpr (!UP) {
+            __syncthreads();  // every b of the tile has been read
+#pragma unroll
+            for (int u = 0; u < 2; ++u) rs[resq[u]] = res[u];
+            __syncthreads();
+            // restriction: 4^3 coarse cells, the 2x2x2 children in (di, dj, dk) order
+            if (tid < (kBT / 2) * (kBT / 2) * (kBT / 2)) {
+                const int ci = tid % 4, cj = (tid / 4) % 4, ck = tid / 16;
+                const int ic = kBT / 2 * bx + 1 + ci, jc = kBT / 2 * by + 1 + cj,
+                          kc = kBT / 2 * bz + 1 + ck;
+                if (ic <= L.cg.nx && jc <= L.cg.ny && kc <= L.cg.nz) {
+                    T sum = T(0);
+#pragma unroll
+                    for (int a = 0; a < 2; ++a)
+#pragma unroll
+                        for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                            for (int e = 0; e < 2; ++e) sum += rs[qT(2 * ci + a, 2 * cj + b2, 2 * ck + e)];
+                    // also written on solid coarse cells, where no kernel reads b
+                    out[cidx(L.cg, ic, jc, kc)] = sum;
                 }
             }
         }
-    }
-    if constexpr (!UP) {
-        __syncthreads();  // every b of the tile has been read
-#pragma unroll
-        for (int u = 0; u < 2; ++u) rs[resq[u]] = res[u];
-        __syncthreads();
-        // restriction: 4^3 coarse cells, the 2x2x2 children in (di, dj, dk) order
-        if (tid < (kBT / 2) * (kBT / 2) * (kBT / 2)) {
-            const int ci = tid % 4, cj = (tid / 4) % 4, ck = tid / 16;
-            const int ic = kBT / 2 * bx + 1 + ci, jc = kBT / 2 * by + 1 + cj, kc = kBT / 2 * bz + 1 + ck;
-            if (ic <= L.cg.nx && jc <= L.cg.ny && kc <= L.cg.nz) {
-                T sum = T(0);
-#pragma unroll
-                for (int a = 0; a < 2; ++a)
-#pragma unroll
-                    for (int b2 = 0; b2 < 2; ++b2)
-#pragma unroll
-                        for (int e = 0; e < 2; ++e) sum += rs[qT(2 * ci + a, 2 * cj + b2, 2 * ck + e)];
-                // also written on solid coarse cells, where no kernel reads b
-                out[cidx(L.cg, ic, jc, kc)] = sum;
-            }
+        if constexpr (UP && ZDOT) {
+            double tot[3];
+            if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
         }
-    }
-    if constexpr (UP && ZDOT) {
-        double tot[3];
-        if (reduce_last<3>(acc, partials, &cg->counter[2], tot)) finish_zdot(cg, tot);
+    };
+    if constexpr (FINE) {
+        run(std::false_type{});
+    } else {
+        if (tr) run(std::true_type{});
+        else run(std::false_type{});
     }
 }
 

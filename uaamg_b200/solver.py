@@ -337,6 +337,14 @@ class Handle:
                                               _ptr(cz)), "copy_level")
         return solid, cx, cy, cz
 
+    def level_trim(self, l, precision="fp64"):
+        """(boxes, trimmed boxes) of level l (uaamg_level_trim)."""
+        a, b = C.c_int(), C.c_int()
+        prec = _capi.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        self._check(self.lib.uaamg_level_trim(self.h, prec, l, C.byref(a), C.byref(b)),
+                    "level_trim")
+        return a.value, b.value
+
     def device_bytes(self) -> int:
         b = C.c_size_t()
         self._check(self.lib.uaamg_device_bytes(self.h, C.byref(b)), "device_bytes")
