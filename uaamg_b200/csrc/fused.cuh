@@ -838,52 +838,77 @@ __global__ void __launch_bounds__(kThreads)
             }
         };
 
-        // 1. odd values on the whole box
-        for (int c = tid; c < kBB * kBB * kBB; c += kThreads) {
-            const int di = c % kBB - 2, dj = (c / kBB) % kBB - 2, dk = c / (kBB * kBB) - 2;
-            if (((di + dj + dk + par0) & 1) == 0) continue;
-            const int q = qT(di, dj, dk);
-            const uint32_t code = code_at(di, dj, dk);
-            T v = T(0);
-            if (code & kActive) {
-                const T d = diag(code, q);
-                v = d < T(1e-30) ? T(0) : mdiv<T, CS>(bs[q] + T(0), d);
-                if constexpr (UP) v = v + prolong(di, dj, dk);
-            }
-            xs[q] = v;
-        }
-        __syncthreads();
-        // 2. even values on the tile and the inner ring
-        for (int c = tid; c < (kBT + 2) * (kBT + 2) * (kBT + 2); c += kThreads) {
-            const int di = c % (kBT + 2) - 1, dj = (c / (kBT + 2)) % (kBT + 2) - 1,
-                      dk = c / ((kBT + 2) * (kBT + 2)) - 1;
-            if (((di + dj + dk + par0) & 1) != 0) continue;
-            const int q = qT(di, dj, dk);
-            const uint32_t code = code_at(di, dj, dk);
-            T v = T(0);
-            if (code & kActive) {
-                const T d = diag(code, q);
-                if (d < T(1e-30)) {
-                    if constexpr (UP) v = T(0) + prolong(di, dj, dk);
-                } else {
-                    T cc[6];
-                    coup(qS(di, dj, dk), cc);
-                    v = mdiv<T, CS>(bs[q] + nbsum(cc, q), d);
+        // Cells are enumerated by colour: the rows (dj, dk) of a region hold
+        // alternating colours, so the k-th cell of a colour in a row is di = first +
+        // 2 m + s with s fixed by the row's parity.  A thread steps its enumeration
+        // index by the block size, updating (m, row) incrementally.
+        static_assert(kThreads == 256, "incremental colour enumeration assumes 256 threads");
+        // 1. odd values on the whole box: 144 rows of 12 cells, 6 odd per row; a step
+        // of 256 is 42 rows (3 planes and 6 rows) and 4 cells
+        {
+            int m = tid % 6, jj = (tid / 6) % kBB, kk = tid / (6 * kBB);
+            while (kk < kBB) {
+                const int dj = jj - 2, dk = kk - 2;
+                const int di = -2 + 2 * m + ((1 + dj + dk + par0) & 1);
+                const int q = qT(di, dj, dk);
+                const uint32_t code = code_at(di, dj, dk);
+                T v = T(0);
+                if (code & kActive) {
+                    const T d = diag(code, q);
+                    v = d < T(1e-30) ? T(0) : mdiv<T, CS>(bs[q] + T(0), d);
+                    if constexpr (UP) v = v + prolong(di, dj, dk);
                 }
+                xs[q] = v;
+                m += 4;
+                jj += 6;
+                kk += 3;
+                if (m >= 6) { m -= 6; jj += 1; }
+                if (jj >= kBB) { jj -= kBB; kk += 1; }
             }
-            xs[q] = v;
         }
         __syncthreads();
-        // 3. final results on the tile
+        // 2. even values on the tile and the inner ring: 100 rows of 10 cells, 5 even
+        // per row; a step of 256 is 51 rows (5 planes and 1 row) and 1 cell
+        {
+            constexpr int R = kBT + 2;
+            int m = tid % 5, jj = (tid / 5) % R, kk = tid / (5 * R);
+            while (kk < R) {
+                const int dj = jj - 1, dk = kk - 1;
+                const int di = -1 + 2 * m + ((1 + dj + dk + par0) & 1);
+                const int q = qT(di, dj, dk);
+                const uint32_t code = code_at(di, dj, dk);
+                T v = T(0);
+                if (code & kActive) {
+                    const T d = diag(code, q);
+                    if (d < T(1e-30)) {
+                        if constexpr (UP) v = T(0) + prolong(di, dj, dk);
+                    } else {
+                        T cc[6];
+                        coup(qS(di, dj, dk), cc);
+                        v = mdiv<T, CS>(bs[q] + nbsum(cc, q), d);
+                    }
+                }
+                xs[q] = v;
+                m += 1;
+                jj += 1;
+                kk += 5;
+                if (m >= 5) { m -= 5; jj += 1; }
+                if (jj >= R) { jj -= R; kk += 1; }
+            }
+        }
+        __syncthreads();
+        // 3. final results on the tile: thread = the x pair (2 m, 2 m + 1) of row (dj,
+        // dk); u = 0 its odd cell, u = 1 its even cell (no lane diverges on colour)
         double acc[3] = {0.0, 0.0, 0.0};
         T* rs = reinterpret_cast<T*>(sm + P::OFF_B);  // way down: residuals replace b (tile only)
         T res[2];
         int resq[2];
+        const int pm = tid & 3, pj = (tid >> 2) & 7, pk = tid >> 5;
+        const int sO = (1 + pj + pk + par0) & 1;  // the odd cell is di = 2 pm + sO
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
-            const int c = tid + u * kThreads;  // 512 tile cells, two a thread
-            const int di = c % kBT, dj = (c / kBT) % kBT, dk = c / (kBT * kBT);
-            const bool odd = ((di + dj + dk + par0) & 1) != 0;
+            const bool odd = u == 0;
+            const int di = 2 * pm + (u == 0 ? sO : 1 - sO), dj = pj, dk = pk;
             const int q = qT(di, dj, dk);
             const uint32_t code = code_at(di, dj, dk);
             const T x0 = xs[q];
