@@ -141,6 +141,22 @@ def test_vcycle_fp64_bit_exact_random(handle, vkernels, seed):
     assert np.array_equal(z[sl], zr[sl])
 
 
+@pytest.mark.parametrize("shape,frac", [((134, 140, 146), 0.1), ((112, 150, 138), 0.3)])
+def test_vcycle_fp64_bit_exact_coarse_march_levels(handle, shape, frac):
+    """Grids whose level 1 has more than 64^3 cells, so that coarse levels run as z
+    marches (the smaller random cases reach only whole-tile box levels), with odd
+    dimensions and solids: the FP64 V-cycle equals the oracle's bit for bit."""
+    rng = np.random.default_rng(sum(shape))
+    solid = (rng.random(shape) < frac).astype(np.uint8)
+    r = rng.standard_normal(shape)
+    sp = (0.7, 1.1, 0.9)
+    handle.set_problem(solid, *sp)
+    z = handle.precond_apply(r, "fp64")
+    zr = O.Hierarchy(solid, *sp).vcycle(r)
+    sl = tuple(slice(1, -1) for _ in z.shape)
+    assert np.array_equal(z[sl], zr[sl])
+
+
 def test_apply_twice_is_stateless(handle):
     """Repeated applications on one handle give identical results
     (src/solver/cuda/test_apply_twice.cu:22-159)."""
