@@ -138,14 +138,18 @@ public:
         if (cap_) cudaStreamDestroy(cap_);
     }
 
+    // A new problem.  The previous problem's device buffers are kept for reuse by size
+    // (a mask change on the same grid -- moving solids -- allocates nothing) and the
+    // ones the new hierarchy does not take are freed afterwards.
     int set_problem(int dim, int nx, int ny, int nz, double dx, double dy, double dz,
                     const uint8_t* d_solid, int dirichlet) override {
-        release();
-        if (dim != 2 && dim != 3) return E_ARG;
-        if (nx < 2 || ny < 2 || (dim == 3 && nz < 2)) return E_ARG;
+        release(true);
+        if (dim != 2 && dim != 3) { release(); return E_ARG; }
+        if (nx < 2 || ny < 2 || (dim == 3 && nz < 2)) { release(); return E_ARG; }
         dim_ = dim; dirichlet_ = dirichlet;
         dx_ = dx; dy_ = dy; dz_ = dim == 3 ? dz : 1.0;
         int e = dim == 3 ? build<3>(nx, ny, nz, d_solid) : build<2>(nx, ny, nz, d_solid);
+        free_pool();
         if (e != E_OK) { release(); return e; }
         return E_OK;
     }
@@ -405,7 +409,8 @@ private:
     int* flag_host_ = nullptr;    // pinned, 2 slots
     cudaEvent_t ev_[2] = {nullptr, nullptr};
     cudaStream_t st_ = 0;
-    std::vector<void*> allocs_;
+    std::vector<std::pair<void*, size_t>> allocs_;  // device buffers and their bytes
+    std::multimap<size_t, void*> pool_;               // kept for reuse by set_problem
     size_t bytes_ = 0;
     long launches_ = 0;
     int num_sms_ = 148;
@@ -494,21 +499,32 @@ private:
     template <class P>
     int alloc(P*& p, size_t count) {
         void* q = nullptr;
-        if (cudaMalloc(&q, count * sizeof(P)) != cudaSuccess) {
+        const size_t nb = count * sizeof(P);
+        auto it = pool_.find(nb);
+        if (it != pool_.end()) {
+            q = it->second;
+            pool_.erase(it);
+        } else if (cudaMalloc(&q, nb) != cudaSuccess) {
             cudaGetLastError();
             return E_OOM;
         }
-        allocs_.push_back(q);
-        bytes_ += count * sizeof(P);
+        allocs_.push_back({q, nb});
+        bytes_ += nb;
         if (cudaMemsetAsync(q, 0, count * sizeof(P), st_) != cudaSuccess) return E_CUDA;
         p = static_cast<P*>(q);
         return E_OK;
     }
 
-    void release() {
+    // keep: the device buffers go to the reuse pool (set_problem) instead of being
+    // freed, and the pinned host words and events stay.
+    void release(bool keep = false) {
         if (!allocs_.empty() || cg_host_) cudaStreamSynchronize(st_);
-        for (void* q : allocs_) cudaFree(q);
+        for (const auto& a : allocs_) {
+            if (keep) pool_.emplace(a.second, a.first);
+            else cudaFree(a.first);
+        }
         allocs_.clear();
+        if (!keep) free_pool();
         lv_.clear();
         bytes_ = 0;
         r_ = z_ = p_ = p2_ = ap_ = xlo_ = nullptr;
@@ -517,9 +533,11 @@ private:
         vconv_ = -1;
         err_ = nullptr;
         cg_ = nullptr;
-        if (cg_host_) { cudaFreeHost(cg_host_); cg_host_ = nullptr; }
-        if (flag_host_) { cudaFreeHost(flag_host_); flag_host_ = nullptr; }
-        for (auto& e : ev_) if (e) { cudaEventDestroy(e); e = nullptr; }
+        if (!keep) {
+            if (cg_host_) { cudaFreeHost(cg_host_); cg_host_ = nullptr; }
+            if (flag_host_) { cudaFreeHost(flag_host_); flag_host_ = nullptr; }
+            for (auto& e : ev_) if (e) { cudaEventDestroy(e); e = nullptr; }
+        }
         for (auto& pr : prof_ev_) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
         prof_ev_.clear();
         if (gexec_) { cudaGraphExecDestroy(gexec_); gexec_ = nullptr; }
@@ -527,6 +545,11 @@ private:
         ghist_ = nullptr;
         prof_tag_.clear();
         prof_count_ = 0;
+    }
+
+    void free_pool() {
+        for (const auto& kv : pool_) cudaFree(kv.second);
+        pool_.clear();
     }
 
     int sync_check() {
@@ -676,10 +699,10 @@ private:
         if ((e = alloc(partials_, (size_t)reduce_blocks_ * 4))) return e;
         if ((e = alloc(err_, 1))) return e;
         if ((e = alloc(cg_, 1))) return e;
-        if (cudaMallocHost(&cg_host_, sizeof(CGState)) != cudaSuccess) return E_OOM;
-        if (cudaMallocHost(&flag_host_, 2 * sizeof(int)) != cudaSuccess) return E_OOM;
+        if (!cg_host_ && cudaMallocHost(&cg_host_, sizeof(CGState)) != cudaSuccess) return E_OOM;
+        if (!flag_host_ && cudaMallocHost(&flag_host_, 2 * sizeof(int)) != cudaSuccess) return E_OOM;
         for (auto& ev : ev_)
-            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return E_CUDA;
+            if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return E_CUDA;
         // dynamic shared memory of the marches
         if ((e = march_attrs<DIM, true, CS>()) || (e = march_attrs<DIM, false, CS>()) ||
             (e = smem_attr(k_pmatvec<DIM, T, true>, PmvCfg<DIM, T>::BYTES)) ||
