@@ -85,6 +85,19 @@ struct CGState {
     unsigned int counter[8];  // last-block counters, one per reduction site
 };
 
+// q = a / d and r = a % d for 0 <= a < 2^31, 0 < d, from a reciprocal 1/d computed
+// once (rd): the double-precision estimate is off by at most one and one exact
+// correction step fixes it.  A fraction of the instructions of an integer division
+// by a value known only at run time, which the grid-stride walks would otherwise
+// pay per item.
+__device__ __forceinline__ int divmod_rcp(int a, int d, double rd, int& r) {
+    int q = (int)((double)a * rd);
+    r = a - q * d;
+    if (r < 0) { --q; r += d; }
+    else if (r >= d) { ++q; r -= d; }
+    return q;
+}
+
 // Programmatic dependent launch: the engine launches its kernels so that each may
 // be scheduled while its predecessor on the stream is still finishing.  Every
 // kernel therefore first waits until the preceding grid has completed and its

@@ -905,6 +905,8 @@ private:
             t.dg = L.dg;
             t.x = L.x;
             t.b = L.b;
+            t.rnx = 1.0f / (float)L.g.nx;
+            t.rny = 1.0f / (float)L.g.ny;
             // codes, couplings and diagonal read once per pass, four passes
             bytes += 4.0 * cells(L.g) * ((1.0 + DIM) * sizeof(T) + 1.0);
         }

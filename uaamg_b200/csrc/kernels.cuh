@@ -366,16 +366,18 @@ template <int DIM, class F>
 __device__ __forceinline__ void for_cells(const Geom& g, F&& f) {
     const int nxc = (g.nx + 31) >> 5;
     const int nrows = g.ny * (DIM == 3 ? g.nz : 1);
-    const long long nitems = (long long)nrows * nxc;
-    for (long long it = (long long)blockIdx.x * blockDim.y + threadIdx.y; it < nitems;
-         it += (long long)gridDim.x * blockDim.y) {
-        const int row = (int)(it / nxc);
-        const int ch = (int)(it - (long long)row * nxc);
+    const int nitems = nrows * nxc;  // < 2^26: padded grids have fewer than 2^31 cells
+    const double rx = 1.0 / nxc, ry = 1.0 / g.ny;
+    for (int it = (int)(blockIdx.x * blockDim.y + threadIdx.y); it < nitems;
+         it += (int)(gridDim.x * blockDim.y)) {
+        int ch, jr = 0;
+        const int row = divmod_rcp(it, nxc, rx, ch);
         const int i = 1 + (ch << 5) + (int)threadIdx.x;
         if (i > g.nx) continue;
-        const int j = 1 + row % g.ny;
-        const int k = DIM == 3 ? 1 + row / g.ny : 0;
-        f(i, j, k, cidx(g, i, j, k));
+        int kr = 0;
+        if (DIM == 3) kr = divmod_rcp(row, g.ny, ry, jr);
+        else jr = row;
+        f(i, 1 + jr, DIM == 3 ? 1 + kr : 0, cidx(g, i, 1 + jr, DIM == 3 ? 1 + kr : 0));
     }
 }
 
@@ -607,11 +609,12 @@ __global__ void __launch_bounds__(256) k_pmatvec_2d(Geom g, const uint8_t* __res
     double acc[1] = {0.0};
     const int sx = g.sx;
     const int nxc = (g.nx + 31) >> 5;
-    const long long nitems = (long long)((g.ny + 1) >> 1) * nxc;
-    for (long long it = (long long)blockIdx.x * blockDim.y + threadIdx.y; it < nitems;
-         it += (long long)gridDim.x * blockDim.y) {
-        const int pr = (int)(it / nxc);
-        const int ch = (int)(it - (long long)pr * nxc);
+    const int nitems = ((g.ny + 1) >> 1) * nxc;  // < 2^26
+    const double rx = 1.0 / nxc;
+    for (int it = (int)(blockIdx.x * blockDim.y + threadIdx.y); it < nitems;
+         it += (int)(gridDim.x * blockDim.y)) {
+        int ch;
+        const int pr = divmod_rcp(it, nxc, rx, ch);
         const int i = 1 + (ch << 5) + (int)threadIdx.x;
         if (i > g.nx) continue;
         const int j = 1 + 2 * pr;

@@ -45,6 +45,7 @@ struct TailLevel {
     const T* dg;
     T* x;            // global x and b: used for the first level only
     const T* b;
+    float rnx, rny;  // 1/nx, 1/ny (cell number -> (i, j, k))
 };
 
 template <class T>
@@ -93,13 +94,33 @@ __device__ __forceinline__ T tail_nb(const T (&c)[6], T xr, T xl, T xt, T xb, T 
     return nb;
 }
 
-// Interior cell number c (x fastest) -> (i, j, k).
-template <int DIM>
-__device__ __forceinline__ void tail_ijk(const Geom& g, int c, int& i, int& j, int& k) {
-    i = 1 + c % g.nx;
-    const int r = c / g.nx;
-    j = 1 + (DIM == 3 ? r % g.ny : r);
-    k = DIM == 3 ? 1 + r / g.ny : 0;
+// q = a / d, r = a % d for 0 <= a < 2^24, 0 < d, from the reciprocal rd = 1/d
+// rounded to single precision (computed on the host): the estimate is off by at most
+// one, and one exact correction step fixes it (every phase maps each thread's cell
+// number to (i, j, k); an integer division by a value known only at run time costs as
+// much as the cell's own arithmetic).
+__device__ __forceinline__ int tail_divmod(int a, int d, float rd, int& r) {
+    int q = __float2int_rz((float)a * rd);
+    r = a - q * d;
+    if (r < 0) { --q; r += d; }
+    else if (r >= d) { ++q; r -= d; }
+    return q;
+}
+
+// Interior cell number c (x fastest) -> (i, j, k) of level L.
+template <int DIM, class T>
+__device__ __forceinline__ void tail_ijk(const TailLevel<T>& L, int c, int& i, int& j, int& k) {
+    int ri;
+    const int r = tail_divmod(c, L.g.nx, L.rnx, ri);
+    i = 1 + ri;
+    if (DIM == 3) {
+        int rj;
+        k = 1 + tail_divmod(r, L.g.ny, L.rny, rj);
+        j = 1 + rj;
+    } else {
+        j = 1 + r;
+        k = 0;
+    }
 }
 
 // Value after the forward sweep's first colour: (b + 0)/d on an active odd cell
@@ -122,7 +143,7 @@ __device__ void tail_fwd(const TailView<DIM, T>& V) {
     const int n = tail_ncell<DIM>(g), gx = g.sx, gxy = g.sxy, sx = V.L.csx, sxy = V.L.csxy;
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
         int i, j, k;
-        tail_ijk<DIM>(g, c, i, j, k);
+        tail_ijk<DIM>(V.L, c, i, j, k);
         const int id = V.gid(i, j, k), sd = V.sid(i, j, k);
         const uint32_t code = __ldg(V.L.code + id);
         const T d = __ldg(V.L.dg + id);
@@ -171,7 +192,7 @@ __device__ void tail_res(const TailView<DIM, T>& F, const TailView<DIM, T>& C) {
     const int n = tail_ncell<DIM>(cg);
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
         int ic, jc, kc;
-        tail_ijk<DIM>(cg, c, ic, jc, kc);
+        tail_ijk<DIM>(C.L, c, ic, jc, kc);
         const int i0 = 2 * ic - 1, j0 = 2 * jc - 1, k0 = DIM == 3 ? 2 * kc - 1 : 0;
         T r[8];
 #pragma unroll
@@ -217,7 +238,7 @@ __device__ void tail_up_even(const TailView<DIM, T>& V, const TailView<DIM, T>& 
     const int n = tail_ncell<DIM>(g);
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
         int i, j, k;
-        tail_ijk<DIM>(g, c, i, j, k);
+        tail_ijk<DIM>(V.L, c, i, j, k);
         const int id = V.gid(i, j, k), sd = V.sid(i, j, k);
         const uint32_t code = __ldg(V.L.code + id);
         const T d = __ldg(V.L.dg + id);
@@ -247,7 +268,7 @@ __device__ void tail_up_odd(const TailView<DIM, T>& V) {
     const int n = tail_ncell<DIM>(g), sx = V.L.csx, sxy = V.L.csxy;
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
         int i, j, k;
-        tail_ijk<DIM>(g, c, i, j, k);
+        tail_ijk<DIM>(V.L, c, i, j, k);
         const int id = V.gid(i, j, k), sd = V.sid(i, j, k);
         const uint32_t code = __ldg(V.L.code + id);
         const T d = __ldg(V.L.dg + id);
@@ -285,7 +306,7 @@ __device__ void tail_coarsest(const TailView<DIM, T>& V) {
         for (int q = 0; q < 6; ++q) c2[s][q] = T(0);
         if (c < n) {
             int i, j, k;
-            tail_ijk<DIM>(g, c, i, j, k);
+            tail_ijk<DIM>(V.L, c, i, j, k);
             const int id = V.gid(i, j, k);
             const uint32_t code = __ldg(V.L.code + id);
             const T d = __ldg(V.L.dg + id);
@@ -332,7 +353,7 @@ __global__ void __launch_bounds__(tail_threads<T>()) k_tail(const __grid_constan
         const int n = tail_ncell<DIM>(L.g);
         for (int c = threadIdx.x; c < n; c += blockDim.x) {
             int i, j, k;
-            tail_ijk<DIM>(L.g, c, i, j, k);
+            tail_ijk<DIM>(L, c, i, j, k);
             sm[L.bs + i + j * L.csx + k * L.csxy] = __ldg(L.b + cidx(L.g, i, j, k));
         }
     }
@@ -357,7 +378,7 @@ __global__ void __launch_bounds__(tail_threads<T>()) k_tail(const __grid_constan
         const int n = tail_ncell<DIM>(L.g);
         for (int c = threadIdx.x; c < n; c += blockDim.x) {
             int i, j, k;
-            tail_ijk<DIM>(L.g, c, i, j, k);
+            tail_ijk<DIM>(L, c, i, j, k);
             L.x[cidx(L.g, i, j, k)] = sm[L.xs + i + j * L.csx + k * L.csxy];
         }
     }
