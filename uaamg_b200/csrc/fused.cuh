@@ -95,9 +95,9 @@ struct FCfg {
     static constexpr size_t OFF_X = OFF_RING + S * P::STAGE;
     static constexpr size_t XB = align128(RBox<T>::BYTES);
     static constexpr size_t BYTES = OFF_X + NXP * XB;
-    // resident blocks per SM the finest FP32 level is compiled for (registers);
-    // its shared memory fits five
-    static constexpr int MINB = LEAN && DIM == 3 ? 5 : 1;
+    // resident blocks per SM the finest FP32 level is compiled for (registers): 3D,
+    // five (its shared memory fits five); 2D, eight (a full SM of 256-thread blocks)
+    static constexpr int MINB = LEAN ? (DIM == 3 ? 5 : 8) : 1;
     static_assert(S <= 16, "stage barriers: 128 bytes");
 };
 

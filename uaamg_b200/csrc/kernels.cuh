@@ -71,7 +71,22 @@ __device__ __forceinline__ bool reduce_last(double (&v)[NV], double* partials,
     double acc[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-    for (unsigned b = tid; b < nblk; b += nthr)
+    // partials b = tid, tid + nthr, ... added in that order; the loads of four are
+    // issued together (a launch of thousands of blocks would otherwise pay one L2
+    // round trip per partial here, in one block, at its end)
+    unsigned b = tid;
+    for (; b + 3 * nthr < nblk; b += 4 * nthr) {
+        double t[4][NV];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) t[u][q] = __ldcg(&partials[(size_t)(b + u * nthr) * NV + q]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) acc[q] += t[u][q];
+    }
+    for (; b < nblk; b += nthr)
 #pragma unroll
         for (int q = 0; q < NV; ++q) acc[q] += __ldcg(&partials[(size_t)b * NV + q]);
 #pragma unroll
