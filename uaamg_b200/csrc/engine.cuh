@@ -127,6 +127,8 @@ public:
         // attribute (fully serialised on the stream), for comparisons
         const char* v = std::getenv("UAAMG_NO_PDL");
         pdl_ = !(v && v[0] == '1');
+        const char* pv = std::getenv("UAAMG_PMV2D_PER_SM");
+        if (pv && pv[0]) pmv2d_env_ = std::max(1, std::atoi(pv));
         const char* bc = std::getenv("UAAMG_BOX_MAX_CELLS");
         if (bc && bc[0]) box_cells_ = std::atof(bc);
         // UAAMG_NO_TRIM=1: coarse boxes always load their diagonals and couplings
@@ -420,6 +422,11 @@ private:
     bool tail_on_ = true;    // small levels in one one-block kernel (tail.cuh)
     bool fused_ = true;      // two fused marches a level (fused.cuh) instead of four
     double box_cells_ = kBoxCells;
+    // blocks per SM of the 2D search direction: as many as are resident at once (one
+    // wave: a second, partial wave left SMs idle at its end); UAAMG_PMV2D_PER_SM overrides
+    int pmv2d_per_sm_ = 8;
+    int pmv2d_env_ = 0;
+    int resid_per_sm_ = 8;  // the FP64 residual walk: resident blocks per SM (one wave)
     bool trim_ = true;       // trimmed coarse boxes (fused.cuh k_box_trim)
     bool pdl_ = true;        // programmatic dependent launch between the kernels
     bool nopdl_next_ = false;  // the next launch is plain (a kernel that usually exits at
@@ -455,7 +462,7 @@ private:
     // the partials' capacity)
     dim3 flat2d_grid(const Geom& g) const {
         const long long items = (long long)((g.ny + 1) / 2) * ((g.nx + 31) / 32);
-        long long nb = std::min<long long>((items + 7) / 8, 8LL * num_sms_);
+        long long nb = std::min<long long>((items + 7) / 8, (long long)pmv2d_per_sm_ * num_sms_);
         nb = std::min<long long>(nb, reduce_blocks_);
         return dim3((unsigned)(nb < 1 ? 1 : nb));
     }
@@ -466,7 +473,7 @@ private:
     dim3 resid_grid(const Geom& g) const {
         const long long tiles = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8) *
                                 (g.nz ? (g.nz + kResidZc - 1) / kResidZc : 1);
-        return dim3((unsigned)std::min<long long>(tiles, 8LL * num_sms_));
+        return dim3((unsigned)std::min<long long>(tiles, (long long)resid_per_sm_ * num_sms_));
     }
 
     // grid of the row-walk kernels (kernels.cuh for_cells): capped at 4 blocks per SM
@@ -646,6 +653,24 @@ private:
         cudaGetDevice(&dev);
         if (cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
             return E_CUDA;
+        {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resid_x64<DIM, T>, 256, 0) ==
+                    cudaSuccess && per_sm > 0)
+                resid_per_sm_ = std::min(per_sm, 8);
+            else
+                cudaGetLastError();
+        }
+        if (pmv2d_env_ > 0) {
+            pmv2d_per_sm_ = pmv2d_env_;
+        } else {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pmatvec_2d<T>, 256, 0) ==
+                    cudaSuccess && per_sm > 0)
+                pmv2d_per_sm_ = std::min(per_sm, 8);
+            else
+                cudaGetLastError();
+        }
         const int nl = (int)lv_.size();
         int e;
         for (int l = 0; l < nl; ++l) {
