@@ -1366,13 +1366,14 @@ private:
             pm.v[0] = lv_[0].mx;
             pm.v[1] = from_p ? map_p_ : map_p2_;
             const KTag tag{K_PMATVEC, 0, cells(g) * (4.0 * sizeof(T) + 1.0)};
+            const int zc = lv_[0].zc;
             if (dirichlet_)
-                UAAMG_LAUNCH_SMEM(tag, (k_pmatvec<DIM, T, true>), march_grid<DIM>(g, lv_[0].zc),
-                                  dim3(kThreads), (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st,
+                UAAMG_LAUNCH_SMEM(tag, (k_pmatvec<DIM, T, true>), march_grid<DIM>(g, zc),
+                                  dim3(kThreads), (PmvCfg<DIM, T>::BYTES), pm, g, zc, pnew, ap_, st,
                                   partials_, cg_, err_);
             else
-                UAAMG_LAUNCH_SMEM(tag, (k_pmatvec<DIM, T, false>), march_grid<DIM>(g, lv_[0].zc),
-                                  dim3(kThreads), (PmvCfg<DIM, T>::BYTES), pm, g, lv_[0].zc, pnew, ap_, st,
+                UAAMG_LAUNCH_SMEM(tag, (k_pmatvec<DIM, T, false>), march_grid<DIM>(g, zc),
+                                  dim3(kThreads), (PmvCfg<DIM, T>::BYTES), pm, g, zc, pnew, ap_, st,
                                   partials_, cg_, err_);
         }
         const long long nvec = (long long)g.n / Vec16<T>::N;

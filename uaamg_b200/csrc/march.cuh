@@ -370,11 +370,17 @@ template <int DIM, class T, bool FINE, class CS = T> struct UpoCfg {
     using Lay = MLayout<T, S, P>;
     static constexpr size_t BYTES = Lay::OFF_EXTRA;
 };
+// The search-direction march forms each plane's p into one of two plane buffers
+// and frees the plane's stage at once, so 3 stages keep two planes in flight.
+// MINB: six resident blocks (40 registers) in FP32; compiled for eight (32
+// registers) it issued 16 % more instructions and ran slower (256^3: 85.9 against
+// 78.6 us a launch).
 template <int DIM, class T> struct PmvCfg {
     using P = MPlan<DIM, T, true, false, false>;
-    static constexpr int S = DIM == 2 ? 1 : sizeof(T) == 4 ? 5 : 4;
+    static constexpr int S = DIM == 2 ? 1 : 3;
+    static constexpr int MINB = sizeof(T) == 4 ? 6 : 1;
     using Lay = MLayout<T, S, P>;
-    static constexpr size_t BYTES = Lay::OFF_EXTRA;
+    static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * align128(PBox<T>::BYTES);
 };
 
 // z range of this block: planes kb .. ke-1 (3D); the single plane 0 (2D).
@@ -830,18 +836,24 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
 }
 
 // CG search direction fused with the operator: p = (z - m) + beta p_old on fluid
-// cells (pcg_3d.cpp:113-122) and Ap from the new p of the neighbours, formed on
-// the fly from the staged z and p_old (a solid or out-of-domain neighbour reads
-// p_C -- Neumann -- or -p_C at a Dirichlet wall; pcg_3d.cpp:38-55); p.Ap is
-// reduced and the last block sets alpha = rz_old / p.Ap or stops on breakdown
-// (pcg_3d.cpp:94-99).  p_old and p_new are distinct buffers.  DIRW: the problem has
-// Dirichlet walls (with Neumann walls a missing neighbour always reads p_C, so the
-// wall tests drop out; the selected values are the same).
+// cells (pcg_3d.cpp:113-122) and Ap from the new p of the neighbours (a solid or
+// out-of-domain neighbour reads p_C -- Neumann -- or -p_C at a Dirichlet wall;
+// pcg_3d.cpp:38-55); p.Ap is reduced and the last block sets alpha = rz_old / p.Ap
+// or stops on breakdown (pcg_3d.cpp:94-99).  p_old and p_new are distinct buffers.
+// DIRW: the problem has Dirichlet walls (with Neumann walls a missing neighbour
+// always reads p_C, so the wall tests drop out; the selected values are the same).
+//
+// Each plane's p is formed once, into a shared plane buffer (two, alternating):
+// step k forms plane k+1 (every thread its own pair and the pair's codes, threads
+// 0-99 the 1-cell ring) while it applies the stencil on plane k, whose p the
+// previous step formed; the step barrier hands the new plane to the in-plane
+// neighbours.  The pair's own column at k-1, k, k+1 stays in registers, so the z
+// neighbours need no shared-memory read, and a plane's ring stage is free as soon
+// as its p is formed: three stages keep two planes in flight.
 template <int DIM, class T, bool DIRW = true>
-__global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ MarchMaps M, Geom g,
-                                                      int zc, T* __restrict__ pnew,
-                                                      T* __restrict__ ap, Stencil st,
-                                                      double* partials, CGState* cg, int* err) {
+__global__ void __launch_bounds__(kThreads, DIRW ? 1 : PmvCfg<DIM, T>::MINB)
+    k_pmatvec(const __grid_constant__ MarchMaps M, Geom g, int zc, T* __restrict__ pnew,
+              T* __restrict__ ap, Stencil st, double* partials, CGState* cg, int* err) {
     pdl_entry();
     if (cg->done) return;
     using C = PmvCfg<DIM, T>;
@@ -849,6 +861,8 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
     using Lay = typename C::Lay;
     constexpr int S = C::S, W = PBox<T>::W, WC = PBox<uint8_t>::W;
     UAAMG_MARCH_SMEM(sm, err)
+    T* pbuf0 = reinterpret_cast<T*>(sm + Lay::OFF_EXTRA);
+    T* pbuf1 = reinterpret_cast<T*>(sm + Lay::OFF_EXTRA + align128(PBox<T>::BYTES));
     const int tid = threadIdx.x;
     const Pair o = own_pair<T>(g);
     const T m = (T)cg->mean_z, beta = (T)cg->beta;
@@ -864,31 +878,63 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
         ok = R.wait(R.p0) && (DIM == 2 || (R.wait(kb) && R.wait(kb + 1)));
     }
     if (!step_barrier(ok, err)) return;
+    // box position of this thread's ring cell: rows 0 and 17 (34 cells each), then
+    // columns 0 and 33 of rows 1-16
+    int rq = -1;
+    if (tid < 2 * (kMX + 2) + 2 * kMY) {
+        const int t = tid;
+        rq = t < kMX + 2               ? t
+             : t < 2 * (kMX + 2)       ? (kMY + 1) * W + (t - (kMX + 2))
+             : t < 2 * (kMX + 2) + kMY ? (t - 2 * (kMX + 2) + 1) * W
+                                       : (t - 2 * (kMX + 2) - kMY + 1) * W + kMX + 1;
+    }
     auto pv = [&](const unsigned char* s_, int qq) -> T {
         return (boxv<T>(s_, P::QB * P::VB, qq) - m) + beta * boxv<T>(s_, P::QX * P::VB, qq);
     };
-    Stages sg = stages_at<DIM, S, P>(R, kb);
-#pragma unroll 1
-    for (int k = kb; k < ke; ++k) {
-        const uint32_t cc[2] = {sg.c[P::OFF_CODE + o.ca], sg.c[P::OFF_CODE + o.ca + WC]};
-        T pc[2], a_[2] = {T(0), T(0)};
-#pragma unroll
-        for (int e = 0; e < 2; ++e) pc[e] = (cc[e] & kActive) ? pv(sg.c, o.qa + e * W) : T(0);
+    // p of the staged plane s_ into the buffer pb: the pair's cells (also returned,
+    // with their codes, B's in bits 8-15) and this thread's ring cell
+    auto form = [&](const unsigned char* s_, T* pb, T (&out)[2], uint32_t& code) {
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            const uint32_t c = cc[e];
+            out[e] = pv(s_, o.qa + e * W);
+            pb[o.qa + e * W] = out[e];
+        }
+        code = (uint32_t)s_[P::OFF_CODE + o.ca] | ((uint32_t)s_[P::OFF_CODE + o.ca + WC] << 8);
+        if (rq >= 0) pb[rq] = pv(s_, rq);
+    };
+    T pm[2] = {T(0), T(0)}, pc[2], pn[2] = {T(0), T(0)};
+    uint32_t cc, cn = 0u;
+    if (DIM == 3) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) pm[e] = pv(R.at(kb - 1), o.qa + e * W);
+    }
+    form(R.at(kb), pbuf0, pc, cc);
+    __syncthreads();
+    if (DIM == 3 && tid == 0) {
+        R.refill(M, kb - 1);
+        R.refill(M, kb);
+    }
+    T* pbc = pbuf0;
+    T* pbn = pbuf1;
+#pragma unroll 1
+    for (int k = kb; k < ke; ++k) {
+        if (DIM == 3) form(R.at(k + 1), pbn, pn, cn);
+        T a_[2] = {T(0), T(0)};
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const uint32_t c = (cc >> (8 * e)) & 0xffu;
             if (c & kActive) {
                 const int q = o.qa + e * W, i = o.i, j = o.j + e;
                 const T p0 = pc[e];
                 const T wall = DIRW && st.dirichlet ? -p0 : p0;
-                const T vL = (c & 2u) ? pv(sg.c, q - 1) : (!DIRW || i > 1 ? p0 : wall);
-                const T vR = (c & 1u) ? pv(sg.c, q + 1) : (!DIRW || i < g.nx ? p0 : wall);
+                const T vL = (c & 2u) ? pbc[q - 1] : (!DIRW || i > 1 ? p0 : wall);
+                const T vR = (c & 1u) ? pbc[q + 1] : (!DIRW || i < g.nx ? p0 : wall);
                 // the pair's other cell is the +y (A) or -y (B) neighbour
-                const T vB = (c & 8u) ? (e ? pc[0] : pv(sg.c, q - W)) : (!DIRW || j > 1 ? p0 : wall);
-                const T vT = (c & 4u) ? (e ? pv(sg.c, q + W) : pc[1]) : (!DIRW || j < g.ny ? p0 : wall);
+                const T vB = (c & 8u) ? (e ? pc[0] : pbc[q - W]) : (!DIRW || j > 1 ? p0 : wall);
+                const T vT = (c & 4u) ? (e ? pbc[q + W] : pc[1]) : (!DIRW || j < g.ny ? p0 : wall);
                 if (DIM == 3) {
-                    const T vF = (c & 32u) ? pv(sg.m, q) : (!DIRW || k > 1 ? p0 : wall);
-                    const T vK = (c & 16u) ? pv(sg.n, q) : (!DIRW || k < g.nz ? p0 : wall);
+                    const T vF = (c & 32u) ? pm[e] : (!DIRW || k > 1 ? p0 : wall);
+                    const T vK = (c & 16u) ? pn[e] : (!DIRW || k < g.nz ? p0 : wall);
                     a_[e] = sizeof(T) == 8
                                 ? diag * p0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2
                                 : ((p0 - vL) + (p0 - vR)) * idx2 + ((p0 - vB) + (p0 - vT)) * idy2 +
@@ -901,13 +947,21 @@ __global__ void __launch_bounds__(kThreads) k_pmatvec(const __grid_constant__ Ma
             }
         }
         const int id = o.gid + k * g.sxy;
-        if (o.ina) { pnew[id] = pc[0]; ap[id] = a_[0]; }
-        if (o.inb) { pnew[id + g.sx] = pc[1]; ap[id + g.sx] = a_[1]; }
+        if (o.ina) { pnew[id] = (cc & kActive) ? pc[0] : T(0); ap[id] = a_[0]; }
+        if (o.inb) { pnew[id + g.sx] = (cc & (kActive << 8)) ? pc[1] : T(0); ap[id + g.sx] = a_[1]; }
         if (DIM == 2) break;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            pm[e] = pc[e];
+            pc[e] = pn[e];
+        }
+        cc = cn;
+        T* t = pbc;
+        pbc = pbn;
+        pbn = t;
         if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
         if (!step_barrier(ok, err)) return;
-        if (tid == 0) R.refill(M, k - 1);
-        stages_next<DIM, S, P>(R, sg, k);
+        if (tid == 0) R.refill(M, k + 1);
     }
     double tot[1];
     if (reduce_last<1>(acc, partials, &cg->counter[0], tot)) {
