@@ -400,6 +400,7 @@ private:
     double *b64_ = nullptr, *xd_ = nullptr, *partials_ = nullptr;
     int* err_ = nullptr;             // set by a kernel whose TMA wait gave up
     CUtensorMap map_p_, map_p2_;     // plane boxes of the two search-direction buffers
+    CUtensorMap map_b64_, map_xd_, map_xlo_;  // plane boxes of b, x_hi (FP64) and x_lo (3D)
     SolveArgs cur_{};                // the solve in progress
     bool use_graph_ = false;
     int it_ = 0;                     // iterations queued
@@ -425,6 +426,7 @@ private:
     // blocks per SM of the 2D search direction: as many as are resident at once (one
     // wave: a second, partial wave left SMs idle at its end); UAAMG_PMV2D_PER_SM overrides
     int pmv2d_per_sm_ = 8;
+    int rx_zc_ = 16;  // planes per block of the 3D replacement march (k_resid_march)
     int pmv2d_env_ = 0;
     int resid_per_sm_ = 8;  // the FP64 residual walk: resident blocks per SM (one wave)
     bool trim_ = true;       // trimmed coarse boxes (fused.cuh k_box_trim)
@@ -738,6 +740,26 @@ private:
             if ((e = march_attrs<DIM, false, T>()) || (e = fused_attrs<DIM, false, T>())) return e;
         }
         if (DIM == 3) {
+            if ((e = smem_attr(k_resid_march<T, true>, RxCfg<T>::BYTES)) ||
+                (e = smem_attr(k_resid_march<T, false>, RxCfg<T>::BYTES)))
+                return e;
+            // planes per block of the replacement march: chunks doubled until the blocks
+            // fit in one wave (256^3: 64 planes, 512 blocks; 1.31 against 1.37 ms a solve
+            // with 32 planes and 1024 blocks)
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resid_march<T, false>, kThreads,
+                                                              RxCfg<T>::BYTES) != cudaSuccess ||
+                per_sm < 1) {
+                cudaGetLastError();
+                per_sm = 1;
+            }
+            const Geom& g = lv_[0].g;
+            const long long tiles = (long long)((g.nx + kMX - 1) / kMX) * ((g.ny + kMY - 1) / kMY);
+            rx_zc_ = 2;
+            while (rx_zc_ < g.nz && tiles * ((g.nz + rx_zc_ - 1) / rx_zc_) > (long long)per_sm * num_sms_)
+                rx_zc_ *= 2;
+        }
+        if (DIM == 3) {
             if ((e = box_attrs<true, CS>()) || (e = box_attrs<false, CS>())) return e;
             if constexpr (kHalf) {
                 if ((e = box_attrs<false, T>())) return e;
@@ -804,6 +826,11 @@ private:
         }
         if (!encode_level_map<T>(&map_p_, p_, g0, DIM, BW, BH, 1) ||
             !encode_level_map<T>(&map_p2_, p2_, g0, DIM, BW, BH, 1))
+            return E_CUDA;
+        if (DIM == 3 &&
+            (!encode_level_map<double>(&map_b64_, b64_, g0, DIM, PBox<double>::W, PBox<double>::H, 1) ||
+             !encode_level_map<double>(&map_xd_, xd_, g0, DIM, PBox<double>::W, PBox<double>::H, 1) ||
+             !encode_level_map<T>(&map_xlo_, xlo_, g0, DIM, BW, BH, 1)))
             return E_CUDA;
 
         // hierarchy: masks, couplings, coarse diagonals
@@ -1385,9 +1412,25 @@ private:
             // residual replacement (when due, one iteration in replace_every; the others
             // return at once): b, x_hi, x_lo, codes in; r out
             nopdl_next_ = true;
-            UAAMG_LAUNCH((KTag{K_REPLACE, 0, cells(g) * (17.0 + 2.0 * sizeof(T))}),
-                         (k_resid_x64<DIM, T>), resid_grid(g), dim3(32, 8), g, lv_[0].code, b64_, xd_,
-                         xlo_, r_, st, kResidZc, partials_, cg_, 5, 1, cur_.tol, cur_.tol_mode);
+            const KTag tag{K_REPLACE, 0, cells(g) * (17.0 + 2.0 * sizeof(T))};
+            if (DIM == 3) {
+                MarchMaps rm;
+                rm.v[0] = map_b64_;
+                rm.v[1] = map_xd_;
+                rm.v[2] = map_xlo_;
+                rm.code = lv_[0].mcode;
+                if (dirichlet_)
+                    UAAMG_LAUNCH_SMEM(tag, (k_resid_march<T, true>), march_grid<DIM>(g, rx_zc_),
+                                      dim3(kThreads), (RxCfg<T>::BYTES), rm, g, rx_zc_, r_, st, partials_,
+                                      cg_, 5, cur_.tol, cur_.tol_mode, err_);
+                else
+                    UAAMG_LAUNCH_SMEM(tag, (k_resid_march<T, false>), march_grid<DIM>(g, rx_zc_),
+                                      dim3(kThreads), (RxCfg<T>::BYTES), rm, g, rx_zc_, r_, st, partials_,
+                                      cg_, 5, cur_.tol, cur_.tol_mode, err_);
+            } else {
+                UAAMG_LAUNCH(tag, (k_resid_x64<DIM, T>), resid_grid(g), dim3(32, 8), g, lv_[0].code, b64_,
+                             xd_, xlo_, r_, st, kResidZc, partials_, cg_, 5, 1, cur_.tol, cur_.tol_mode);
+            }
         }
         cg_precond<DIM>();
     }

@@ -96,8 +96,11 @@ struct FCfg {
     static constexpr size_t XB = align128(RBox<T>::BYTES);
     static constexpr size_t BYTES = OFF_X + NXP * XB;
     // resident blocks per SM the finest FP32 level is compiled for (registers): 3D,
-    // five (its shared memory fits five); 2D, eight (a full SM of 256-thread blocks)
-    static constexpr int MINB = LEAN ? (DIM == 3 ? 5 : 8) : 1;
+    // five on the way down (its shared memory fits five) and four on the way up (48
+    // registers made the compiler recompute values: 256^3, 98 against 80 us a launch;
+    // the way down at four, 70 against 73 us); 2D, eight (a full SM of 256-thread
+    // blocks)
+    static constexpr int MINB = LEAN ? (DIM == 3 ? (UP ? 4 : 5) : 8) : 1;
     static_assert(S <= 16, "stage barriers: 128 bytes");
 };
 

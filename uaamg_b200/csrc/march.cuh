@@ -835,6 +835,22 @@ __global__ void __launch_bounds__(kThreads) k_up_odd(const __grid_constant__ Mar
     }
 }
 
+// The t-th cell of a plane box's 1-cell ring (t < 100) as box column a and row r:
+// rows 0 and 17 (34 cells each), then columns 0 and 33 of rows 1-16.
+__device__ __forceinline__ bool ring_cell(int t, int& a, int& r) {
+    constexpr int kRow = kMX + 2;
+    if (t >= 2 * kRow + 2 * kMY) return false;
+    if (t < 2 * kRow) {
+        a = t % kRow;
+        r = t < kRow ? 0 : kMY + 1;
+    } else {
+        const int u = t - 2 * kRow;
+        a = u < kMY ? 0 : kMX + 1;
+        r = 1 + u % kMY;
+    }
+    return true;
+}
+
 // CG search direction fused with the operator: p = (z - m) + beta p_old on fluid
 // cells (pcg_3d.cpp:113-122) and Ap from the new p of the neighbours (a solid or
 // out-of-domain neighbour reads p_C -- Neumann -- or -p_C at a Dirichlet wall;
@@ -878,16 +894,8 @@ __global__ void __launch_bounds__(kThreads, DIRW ? 1 : PmvCfg<DIM, T>::MINB)
         ok = R.wait(R.p0) && (DIM == 2 || (R.wait(kb) && R.wait(kb + 1)));
     }
     if (!step_barrier(ok, err)) return;
-    // box position of this thread's ring cell: rows 0 and 17 (34 cells each), then
-    // columns 0 and 33 of rows 1-16
-    int rq = -1;
-    if (tid < 2 * (kMX + 2) + 2 * kMY) {
-        const int t = tid;
-        rq = t < kMX + 2               ? t
-             : t < 2 * (kMX + 2)       ? (kMY + 1) * W + (t - (kMX + 2))
-             : t < 2 * (kMX + 2) + kMY ? (t - 2 * (kMX + 2) + 1) * W
-                                       : (t - 2 * (kMX + 2) - kMY + 1) * W + kMX + 1;
-    }
+    int rq = -1, ra, rr;
+    if (ring_cell(tid, ra, rr)) rq = rr * W + ra;
     auto pv = [&](const unsigned char* s_, int qq) -> T {
         return (boxv<T>(s_, P::QB * P::VB, qq) - m) + beta * boxv<T>(s_, P::QX * P::VB, qq);
     };
@@ -970,6 +978,149 @@ __global__ void __launch_bounds__(kThreads, DIRW ? 1 : PmvCfg<DIM, T>::MINB)
         if (!(pap == pap)) { cg->status = CG_NAN; cg->done = 1; }
         else if (pap < cg->breakdown) { cg->status = CG_BREAKDOWN; cg->done = 1; }
         else cg->alpha = cg->rz_old / pap;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 residual replacement of the mixed 3D solve as a z march: r = b - A x with
+// x = x_hi + x_lo (pcg_3d.cpp:38-55 operator, the arithmetic of k_resid_x64), r
+// written as T (0 on solid cells), r.r reduced; the last block asks the next x
+// update to fold x_lo into x_hi and runs the convergence test.  Each plane of b,
+// x_hi (FP64), x_lo (T) and the codes arrives as one TMA box per array; step k
+// forms x of plane k+1 once into one of two FP64 plane buffers (pairs and ring,
+// as in k_pmatvec), keeps the pair's own x at k-1, k, k+1 and b at k, k+1 in
+// registers, and applies the operator on plane k.
+template <class T>
+struct RPlan {
+    static constexpr int NV = 3;  // b, x_hi (FP64), x_lo (T)
+    static constexpr size_t DB = align128(PBox<double>::BYTES);
+    static constexpr size_t OFF_XH = DB, OFF_XL = 2 * DB;
+    static constexpr size_t OFF_CODE = OFF_XL + align128(PBox<T>::BYTES);
+    static constexpr size_t STAGE = OFF_CODE + align128(PBox<uint8_t>::BYTES);
+    static constexpr bool XCB = false;
+    static constexpr uint32_t TX_BYTES =
+        2 * PBox<double>::BYTES + PBox<T>::BYTES + PBox<uint8_t>::BYTES;
+    __host__ __device__ static constexpr size_t box_off(int q) {
+        return q == 0 ? 0 : q == 1 ? OFF_XH : OFF_XL;
+    }
+};
+template <class T> struct RxCfg {
+    using P = RPlan<T>;
+    static constexpr int S = 3;
+    using Lay = MLayout<double, S, P>;
+    static constexpr size_t BYTES = Lay::OFF_EXTRA + 2 * align128(PBox<double>::BYTES);
+};
+
+template <class T, bool DIRW = true>
+__global__ void __launch_bounds__(kThreads) k_resid_march(const __grid_constant__ MarchMaps M, Geom g,
+                                                          int zc, T* __restrict__ rw, Stencil st,
+                                                          double* partials, CGState* cg, int slot,
+                                                          double tol, int tol_mode, int* err) {
+    pdl_entry();
+    if (!replacement_due(cg)) return;
+    using C = RxCfg<T>;
+    using P = typename C::P;
+    using Lay = typename C::Lay;
+    constexpr int S = C::S, WD = PBox<double>::W, WT = PBox<T>::W, WC = PBox<uint8_t>::W;
+    UAAMG_MARCH_SMEM(sm, err)
+    double* xbuf0 = reinterpret_cast<double*>(sm + Lay::OFF_EXTRA);
+    double* xbuf1 = reinterpret_cast<double*>(sm + Lay::OFF_EXTRA + align128(PBox<double>::BYTES));
+    const int tid = threadIdx.x;
+    const Pair o = own_pair<T>(g);
+    const int qd = o.rb * WD + o.a, qt = o.rb * WT + o.a;  // A in the FP64 and T boxes
+    const double idx2 = st.idx2, idy2 = st.idy2, idz2 = st.idz2, diag = st.diag;
+    double acc[1] = {0.0};
+    int kb, ke;
+    zrange<3>(g, zc, kb, ke);
+    MRing<3, S, P> R{reinterpret_cast<uint64_t*>(sm), sm + Lay::OFF_RING, kb - 1, ke};
+    bool ok = true;
+    if (tid == 0) {
+        R.start(M);
+        ok = R.wait(R.p0) && R.wait(kb) && R.wait(kb + 1);
+    }
+    if (!step_barrier(ok, err)) return;
+    int rqd = -1, rqt = 0, ra, rr;
+    if (ring_cell(tid, ra, rr)) {
+        rqd = rr * WD + ra;
+        rqt = rr * WT + ra;
+    }
+    auto X = [&](const unsigned char* s_, int q_d, int q_t) -> double {
+        return boxv<double>(s_, P::OFF_XH, q_d) + (double)boxv<T>(s_, P::OFF_XL, q_t);
+    };
+    // x of the staged plane s_ into the buffer xb (the pair's cells also returned,
+    // with b and the codes, B's in bits 8-15) and this thread's ring cell
+    auto form = [&](const unsigned char* s_, double* xb, double (&xo)[2], double (&bo)[2],
+                    uint32_t& code) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            xo[e] = X(s_, qd + e * WD, qt + e * WT);
+            xb[qd + e * WD] = xo[e];
+            bo[e] = boxv<double>(s_, 0, qd + e * WD);
+        }
+        code = (uint32_t)s_[P::OFF_CODE + o.ca] | ((uint32_t)s_[P::OFF_CODE + o.ca + WC] << 8);
+        if (rqd >= 0) xb[rqd] = X(s_, rqd, rqt);
+    };
+    double xm[2], xc[2], xn[2] = {0.0, 0.0}, bc[2], bn[2] = {0.0, 0.0};
+    uint32_t cc, cn = 0u;
+    {
+        const unsigned char* s0 = R.at(kb - 1);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) xm[e] = X(s0, qd + e * WD, qt + e * WT);
+    }
+    form(R.at(kb), xbuf0, xc, bc, cc);
+    __syncthreads();
+    if (tid == 0) {
+        R.refill(M, kb - 1);
+        R.refill(M, kb);
+    }
+    double* xbc = xbuf0;
+    double* xbn = xbuf1;
+#pragma unroll 1
+    for (int k = kb; k < ke; ++k) {
+        form(R.at(k + 1), xbn, xn, bn, cn);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const uint32_t c = (cc >> (8 * e)) & 0xffu;
+            const int q = qd + e * WD, i = o.i, j = o.j + e;
+            const double x0 = xc[e];
+            const double wall = DIRW && st.dirichlet ? -x0 : x0;
+            const double vL = (c & 2u) ? xbc[q - 1] : (!DIRW || i > 1 ? x0 : wall);
+            const double vR = (c & 1u) ? xbc[q + 1] : (!DIRW || i < g.nx ? x0 : wall);
+            // the pair's other cell is the +y (A) or -y (B) neighbour
+            const double vB = (c & 8u) ? (e ? xc[0] : xbc[q - WD]) : (!DIRW || j > 1 ? x0 : wall);
+            const double vT = (c & 4u) ? (e ? xbc[q + WD] : xc[1]) : (!DIRW || j < g.ny ? x0 : wall);
+            const double vF = (c & 32u) ? xm[e] : (!DIRW || k > 1 ? x0 : wall);
+            const double vK = (c & 16u) ? xn[e] : (!DIRW || k < g.nz ? x0 : wall);
+            const double ax = diag * x0 - (vL + vR) * idx2 - (vB + vT) * idy2 - (vF + vK) * idz2;
+            const double r = (c & kActive) ? bc[e] - ax : 0.0;
+            if (e ? o.inb : o.ina) {
+                acc[0] += r * r;
+                rw[o.gid + k * g.sxy + (e ? g.sx : 0)] = (T)r;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            xm[e] = xc[e];
+            xc[e] = xn[e];
+            bc[e] = bn[e];
+        }
+        cc = cn;
+        double* t = xbc;
+        xbc = xbn;
+        xbn = t;
+        if (tid == 0 && k + 2 <= R.plast) ok = R.wait(k + 2);
+        if (!step_barrier(ok, err)) return;
+        if (tid == 0) R.refill(M, k + 1);
+    }
+    double tot[1];
+    if (reduce_last<1>(acc, partials, &cg->counter[slot], tot)) {
+        cg->fold = 1;
+        true_residual_done(cg, tot[0], 1, tol, tol_mode);
+        // a replacement at max_iter that did not confirm convergence ends the solve
+        if (!cg->done && cg->iter >= cg->max_iter) {
+            cg->status = CG_MAXITER;
+            cg->done = 1;
+        }
     }
 }
 
