@@ -98,8 +98,9 @@ struct FCfg {
     // resident blocks per SM the finest FP32 level is compiled for (registers): 3D,
     // five on the way down (its shared memory fits five) and four on the way up (48
     // registers made the compiler recompute values: 256^3, 98 against 80 us a launch;
-    // the way down at four, 70 against 73 us); 2D, eight (a full SM of 256-thread
-    // blocks)
+    // the way down at four, 73 against 69 us); 2D, eight (a full SM of 256-thread
+    // blocks; the 2D way up at five blocks and 48 registers: 2048 x 1024 solve 10.24
+    // against 9.99 ms)
     static constexpr int MINB = LEAN ? (DIM == 3 ? (UP ? 4 : 5) : 8) : 1;
     static_assert(S <= 16, "stage barriers: 128 bytes");
 };
