@@ -96,9 +96,10 @@ struct FCfg {
     static constexpr size_t XB = align128(RBox<T>::BYTES);
     static constexpr size_t BYTES = OFF_X + NXP * XB;
     // resident blocks per SM the finest FP32 level is compiled for (registers): 3D,
-    // five on the way down (its shared memory fits five) and four on the way up (48
-    // registers made the compiler recompute values: 256^3, 98 against 80 us a launch;
-    // the way down at four, 73 against 69 us); 2D, eight (a full SM of 256-thread
+    // five on the way down (its shared memory fits five) and four on the way up (at 48
+    // registers the compiler recomputed values: 256^3, 74.3 M against 58.0 M warp
+    // instructions, 101 against 89 us a launch; the way down at four, 73 against
+    // 69 us); 2D, eight (a full SM of 256-thread
     // blocks; the 2D way up at five blocks and 48 registers: 2048 x 1024 solve 10.24
     // against 9.99 ms)
     static constexpr int MINB = LEAN ? (DIM == 3 ? (UP ? 4 : 5) : 8) : 1;

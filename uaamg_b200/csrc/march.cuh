@@ -373,8 +373,8 @@ template <int DIM, class T, bool FINE, class CS = T> struct UpoCfg {
 // The search-direction march forms each plane's p into one of two plane buffers
 // and frees the plane's stage at once, so 3 stages keep two planes in flight.
 // MINB: six resident blocks (40 registers) in FP32; compiled for eight (32
-// registers) it issued 16 % more instructions and ran slower (256^3: 85.9 against
-// 78.6 us a launch).
+// registers) it ran slower (256^3: 85.9 against 78.6 us a launch, 69.0 M warp
+// instructions).
 template <int DIM, class T> struct PmvCfg {
     using P = MPlan<DIM, T, true, false, false>;
     static constexpr int S = DIM == 2 ? 1 : 3;
